@@ -1,0 +1,203 @@
+/*
+ * rgf.h -- C ABI of the B200 (sm_100a) recursive Green's function library.
+ *
+ * The library replaces the per-energy Fortran subroutines
+ *
+ *   green_RGF_RS   src/green_rgf.f90:3950-3958   (module green_rgf)
+ *   RGF_G          src/rgf_mod.f90:26-35         (module rgf_mod, same math)
+ *
+ * of liteQT / eXcitonQT, and the loops that call them once per energy
+ * (`do ik / !$omp do ie` at src/green_rgf.f90:2914-2925, :733-742, :968-977,
+ * :3174-3178, src/gw_sparse.f90:283-294) with one batched launch.
+ *
+ * Conventions (identical to the Fortran callers, so ISO_C_BINDING binds them
+ * with no copies):
+ *   - every matrix array is complex(8), column-major, dimension (nm,nm,nx):
+ *     element (i,j) of block l (all 0-based) sits at i + j*nm + l*nm*nm;
+ *     rgf_c16 is bit-compatible with complex(8), double _Complex and
+ *     std::complex<double>;
+ *   - `cur` is real(8) with the same (nm,nm,nx) layout;
+ *   - dimensions are int64_t so that `-i8` (ILP64, Makefile.intel:6) and
+ *     default-integer builds both bind through integer(c_int64_t);
+ *   - pointers may be host or device memory; the library detects which with
+ *     cudaPointerGetAttributes and stages host arrays itself;
+ *   - a NULL output pointer means "not requested" (the optional Fortran
+ *     arguments GRi1 / GLi1 / GGi1, and outputs a batched caller skips).
+ *
+ * Error behaviour: the reference has no error return; it prints
+ * "SEVERE warning" and substitutes a zero block for a singular inverse
+ * (green_rgf.f90:4429-4437) and drops the lead self-energy when Sancho does
+ * not converge in nmax iterations (:4513-4518).  The library reproduces both
+ * and in addition reports them: every entry point returns RGF_OK or an
+ * RGF_E* code, and per-task status words carry RGF_ST_* bits.
+ */
+#ifndef LITEQT_B200_RGF_H
+#define LITEQT_B200_RGF_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RGF_API __attribute__((visibility("default")))
+#else
+#define RGF_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct rgf_c16 { double re, im; } rgf_c16;
+
+/* return codes */
+#define RGF_OK             0
+#define RGF_E_ARG         -1   /* invalid argument (sizes, pointers) */
+#define RGF_E_CUDA        -2   /* a CUDA call failed; see rgf_last_error() */
+#define RGF_E_NOMEM       -3   /* device allocation failed */
+#define RGF_E_UNSUPPORTED -4   /* option or size not supported by this build */
+#define RGF_E_STATUS      -5   /* solve ran; some task has a non-zero status word */
+
+/* per-task status bits */
+#define RGF_ST_SINGULAR    1   /* a block inverse hit a zero pivot; block set to 0 (compat) */
+#define RGF_ST_SANCHO_NC   2   /* Sancho-Rubio hit nmax; lead self-energy dropped (compat) */
+#define RGF_ST_BAD_TASK    4   /* task descriptor rejected on the device */
+#define RGF_ST_REFINE_NC   8   /* mixed precision: refinement did not converge */
+
+/* precision modes */
+#define RGF_PREC_FP64  0       /* complex FP64 throughout: the drop-in */
+#define RGF_PREC_MIXED 1       /* split-precision GEMMs on tcgen05 with FP64 refinement */
+
+typedef struct rgf_opts {
+  int32_t struct_size;     /* sizeof(rgf_opts); filled by rgf_opts_default */
+  int32_t device;          /* CUDA device ordinal */
+  double eta_dev;          /* device broadening; 0 = z = dcmplx(E,0.0d-6) (green_rgf.f90:3974) */
+  double eta_lead;         /* Sancho broadening; 1e-3 (green_rgf.f90:4474) */
+  double boltz;            /* 8.61734e-5 eV/K (green_rgf.f90:3968); RGF_G uses 8.617333262e-5 */
+  double sancho_tol;       /* 1e-100 (green_rgf.f90:4457) */
+  int32_t sancho_nmax;     /* 100 (green_rgf.f90:4473) */
+  int32_t consistent;      /* 0: backward sweep couples with H1i(:,:,l) as the reference does
+                              (green_rgf.f90:4070); 1: with H1i(:,:,l+1) = H_{l+1,l} */
+  int32_t precision;       /* RGF_PREC_FP64 or RGF_PREC_MIXED */
+  int32_t want_T;          /* also compute Caroli T(E) (green.f90:2571-2580) */
+  int32_t verbose;         /* 1: print "SEVERE warning" lines like the reference */
+  int32_t reserved[7];
+} rgf_opts;
+
+typedef struct rgf_ctx rgf_ctx;
+
+/* One device (Hamiltonian) shared by many energy points.  Hii and H1i are
+ * (nm,nm,nx); H1i(:,:,l) couples block l-1 to block l (forward-sweep meaning),
+ * H1i(:,:,1) and Hii(:,:,1) / Hii(:,:,nx), H1i(:,:,nx) also define the two
+ * semi-infinite leads, exactly as in green_RGF_RS. */
+typedef struct rgf_device {
+  int64_t nm, nx;
+  const rgf_c16* Hii;
+  const rgf_c16* H1i;
+  double mu[2];            /* (muL, muR) eV */
+  double temp[2];          /* (TL, TR) K */
+} rgf_device;
+
+/* One (device, k, E) task: one call of green_RGF_RS.  Inputs and outputs are
+ * (nm,nm,nx) arrays of the task's device, or NULL. */
+typedef struct rgf_task {
+  int32_t device;          /* index into the rgf_device array */
+  int32_t reserved;
+  double E;                /* energy, eV */
+  const rgf_c16* sigma_lesser;   /* sigma_lesser_ph, or NULL = 0 */
+  const rgf_c16* sigma_r;        /* sigma_r_ph, or NULL = 0 */
+  rgf_c16* ldos;           /* G^R_ll        (ldos)   */
+  rgf_c16* ndens;          /* G^<_ll        (ndens)  */
+  rgf_c16* pdens;          /* G^>_ll        (pdens)  */
+  rgf_c16* GRi1;           /* G^R_{l,l+1}   (GRi1)   */
+  rgf_c16* GLi1;           /* G^<_{l,l+1}   (GLi1)   */
+  rgf_c16* GGi1;           /* GGi1 exactly as the reference fills it (green_rgf.f90:4094-4103) */
+  double* cur;             /* bond-current matrix cur(:,:,l) */
+  double* tr;              /* right-contact current spectrum (scalar) */
+  double* tre;             /* left-contact current spectrum (scalar) */
+  double* T;               /* Caroli transmission (scalar; needs opts.want_T) */
+} rgf_task;
+
+/* Per-task diagnostics written by rgf_solve_batch when `info` is non-NULL. */
+typedef struct rgf_task_info {
+  int32_t status;          /* RGF_ST_* bits */
+  int32_t sancho_iters_left;
+  int32_t sancho_iters_right;
+  int32_t n_gemm;          /* nb^3 complex products executed */
+  int32_t n_inv;           /* nb x nb inversions executed */
+  int32_t reserved;
+} rgf_task_info;
+
+/* Measurements of the last rgf_solve_batch on a context. */
+typedef struct rgf_stats {
+  double last_kernel_ms;   /* device time of its solver launches (CUDA events on its stream) */
+  double last_flops;       /* executed real flops: 8 nb^3 (n_gemm + n_inv) summed over tasks */
+  int64_t last_tasks;      /* tasks in it */
+  int64_t launches;        /* solver kernel launches since the context was created */
+  int64_t reserved[4];
+} rgf_stats;
+
+/* Options with the reference's behaviour (compat mode). */
+RGF_API void rgf_opts_default(rgf_opts* opts);
+
+/* Context: owns the device workspace and streams.  Not thread-safe: use one
+ * context per host thread, or serialise calls. */
+RGF_API int rgf_ctx_create(const rgf_opts* opts, rgf_ctx** ctx);
+RGF_API int rgf_ctx_destroy(rgf_ctx* ctx);
+RGF_API int rgf_ctx_set_opts(rgf_ctx* ctx, const rgf_opts* opts);
+RGF_API int rgf_ctx_get_stats(const rgf_ctx* ctx, rgf_stats* stats);
+
+/* Batched solve: replaces the whole `do ik / !$omp do ie / call green_RGF_RS`
+ * loop.  All tasks run in one persistent launch that drains a work queue.
+ * `stream` is a cudaStream_t (NULL = the context's stream).  The call returns
+ * when all outputs are written (host outputs copied back).  Returns RGF_OK,
+ * RGF_E_STATUS if any task status is non-zero, or an error code. */
+RGF_API int rgf_solve_batch(rgf_ctx* ctx, const rgf_device* devices, int32_t n_devices,
+                    const rgf_task* tasks, int64_t n_tasks, rgf_task_info* info, void* stream);
+
+/* Drop-in for green_RGF_RS (src/green_rgf.f90:3950): same arguments in the
+ * same order, scalars by reference.  sigma_greater_ph is accepted and unused,
+ * as in the reference.  GRi1 / GLi1 / GGi1 may be NULL (absent optional). */
+RGF_API int rgf_green_rgf_rs(rgf_ctx* ctx, const double* temp, const int64_t* nm, const int64_t* nx,
+                     const double* E, const double* mu, const rgf_c16* Hii, const rgf_c16* H1i,
+                     const rgf_c16* sigma_lesser_ph, const rgf_c16* sigma_greater_ph,
+                     const rgf_c16* sigma_r_ph, rgf_c16* ndens, rgf_c16* pdens, rgf_c16* ldos,
+                     double* tr, double* tre, double* cur, rgf_c16* GRi1, rgf_c16* GLi1,
+                     rgf_c16* GGi1);
+
+/* Drop-in for RGF_G (src/rgf_mod.f90:26): its argument order (tr, tre before
+ * the density arrays) and its BOLTZ (8.617333262e-5, parameters.f90:38). */
+RGF_API int rgf_rgf_g(rgf_ctx* ctx, const double* temperature, const int64_t* nm, const int64_t* nx,
+              const double* E, const double* mu, const rgf_c16* Hii, const rgf_c16* H1i,
+              const rgf_c16* sigma_lesser_ph, const rgf_c16* sigma_greater_ph,
+              const rgf_c16* sigma_r_ph, double* tr, double* tre, rgf_c16* ndens,
+              rgf_c16* pdens, rgf_c16* ldos, double* cur, rgf_c16* GRi1, rgf_c16* GLi1,
+              rgf_c16* GGi1);
+
+/* Strided batch over the energies of one device, in the layout the reference
+ * drivers allocate: g(nm,nm,nx,nen) (green_rgf.f90:2880-2890, one ik slice).
+ * Any array may be NULL.  Equivalent to nen calls of green_RGF_RS. */
+RGF_API int rgf_solve_energies(rgf_ctx* ctx, const rgf_device* device, int64_t nen, const double* E,
+                       const rgf_c16* sigma_lesser, const rgf_c16* sigma_r, rgf_c16* ldos,
+                       rgf_c16* ndens, rgf_c16* pdens, rgf_c16* GRi1, double* cur, double* tr,
+                       double* tre, double* T, rgf_task_info* info, void* stream);
+
+/* Terminal current of one energy sweep: sum(tr)*dE*e0/tpi/hbar*e0*spindeg/nk
+ * (green_rgf.f90:2938), summed on the device in a fixed order. */
+RGF_API int rgf_terminal_current(rgf_ctx* ctx, const double* tr, int64_t nen, double dE, double spindeg,
+                         int64_t nk, double* current);
+
+/* Electron / hole densities from Im G^<_jj and Im G^>_jj split at midgap
+ * (calc_n_electron, green_rgf.f90:3920-3945).  G arrays (nm,nm,nx,nen,nk). */
+RGF_API int rgf_calc_n_electron(rgf_ctx* ctx, const rgf_c16* G_lesser, const rgf_c16* G_greater,
+                        int64_t nen, const double* E, int64_t nm, int64_t nk, int64_t nx,
+                        double* nelec, double* pelec, const double* midgap);
+
+/* Last error message of the calling thread ("" if none). */
+RGF_API const char* rgf_last_error(void);
+
+/* Library version string. */
+RGF_API const char* rgf_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LITEQT_B200_RGF_H */

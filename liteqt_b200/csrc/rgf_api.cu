@@ -1,0 +1,554 @@
+// rgf_api.cu -- the C ABI declared in include/rgf.h.
+//
+// Host responsibilities: argument checks, host/device pointer classification
+// and staging, building the device task table, sizing the per-CTA workspace,
+// launching the persistent solver, and reporting status.  No dense arithmetic
+// happens on the host, and there is no CPU fallback: if the CUDA path cannot
+// run, the call fails with RGF_E_CUDA / RGF_E_UNSUPPORTED.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "rgf_internal.h"
+
+using namespace rgf;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define RGF_CUDA(call)                                                                   \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(RGF_E_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),    \
+                  __FILE__, __LINE__);                                                   \
+  } while (0)
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Device buffer that grows and is reused across calls.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  int reserve(size_t need) {
+    if (need <= bytes) return RGF_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    if (cudaMalloc(&p, need) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(RGF_E_NOMEM, "cudaMalloc(%zu) failed", need);
+    }
+    bytes = need;
+    return RGF_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+};
+
+}  // namespace
+
+struct rgf_ctx {
+  rgf_opts opts;
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  DevBuf work, tasks, devs, info, queue, stage;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  rgf_stats stats;
+};
+
+extern "C" void rgf_opts_default(rgf_opts* o) {
+  std::memset(o, 0, sizeof(*o));
+  o->struct_size = (int32_t)sizeof(rgf_opts);
+  o->device = 0;
+  o->eta_dev = 0.0;
+  o->eta_lead = 1e-3;
+  o->boltz = 8.61734e-05;
+  o->sancho_tol = 1e-100;
+  o->sancho_nmax = 100;
+  o->consistent = 0;
+  o->precision = RGF_PREC_FP64;
+  o->want_T = 1;
+  o->verbose = 0;
+}
+
+extern "C" const char* rgf_last_error(void) { return g_last_error.c_str(); }
+extern "C" const char* rgf_version(void) { return "liteqt_b200 rgf 0.1 (sm_100a)"; }
+
+static int check_opts(const rgf_opts* o) {
+  if (!o) return fail(RGF_E_ARG, "opts is NULL");
+  if (o->struct_size != (int32_t)sizeof(rgf_opts))
+    return fail(RGF_E_ARG, "rgf_opts.struct_size %d != %zu (header mismatch)", o->struct_size,
+                sizeof(rgf_opts));
+  if (o->sancho_nmax < 1 || o->sancho_nmax > 100000) return fail(RGF_E_ARG, "sancho_nmax out of range");
+  if (!(o->boltz > 0.0)) return fail(RGF_E_ARG, "boltz must be positive");
+  if (o->precision != RGF_PREC_FP64 && o->precision != RGF_PREC_MIXED)
+    return fail(RGF_E_ARG, "unknown precision %d", o->precision);
+  return RGF_OK;
+}
+
+extern "C" int rgf_ctx_create(const rgf_opts* opts, rgf_ctx** out) {
+  if (!out) return fail(RGF_E_ARG, "ctx out-pointer is NULL");
+  *out = nullptr;
+  rgf_opts def;
+  if (!opts) {
+    rgf_opts_default(&def);
+    opts = &def;
+  }
+  int rc = check_opts(opts);
+  if (rc) return rc;
+  std::unique_ptr<rgf_ctx> c(new rgf_ctx());
+  c->opts = *opts;
+  c->device = opts->device;
+  RGF_CUDA(cudaSetDevice(c->device));
+  RGF_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device));
+  RGF_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  RGF_CUDA(cudaEventCreate(&c->ev0));
+  RGF_CUDA(cudaEventCreate(&c->ev1));
+  std::memset(&c->stats, 0, sizeof(c->stats));
+  *out = c.release();
+  return RGF_OK;
+}
+
+extern "C" int rgf_ctx_destroy(rgf_ctx* c) {
+  if (!c) return RGF_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->work.release();
+  c->tasks.release();
+  c->devs.release();
+  c->info.release();
+  c->queue.release();
+  c->stage.release();
+  if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  delete c;
+  return RGF_OK;
+}
+
+extern "C" int rgf_ctx_get_stats(const rgf_ctx* c, rgf_stats* s) {
+  if (!c || !s) return fail(RGF_E_ARG, "NULL argument");
+  *s = c->stats;
+  return RGF_OK;
+}
+
+extern "C" int rgf_ctx_set_opts(rgf_ctx* c, const rgf_opts* o) {
+  if (!c) return fail(RGF_E_ARG, "ctx is NULL");
+  int rc = check_opts(o);
+  if (rc) return rc;
+  if (o->device != c->device) return fail(RGF_E_ARG, "cannot change the device of a context");
+  c->opts = *o;
+  return RGF_OK;
+}
+
+namespace {
+
+// Staging of host arrays.  Every host range is registered with its role;
+// touching or overlapping ranges are merged into segments (the per-energy
+// slices of one host array become one copy), and each segment gets a region
+// of one device buffer.
+struct Stage {
+  struct Item {
+    const char* host;
+    size_t bytes;
+    bool copy_in;   // input, or output whose untouched parts must survive
+    bool copy_out;  // output
+  };
+  struct Seg {
+    const char* host;
+    size_t bytes;
+    size_t off;
+    bool copy_in, copy_out;
+  };
+  std::vector<Item> items;
+  std::vector<Seg> segs;
+  size_t total = 0;
+
+  void add(const void* p, size_t bytes, bool copy_in, bool copy_out) {
+    if (!p || bytes == 0 || is_device_ptr(p)) return;
+    items.push_back({(const char*)p, bytes, copy_in, copy_out});
+  }
+  void layout() {
+    std::vector<Item> v = items;
+    std::sort(v.begin(), v.end(), [](const Item& a, const Item& b) { return a.host < b.host; });
+    segs.clear();
+    for (const Item& it : v) {
+      if (!segs.empty() && it.host <= segs.back().host + segs.back().bytes) {
+        Seg& s = segs.back();
+        const char* end = std::max(s.host + s.bytes, it.host + it.bytes);
+        s.bytes = (size_t)(end - s.host);
+        s.copy_in = s.copy_in || it.copy_in;
+        s.copy_out = s.copy_out || it.copy_out;
+      } else {
+        segs.push_back({it.host, it.bytes, 0, it.copy_in, it.copy_out});
+      }
+    }
+    total = 0;
+    for (Seg& s : segs) {
+      s.off = total;
+      total += (s.bytes + 255) & ~size_t(255);
+    }
+  }
+  // device address of a registered host pointer (or p itself if device / NULL)
+  void* resolve(const void* p, char* dbase) const {
+    if (!p) return nullptr;
+    const char* h = (const char*)p;
+    size_t lo = 0, hi = segs.size();
+    while (lo < hi) {  // last segment with host <= h
+      const size_t mid = (lo + hi) / 2;
+      if (segs[mid].host <= h) lo = mid + 1; else hi = mid;
+    }
+    if (lo > 0) {
+      const Seg& s = segs[lo - 1];
+      if (h < s.host + s.bytes) return dbase + s.off + (size_t)(h - s.host);
+    }
+    return const_cast<void*>(p);
+  }
+};
+
+}  // namespace
+
+extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_devices,
+                               const rgf_task* tasks, int64_t n_tasks, rgf_task_info* info,
+                               void* stream_) {
+  if (!c) return fail(RGF_E_ARG, "ctx is NULL");
+  if (n_tasks < 0 || (n_tasks > 0 && (!tasks || !devices || n_devices < 1)))
+    return fail(RGF_E_ARG, "invalid task list");
+  if (n_tasks == 0) return RGF_OK;
+  if (n_tasks > (int64_t)INT32_MAX) return fail(RGF_E_ARG, "too many tasks in one batch");
+  if (c->opts.precision != RGF_PREC_FP64)
+    return fail(RGF_E_UNSUPPORTED, "precision mode %d is not available in this build", c->opts.precision);
+  RGF_CUDA(cudaSetDevice(c->device));
+  cudaStream_t st = stream_ ? (cudaStream_t)stream_ : c->stream;
+  const bool want_T = c->opts.want_T != 0;
+
+  // ---- validate
+  for (int32_t d = 0; d < n_devices; d++) {
+    const rgf_device& v = devices[d];
+    if (v.nm < 8 || v.nm > kMaxNb || v.nm % 8 != 0)
+      return fail(RGF_E_UNSUPPORTED, "device %d: nm=%lld unsupported (multiple of 8 in [8,%d])", d,
+                  (long long)v.nm, kMaxNb);
+    if (v.nx < 2) return fail(RGF_E_ARG, "device %d: nx=%lld < 2", d, (long long)v.nx);
+    if (!v.Hii || !v.H1i) return fail(RGF_E_ARG, "device %d: Hii/H1i is NULL", d);
+    if (!(v.temp[0] > 0.0) || !(v.temp[1] > 0.0))
+      return fail(RGF_E_ARG, "device %d: temperature must be > 0", d);
+  }
+  for (int64_t t = 0; t < n_tasks; t++)
+    if (tasks[t].device < 0 || tasks[t].device >= n_devices)
+      return fail(RGF_E_ARG, "task %lld: device index %d out of range", (long long)t, tasks[t].device);
+
+  // ---- staging of host arrays
+  Stage sg;
+  for (int32_t d = 0; d < n_devices; d++) {
+    const size_t bytes = (size_t)devices[d].nm * devices[d].nm * devices[d].nx * sizeof(rgf_c16);
+    sg.add(devices[d].Hii, bytes, true, false);
+    sg.add(devices[d].H1i, bytes, true, false);
+  }
+  for (int64_t t = 0; t < n_tasks; t++) {
+    const rgf_task& k = tasks[t];
+    const rgf_device& v = devices[k.device];
+    const size_t cb = (size_t)v.nm * v.nm * v.nx * sizeof(rgf_c16);
+    const size_t rb = (size_t)v.nm * v.nm * v.nx * sizeof(double);
+    sg.add(k.sigma_lesser, cb, true, false);
+    sg.add(k.sigma_r, cb, true, false);
+    sg.add(k.ldos, cb, false, true);
+    sg.add(k.ndens, cb, false, true);
+    sg.add(k.pdens, cb, false, true);
+    sg.add(k.GRi1, cb, true, true);   // block nx is left untouched, as in the reference
+    sg.add(k.GLi1, cb, true, true);
+    sg.add(k.GGi1, cb, true, true);
+    sg.add(k.cur, rb, false, true);
+    sg.add(k.tr, sizeof(double), false, true);
+    sg.add(k.tre, sizeof(double), false, true);
+    if (want_T) sg.add(k.T, sizeof(double), false, true);
+  }
+  sg.layout();
+  int rc = c->stage.reserve(std::max<size_t>(sg.total, 256));
+  if (rc) return rc;
+  char* sbase = (char*)c->stage.p;
+  for (const auto& s : sg.segs)
+    if (s.copy_in) RGF_CUDA(cudaMemcpyAsync(sbase + s.off, s.host, s.bytes, cudaMemcpyHostToDevice, st));
+
+  // ---- device tables
+  std::vector<DDev> ddev(n_devices);
+  for (int32_t d = 0; d < n_devices; d++) {
+    ddev[d].nm = devices[d].nm;
+    ddev[d].nx = devices[d].nx;
+    ddev[d].Hii = (const double2*)sg.resolve(devices[d].Hii, sbase);
+    ddev[d].H1i = (const double2*)sg.resolve(devices[d].H1i, sbase);
+    for (int i = 0; i < 2; i++) {
+      ddev[d].mu[i] = devices[d].mu[i];
+      ddev[d].temp[i] = devices[d].temp[i];
+    }
+  }
+  std::vector<DTask> dtask(n_tasks);
+  for (int64_t t = 0; t < n_tasks; t++) {
+    const rgf_task& k = tasks[t];
+    DTask& o = dtask[t];
+    o.dev = k.device;
+    o.pad = 0;
+    o.E = k.E;
+    o.sig_lesser = (const double2*)sg.resolve(k.sigma_lesser, sbase);
+    o.sig_r = (const double2*)sg.resolve(k.sigma_r, sbase);
+    o.ldos = (double2*)sg.resolve(k.ldos, sbase);
+    o.ndens = (double2*)sg.resolve(k.ndens, sbase);
+    o.pdens = (double2*)sg.resolve(k.pdens, sbase);
+    o.GRi1 = (double2*)sg.resolve(k.GRi1, sbase);
+    o.GLi1 = (double2*)sg.resolve(k.GLi1, sbase);
+    o.GGi1 = (double2*)sg.resolve(k.GGi1, sbase);
+    o.cur = (double*)sg.resolve(k.cur, sbase);
+    o.tr = (double*)sg.resolve(k.tr, sbase);
+    o.tre = (double*)sg.resolve(k.tre, sbase);
+    o.T = want_T ? (double*)sg.resolve(k.T, sbase) : nullptr;
+  }
+
+  // ---- launch plan: one persistent launch per block size, longest devices first
+  std::map<int64_t, std::vector<int32_t>> groups;
+  for (int64_t t = 0; t < n_tasks; t++) groups[devices[tasks[t].device].nm].push_back((int32_t)t);
+  if (groups.size() > 64) return fail(RGF_E_ARG, "too many distinct block sizes in one batch");
+  struct Launch { int nb; int grid; int64_t nx_max, slot; size_t order_off, count; };
+  std::vector<Launch> plan;
+  std::vector<int32_t> order;
+  order.reserve(n_tasks);
+  size_t work_elems = 0;
+  for (auto& kv : groups) {
+    std::vector<int32_t> ids = kv.second;
+    std::stable_sort(ids.begin(), ids.end(), [&](int32_t a, int32_t b) {
+      return devices[tasks[a].device].nx > devices[tasks[b].device].nx;
+    });
+    Launch L;
+    L.nb = (int)kv.first;
+    L.nx_max = devices[tasks[ids.front()].device].nx;
+    L.slot = slot_elems_for(L.nb, L.nx_max);
+    L.grid = std::max(1, c->sm_count * fp64_blocks_per_sm(L.nb));
+    if ((int64_t)L.grid > (int64_t)ids.size()) L.grid = (int)ids.size();
+    L.order_off = order.size();
+    L.count = ids.size();
+    order.insert(order.end(), ids.begin(), ids.end());
+    work_elems = std::max(work_elems, (size_t)L.slot * L.grid);
+    plan.push_back(L);
+  }
+  if ((rc = c->work.reserve(sizeof(double2) * work_elems))) return rc;
+  if ((rc = c->devs.reserve(sizeof(DDev) * n_devices))) return rc;
+  if ((rc = c->tasks.reserve(sizeof(DTask) * n_tasks + sizeof(int32_t) * n_tasks))) return rc;
+  if ((rc = c->info.reserve(sizeof(DInfo) * n_tasks))) return rc;
+  if ((rc = c->queue.reserve(sizeof(int32_t) * 64))) return rc;
+  int32_t* order_d = (int32_t*)((char*)c->tasks.p + sizeof(DTask) * n_tasks);
+  RGF_CUDA(cudaMemcpyAsync(c->devs.p, ddev.data(), sizeof(DDev) * n_devices, cudaMemcpyHostToDevice, st));
+  RGF_CUDA(cudaMemcpyAsync(c->tasks.p, dtask.data(), sizeof(DTask) * n_tasks, cudaMemcpyHostToDevice, st));
+  RGF_CUDA(cudaMemcpyAsync(order_d, order.data(), sizeof(int32_t) * n_tasks, cudaMemcpyHostToDevice, st));
+  RGF_CUDA(cudaMemsetAsync(c->info.p, 0, sizeof(DInfo) * n_tasks, st));
+  RGF_CUDA(cudaMemsetAsync(c->queue.p, 0, sizeof(int32_t) * 64, st));
+  RGF_CUDA(cudaEventRecord(c->ev0, st));
+  for (size_t g = 0; g < plan.size(); g++) {
+    const Launch& L = plan[g];
+    KParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.o.eta_dev = c->opts.eta_dev;
+    p.o.eta_lead = c->opts.eta_lead;
+    p.o.boltz = c->opts.boltz;
+    p.o.sancho_tol = c->opts.sancho_tol;
+    p.o.sancho_nmax = c->opts.sancho_nmax;
+    p.o.consistent = c->opts.consistent;
+    p.o.want_T = c->opts.want_T;
+    p.devs = (const DDev*)c->devs.p;
+    p.tasks = (const DTask*)c->tasks.p;
+    p.n_tasks = (int64_t)L.count;
+    p.order = order_d + L.order_off;
+    p.queue = (int32_t*)c->queue.p + g;
+    p.work = (double2*)c->work.p;
+    p.slot_elems = L.slot;
+    p.nx_max = L.nx_max;
+    p.nb = L.nb;
+    p.info = (DInfo*)c->info.p;
+    cudaError_t e = launch_fp64(p, L.grid, st);  // launches on one stream run in order
+    if (e != cudaSuccess) return fail(RGF_E_CUDA, "solver launch failed: %s", cudaGetErrorString(e));
+    c->stats.launches++;
+  }
+  RGF_CUDA(cudaEventRecord(c->ev1, st));
+
+  // ---- outputs back
+  for (const auto& s : sg.segs)
+    if (s.copy_out)
+      RGF_CUDA(cudaMemcpyAsync(const_cast<char*>(s.host), sbase + s.off, s.bytes, cudaMemcpyDeviceToHost, st));
+  std::vector<DInfo> hinfo(n_tasks);
+  RGF_CUDA(cudaMemcpyAsync(hinfo.data(), c->info.p, sizeof(DInfo) * n_tasks, cudaMemcpyDeviceToHost, st));
+  RGF_CUDA(cudaStreamSynchronize(st));
+  int worst = 0;
+  double flops = 0.0;
+  for (int64_t t = 0; t < n_tasks; t++) {
+    worst |= hinfo[t].status;
+    const double nb = (double)devices[tasks[t].device].nm;
+    flops += 8.0 * nb * nb * nb * (double)(hinfo[t].n_gemm + hinfo[t].n_inv);
+  }
+  float kms = 0.0f;
+  RGF_CUDA(cudaEventElapsedTime(&kms, c->ev0, c->ev1));
+  c->stats.last_kernel_ms = kms;
+  c->stats.last_flops = flops;
+  c->stats.last_tasks = n_tasks;
+  if (info) std::memcpy(info, hinfo.data(), sizeof(DInfo) * n_tasks);
+  if (c->opts.verbose && worst) {
+    for (int64_t t = 0; t < n_tasks; t++) {
+      if (hinfo[t].status & RGF_ST_SINGULAR)
+        printf(" SEVERE warning: zgetrf failed (singular block), task %lld\n", (long long)t);
+      if (hinfo[t].status & RGF_ST_SANCHO_NC)
+        printf(" SEVERE warning: nmax reached in sancho!!! task %lld\n", (long long)t);
+    }
+  }
+  if (worst & RGF_ST_BAD_TASK) return fail(RGF_E_ARG, "a task was rejected on the device");
+  return worst ? RGF_E_STATUS : RGF_OK;
+}
+
+// ------------------------------------------------------------------ drop-ins
+namespace {
+
+// One default context per host thread for the per-energy drop-ins (the
+// reference calls them from `!$omp do` threads concurrently).
+struct TlsCtx {
+  rgf_ctx* ctx = nullptr;
+  double boltz = 0.0;
+  ~TlsCtx() { if (ctx) rgf_ctx_destroy(ctx); }
+};
+thread_local TlsCtx g_tls;
+
+rgf_ctx* default_ctx(double boltz, int* rc) {
+  if (!g_tls.ctx) {
+    rgf_opts o;
+    rgf_opts_default(&o);
+    o.boltz = boltz;
+    *rc = rgf_ctx_create(&o, &g_tls.ctx);
+    if (*rc) return nullptr;
+  }
+  if (g_tls.ctx->opts.boltz != boltz) g_tls.ctx->opts.boltz = boltz;
+  *rc = RGF_OK;
+  return g_tls.ctx;
+}
+
+int solve_one(rgf_ctx* ctx, double boltz, const double* temp, const int64_t* nm, const int64_t* nx,
+              const double* E, const double* mu, const rgf_c16* Hii, const rgf_c16* H1i,
+              const rgf_c16* sl, const rgf_c16* sr, rgf_c16* ndens, rgf_c16* pdens, rgf_c16* ldos,
+              double* tr, double* tre, double* cur, rgf_c16* GRi1, rgf_c16* GLi1, rgf_c16* GGi1) {
+  if (!temp || !nm || !nx || !E || !mu) return fail(RGF_E_ARG, "NULL scalar argument");
+  int rc = RGF_OK;
+  double saved_boltz = 0.0;
+  if (!ctx) {
+    ctx = default_ctx(boltz, &rc);
+    if (!ctx) return rc;
+  } else {
+    saved_boltz = ctx->opts.boltz;
+    ctx->opts.boltz = boltz;
+  }
+  rgf_device d;
+  d.nm = *nm;
+  d.nx = *nx;
+  d.Hii = Hii;
+  d.H1i = H1i;
+  d.mu[0] = mu[0];
+  d.mu[1] = mu[1];
+  d.temp[0] = temp[0];
+  d.temp[1] = temp[1];
+  rgf_task t;
+  std::memset(&t, 0, sizeof(t));
+  t.device = 0;
+  t.E = *E;
+  t.sigma_lesser = sl;
+  t.sigma_r = sr;
+  t.ldos = ldos;
+  t.ndens = ndens;
+  t.pdens = pdens;
+  t.GRi1 = GRi1;
+  t.GLi1 = GLi1;
+  t.GGi1 = GGi1;
+  t.cur = cur;
+  t.tr = tr;
+  t.tre = tre;
+  const int keepT = ctx->opts.want_T;
+  ctx->opts.want_T = 0;
+  rc = rgf_solve_batch(ctx, &d, 1, &t, 1, nullptr, nullptr);
+  ctx->opts.want_T = keepT;
+  if (saved_boltz != 0.0) ctx->opts.boltz = saved_boltz;
+  // the reference has no error return: status bits only mean "SEVERE warning"
+  return rc == RGF_E_STATUS ? RGF_OK : rc;
+}
+
+}  // namespace
+
+extern "C" int rgf_green_rgf_rs(rgf_ctx* ctx, const double* temp, const int64_t* nm, const int64_t* nx,
+                                const double* E, const double* mu, const rgf_c16* Hii,
+                                const rgf_c16* H1i, const rgf_c16* sigma_lesser_ph,
+                                const rgf_c16* sigma_greater_ph, const rgf_c16* sigma_r_ph,
+                                rgf_c16* ndens, rgf_c16* pdens, rgf_c16* ldos, double* tr,
+                                double* tre, double* cur, rgf_c16* GRi1, rgf_c16* GLi1,
+                                rgf_c16* GGi1) {
+  (void)sigma_greater_ph;  // unused by the reference as well
+  return solve_one(ctx, 8.61734e-05, temp, nm, nx, E, mu, Hii, H1i, sigma_lesser_ph, sigma_r_ph,
+                   ndens, pdens, ldos, tr, tre, cur, GRi1, GLi1, GGi1);
+}
+
+extern "C" int rgf_rgf_g(rgf_ctx* ctx, const double* temperature, const int64_t* nm,
+                         const int64_t* nx, const double* E, const double* mu, const rgf_c16* Hii,
+                         const rgf_c16* H1i, const rgf_c16* sigma_lesser_ph,
+                         const rgf_c16* sigma_greater_ph, const rgf_c16* sigma_r_ph, double* tr,
+                         double* tre, rgf_c16* ndens, rgf_c16* pdens, rgf_c16* ldos, double* cur,
+                         rgf_c16* GRi1, rgf_c16* GLi1, rgf_c16* GGi1) {
+  (void)sigma_greater_ph;
+  return solve_one(ctx, 8.617333262e-05, temperature, nm, nx, E, mu, Hii, H1i, sigma_lesser_ph,
+                   sigma_r_ph, ndens, pdens, ldos, tr, tre, cur, GRi1, GLi1, GGi1);
+}
+
+extern "C" int rgf_solve_energies(rgf_ctx* ctx, const rgf_device* device, int64_t nen,
+                                  const double* E, const rgf_c16* sigma_lesser,
+                                  const rgf_c16* sigma_r, rgf_c16* ldos, rgf_c16* ndens,
+                                  rgf_c16* pdens, rgf_c16* GRi1, double* cur, double* tr,
+                                  double* tre, double* T, rgf_task_info* info, void* stream) {
+  if (!ctx || !device || !E || nen < 0) return fail(RGF_E_ARG, "invalid argument");
+  const size_t per = (size_t)device->nm * device->nm * device->nx;
+  std::vector<rgf_task> tasks(nen);
+  for (int64_t e = 0; e < nen; e++) {
+    rgf_task& t = tasks[e];
+    std::memset(&t, 0, sizeof(t));
+    t.device = 0;
+    t.E = E[e];
+    t.sigma_lesser = sigma_lesser ? sigma_lesser + e * per : nullptr;
+    t.sigma_r = sigma_r ? sigma_r + e * per : nullptr;
+    t.ldos = ldos ? ldos + e * per : nullptr;
+    t.ndens = ndens ? ndens + e * per : nullptr;
+    t.pdens = pdens ? pdens + e * per : nullptr;
+    t.GRi1 = GRi1 ? GRi1 + e * per : nullptr;
+    t.cur = cur ? cur + e * per : nullptr;
+    t.tr = tr ? tr + e : nullptr;
+    t.tre = tre ? tre + e : nullptr;
+    t.T = T ? T + e : nullptr;
+  }
+  return rgf_solve_batch(ctx, device, 1, tasks.data(), nen, info, stream);
+}

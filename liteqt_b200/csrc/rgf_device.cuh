@@ -1,0 +1,248 @@
+// rgf_device.cuh -- block-level building blocks of the FP64 RGF kernels.
+//
+// Every routine here is executed cooperatively by all kThreads threads of one
+// CTA on nb x nb complex blocks stored column-major with leading dimension nb
+// (element (i,j) at i + j*nb, interleaved re/im as double2 -- the complex(8)
+// layout of the Fortran caller).  Pointers are generic: a block may live in
+// shared memory or in global memory (L1/L2 cached).
+//
+// The dense products run on the FP64 tensor pipe: mma.sync m8n8k4 f64
+// (DMMA), four real products per complex product.  On B200 the DMMA and DFMA
+// peaks are equal (about 37 TFLOP/s), but DMMA issues 256 FMAs per
+// instruction, which leaves the issue slots to the operand loads.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "rgf_internal.h"
+
+namespace rgf {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+
+// ---------------------------------------------------------------- complex
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ double2 czero() { return make_double2(0.0, 0.0); }
+// 1/(a+ib) with scaling so that neither |a| nor |b| overflows when squared.
+__device__ __forceinline__ double2 crecip(double2 a) {
+  const double s = fmax(fabs(a.x), fabs(a.y));
+  const double ar = a.x / s, ai = a.y / s;
+  const double d = ar * ar + ai * ai;
+  return make_double2(ar / (d * s), -ai / (d * s));
+}
+// |re| + |im|: the pivot measure of LAPACK's izamax (dcabs1), used by zgetrf.
+__device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
+
+__device__ __forceinline__ double fermi(double a) { return 1.0 / (1.0 + exp(a)); }
+
+// ---------------------------------------------------------------- DMMA
+// D(8x8) += A(8x4, row) * B(4x8, col); lane (g = lane/4, t = lane%4) holds
+// a = A[g][t], b = B[t][g], d = D[g][2t], D[g][2t+1].
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
+
+// ---------------------------------------------------------------- reductions
+struct SmemRed {
+  double v[2 * kWarps];
+};
+
+// Sum over the CTA; every thread gets the same value (fixed order).
+__device__ __forceinline__ double2 block_sum2(double2 v, SmemRed& r) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+  }
+  if (lane == 0) { r.v[2 * warp] = v.x; r.v[2 * warp + 1] = v.y; }
+  __syncthreads();
+  double2 s = czero();
+#pragma unroll
+  for (int w = 0; w < kWarps; w++) { s.x += r.v[2 * w]; s.y += r.v[2 * w + 1]; }
+  __syncthreads();
+  return s;
+}
+
+// ---------------------------------------------------------------- elementwise
+// body(i, j, idx) over every element of an n x n block.
+template <class F>
+__device__ __forceinline__ void for_each_elem(int n, F&& body) {
+  const int n2 = n * n;
+  for (int idx = threadIdx.x; idx < n2; idx += kThreads) {
+    const int j = idx / n, i = idx - j * n;
+    body(i, j, idx);
+  }
+}
+
+// ---------------------------------------------------------------- GEMM
+// C = op(A) * op(B) for n x n complex blocks, op = identity or conjugate
+// transpose (cA / cB).  The result is not stored: epi(i, j, value) is called
+// exactly once per output element, by the thread that owns it, so an epilogue
+// may read-modify-write C[i + j*n] (accumulation) or write several outputs.
+// n must be a multiple of 8*TM and 8*TN.  The caller synchronises.
+template <int TM, int TN, class Epi>
+__device__ __forceinline__ void cgemm(int n, const double2* A, bool cA, const double2* B, bool cB,
+                                      Epi&& epi) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int gm = n / (8 * TM), gn = n / (8 * TN);
+  // strides of op(A)[i][k] and op(B)[k][j] in memory
+  const int a_si = cA ? n : 1, a_sk = cA ? 1 : n;
+  const int b_sk = cB ? n : 1, b_sj = cB ? 1 : n;
+  const double a_sg = cA ? -1.0 : 1.0, b_sg = cB ? -1.0 : 1.0;
+  for (int grp = warp; grp < gm * gn; grp += kWarps) {
+    const int m0 = (grp % gm) * (8 * TM), n0 = (grp / gm) * (8 * TN);
+    double cr[TM][TN][2], ci[TM][TN][2];
+#pragma unroll
+    for (int a = 0; a < TM; a++)
+#pragma unroll
+      for (int b = 0; b < TN; b++) { cr[a][b][0] = cr[a][b][1] = ci[a][b][0] = ci[a][b][1] = 0.0; }
+    const double2* Ap[TM];
+    const double2* Bp[TN];
+#pragma unroll
+    for (int a = 0; a < TM; a++) Ap[a] = A + (m0 + 8 * a + g) * a_si + t * a_sk;
+#pragma unroll
+    for (int b = 0; b < TN; b++) Bp[b] = B + t * b_sk + (n0 + 8 * b + g) * b_sj;
+#pragma unroll 4
+    for (int k0 = 0; k0 < n; k0 += 4) {
+      double2 av[TM], bv[TN];
+#pragma unroll
+      for (int a = 0; a < TM; a++) av[a] = Ap[a][k0 * a_sk];
+#pragma unroll
+      for (int b = 0; b < TN; b++) bv[b] = Bp[b][k0 * b_sk];
+#pragma unroll
+      for (int a = 0; a < TM; a++) {
+        const double ar = av[a].x, ai = av[a].y * a_sg;
+#pragma unroll
+        for (int b = 0; b < TN; b++) {
+          const double br = bv[b].x, bi = bv[b].y * b_sg;
+          dmma884(cr[a][b][0], cr[a][b][1], ar, br);
+          dmma884(cr[a][b][0], cr[a][b][1], -ai, bi);
+          dmma884(ci[a][b][0], ci[a][b][1], ar, bi);
+          dmma884(ci[a][b][0], ci[a][b][1], ai, br);
+        }
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < TM; a++)
+#pragma unroll
+      for (int b = 0; b < TN; b++)
+#pragma unroll
+        for (int c = 0; c < 2; c++)
+          epi(m0 + 8 * a + g, n0 + 8 * b + 2 * t + c, make_double2(cr[a][b][c], ci[a][b][c]));
+  }
+}
+
+// ---------------------------------------------------------------- inverse
+struct SmemInv {
+  double2 rowk[kMaxNb];
+  double2 fcol[kMaxNb];
+  int perm[kMaxNb];
+  int colsrc[kMaxNb];
+  double2 pivval;
+  int piv;
+  int singular;
+};
+
+// In-place Gauss-Jordan inversion with partial (row) pivoting of the n x n
+// block X, then dst[:, j] = X[:, colsrc[j]] to undo the row interchanges
+// (and the same into dst2 if non-null).  Pivot: largest |re|+|im| in the
+// column, first index on ties, as LAPACK zgetrf.  A zero pivot makes the
+// result the zero block (the reference's `invert` fallback,
+// green_rgf.f90:4429-4437) and the return value 1.
+// Preconditions: X holds the matrix and is visible to all threads.
+__device__ __noinline__ static int gj_invert(int n, double2* X, double2* dst, double2* dst2, SmemInv& s) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s.singular = 0;
+  for (int k = 0; k < n; k++) {
+    if (warp == 0) {
+      double best = -1.0;
+      int bi = k;
+      for (int i = k + lane; i < n; i += 32) {
+        const double v = cabs1(X[i + k * n]);
+        if (v > best) { best = v; bi = i; }
+      }
+#pragma unroll
+      for (int o = 16; o; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      }
+      if (lane == 0) {
+        s.piv = bi;
+        s.pivval = X[bi + k * n];
+        s.perm[k] = bi;
+        if (best == 0.0) s.singular = 1;
+      }
+    }
+    __syncthreads();
+    if (s.singular) break;  // uniform
+    const int p = s.piv;
+    const double2 pinv = crecip(s.pivval);
+    // swap rows k and p, scale the new row k; X[k][k] becomes 1/pivot
+    for (int j = tid; j < n; j += kThreads) {
+      const double2 a = X[k + j * n];
+      const double2 b = X[p + j * n];
+      if (p != k) X[p + j * n] = a;
+      const double2 r = (j == k) ? pinv : cmul(b, pinv);
+      X[k + j * n] = r;
+      s.rowk[j] = r;
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += kThreads) s.fcol[i] = (i == k) ? czero() : X[i + k * n];
+    __syncthreads();
+    // X[i][j] -= f_i * rowk[j] for i != k, with X[i][k] treated as 0
+    for_each_elem(n, [&](int i, int j, int idx) {
+      if (i == k) return;
+      const double2 f = s.fcol[i];
+      const double2 x = (j == k) ? czero() : X[idx];
+      const double2 r = s.rowk[j];
+      X[idx] = make_double2(x.x - (f.x * r.x - f.y * r.y), x.y - (f.x * r.y + f.y * r.x));
+    });
+    __syncthreads();
+  }
+  const int sing = s.singular;
+  if (sing) {
+    for_each_elem(n, [&](int, int, int idx) {
+      dst[idx] = czero();
+      if (dst2) dst2[idx] = czero();
+    });
+    __syncthreads();
+    return 1;
+  }
+  if (tid == 0) {
+    for (int j = 0; j < n; j++) s.colsrc[j] = j;
+    for (int k = n - 1; k >= 0; k--) {
+      const int q = s.perm[k];
+      if (q != k) { const int tmp = s.colsrc[k]; s.colsrc[k] = s.colsrc[q]; s.colsrc[q] = tmp; }
+    }
+  }
+  __syncthreads();
+  for_each_elem(n, [&](int i, int j, int idx) {
+    const double2 v = X[i + s.colsrc[j] * n];
+    dst[idx] = v;
+    if (dst2) dst2[idx] = v;
+  });
+  __syncthreads();
+  return 0;
+}
+
+// Re/Im of Tr[A * B] = sum_{i,k} A[i][k] B[k][i] (only the diagonal of the
+// product is formed).  opB_plus: B = B1 + (B2 - B2^H) when B2 is non-null.
+__device__ __forceinline__ double2 trace_prod(int n, const double2* A, const double2* B, SmemRed& r) {
+  double2 acc = czero();
+  for_each_elem(n, [&](int i, int k, int idx) { acc = cadd(acc, cmul(A[idx], B[k + i * n])); });
+  return block_sum2(acc, r);
+}
+
+}  // namespace rgf

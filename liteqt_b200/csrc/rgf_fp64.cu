@@ -1,0 +1,497 @@
+// rgf_fp64.cu -- complex FP64 RGF solver: the drop-in form of green_RGF_RS.
+//
+// One persistent launch drains a work queue of (device, k, E) tasks; a CTA
+// takes one task at a time and runs the whole per-energy chain of the
+// reference routine green_RGF_RS (src/green_rgf.f90:3950-4164):
+//
+//   left lead   Sancho-Rubio (sancho, :4451-4537) and Sigma_L     :3990-4012
+//   forward     g_l, g^<_l for l = 2..nx-1                         :4013-4030
+//   right lead  Sancho-Rubio, Sigma_R, G_NN, G^<_NN, tr            :4031-4066
+//   backward    G_ll, G_{l,l+1}, G^<_ll, G^>_ll, cur(:,:,l)        :4069-4149
+//   left trace  tre                                                :4151-4160
+//   T(E)        Caroli Tr[Gamma_R G_N1 Gamma_L G_N1^H] (green.f90:2571-2580)
+//               from a running left-connected column g^L_{l,1}.
+//
+// Differences in *how* (not what) it is computed:
+//   - products the reference forms twice are formed once (17 complex
+//     products per backward block instead of 22; 10 when neither `cur` nor
+//     GLi1 is requested);
+//   - sums, z*I - H - Sigma assembly, Fermi-weighted Sigma^< and the
+//     G^> = G^< + G^R - G^A identity are fused into the product epilogues;
+//   - the traces tr / tre / T form only the diagonal of the final product;
+//   - the dead Sancho GBB inverse (:4527-4529) and the always-zero Glp terms
+//     of GGi1 (:4094-4103) are skipped.
+// The result is the same function of the inputs up to rounding.
+#include <cstdio>
+
+#include "rgf_device.cuh"
+#include "rgf_internal.h"
+
+namespace rgf {
+
+namespace {
+
+enum TmpBlock {
+  T_H00 = 0, T_SA, T_SB, T_HBB, T_HSS, T_H10A, T_H10B, T_H01A, T_H01B, T_GS,
+  T_SIGL, T_SIGR, T_SIG, T_F1, T_F2, T_F3, T_F4, T_GN1A, T_GN1B, T_G00A,
+  T_G00B, T_GNA, T_GNB, T_Q1, T_Q2, T_Q3, T_Q4, T_R5, T_INV,
+  T_COUNT,
+  // aliases (lifetimes do not overlap)
+  T_R7 = T_F4, T_P1 = T_F1, T_P2 = T_F2, T_P3 = T_F3, T_P4 = T_SIG,
+  T_GPN = T_SB, T_X1 = T_SA, T_X2 = T_H10A, T_Y = T_H10B, T_Z = T_H01A,
+  T_GAML = T_H01B, T_GAMR = T_HSS, T_R1 = T_GS,
+};
+static_assert(T_COUNT <= kNumTemps, "temp blocks");
+
+struct Smem {
+  SmemInv inv;
+  SmemRed red;
+  int64_t task;
+};
+
+template <int TM, int TN>
+struct Solver {
+  KOpts o;
+  int64_t nx_max;
+  Smem& sm;
+  double2* X;       // inverse workspace (shared memory if it fits, else a slot block)
+  double2* slot;
+  int n, nx;
+  size_t n2;
+  int status = 0, n_gemm = 0, n_inv = 0;
+
+  __device__ Solver(const KOpts& o_, int64_t nx_max_, Smem& sm_, double2* X_, double2* slot_,
+                    int n_, int nx_)
+      : o(o_), nx_max(nx_max_), sm(sm_), X(X_), slot(slot_), n(n_), nx(nx_), n2((size_t)n_ * n_) {}
+
+  __device__ double2* tmp(int k) const { return slot + 2 * nx_max * n2 + (size_t)k * n2; }
+  __device__ double2* Gl(int l) const { return slot + (size_t)l * n2; }
+  __device__ double2* Gln(int l) const { return slot + (nx_max + l) * n2; }
+
+  template <class Epi>
+  __device__ void gemm(const double2* A, bool cA, const double2* B, bool cB, Epi&& epi) {
+    cgemm<TM, TN>(n, A, cA, B, cB, epi);
+    n_gemm++;
+    __syncthreads();
+  }
+  // C = op(A) op(B)
+  __device__ void gemm_store(const double2* A, bool cA, const double2* B, bool cB, double2* C,
+                             double2* C2 = nullptr) {
+    const int nn = n;
+    gemm(A, cA, B, cB, [&](int i, int j, double2 v) {
+      C[i + j * nn] = v;
+      if (C2) C2[i + j * nn] = v;
+    });
+  }
+  // X holds the matrix; dst (and dst2) receive its inverse.
+  __device__ void invert_X(double2* dst, double2* dst2 = nullptr) {
+    n_inv++;
+    if (gj_invert(n, X, dst, dst2, sm.inv)) status |= RGF_ST_SINGULAR;
+  }
+
+  // sancho (green_rgf.f90:4451-4537) with S00 = I.  H00 is a slot block; the
+  // coupling argument is H10arg = conj_src ? src^H : src.  Result -> GS.
+  __device__ int sancho(double E, const double2* H00, const double2* src, bool conj_src,
+                        double2* GS) {
+    const int nn = n;
+    const double2 z = make_double2(E, o.eta_lead);
+    double2 *H10 = tmp(T_H10A), *H10n = tmp(T_H10B), *H01 = tmp(T_H01A), *H01n = tmp(T_H01B);
+    double2 *HBB = tmp(T_HBB), *HSS = tmp(T_HSS), *SA = tmp(T_SA), *SB = tmp(T_SB);
+    for_each_elem(n, [&](int i, int j, int idx) {
+      HBB[idx] = H00[idx];
+      HSS[idx] = H00[idx];
+      const double2 a = src[idx], at = src[j + i * nn];
+      H10[idx] = conj_src ? cconj(at) : a;
+      H01[idx] = conj_src ? a : cconj(at);
+    });
+    __syncthreads();
+    int taken = 0;
+    for (int it = 1; it <= o.sancho_nmax; it++) {
+      taken = it;
+      // A = inv(z*S00 - H_BB)
+      for_each_elem(n, [&](int i, int j, int idx) {
+        const double2 h = HBB[idx];
+        X[idx] = (i == j) ? make_double2(z.x - h.x, z.y - h.y) : make_double2(-h.x, -h.y);
+      });
+      __syncthreads();
+      invert_X(SA);
+      gemm_store(SA, false, H10, false, SB);                         // B = A H_10
+      gemm(H01, false, SB, false, [&](int i, int j, double2 v) {     // C = H_01 B; H_SS += C; H_BB += C
+        const int idx = i + j * nn;
+        HSS[idx] = cadd(HSS[idx], v);
+        HBB[idx] = cadd(HBB[idx], v);
+      });
+      gemm_store(H10, false, SB, false, H10n);                       // C = H_10 B  (new H_10)
+      gemm_store(SA, false, H01, false, SB);                         // B = A H_01
+      gemm(H10, false, SB, false, [&](int i, int j, double2 v) {     // A = H_10 B; H_BB += A
+        const int idx = i + j * nn;
+        HBB[idx] = cadd(HBB[idx], v);
+      });
+      double err_local = 0.0;
+      gemm(H01, false, SB, false, [&](int i, int j, double2 v) {     // C = H_01 B  (new H_01)
+        H01n[i + j * nn] = v;
+        err_local += sqrt(v.y * v.y + v.x * v.x);
+      });
+      double2* t1 = H10; H10 = H10n; H10n = t1;
+      double2* t2 = H01; H01 = H01n; H01n = t2;
+      const double err = block_sum2(make_double2(err_local, 0.0), sm.red).x;
+      if (fabs(err) < o.sancho_tol) break;
+      if (it == o.sancho_nmax) {
+        for_each_elem(n, [&](int, int, int idx) { HSS[idx] = H00[idx]; HBB[idx] = H00[idx]; });
+        __syncthreads();
+        status |= RGF_ST_SANCHO_NC;
+        taken = o.sancho_nmax + 1;
+      }
+    }
+    // G00 = inv(z*S00 - H_SS); the reference's GBB inverse is unused and skipped
+    for_each_elem(n, [&](int i, int j, int idx) {
+      const double2 h = HSS[idx];
+      X[idx] = (i == j) ? make_double2(z.x - h.x, z.y - h.y) : make_double2(-h.x, -h.y);
+    });
+    __syncthreads();
+    invert_X(GS);
+    return taken;
+  }
+
+  __device__ void run(const DTask& tk, const DDev& dv, DInfo* info) {
+    const int nn = n;
+    const double E = tk.E;
+    const double2 z = make_double2(E, o.eta_dev);
+    const double mul = dv.mu[0], mur = dv.mu[1], templ = dv.temp[0], tempr = dv.temp[1];
+    const double2* Hii = dv.Hii;
+    const double2* H1i = dv.H1i;
+    const double2* sl = tk.sig_lesser;
+    const double2* sr = tk.sig_r;
+    auto blk = [&](const double2* base, int l) { return base + (size_t)l * n2; };
+    auto wblk = [&](double2* base, int l) { return base + (size_t)l * n2; };
+    const bool want_T = o.want_T && tk.T;
+
+    // ------------------------------------------------ left contact
+    double2* H00 = tmp(T_H00);
+    for_each_elem(n, [&](int, int, int idx) {
+      H00[idx] = sr ? cadd(Hii[idx], sr[idx]) : Hii[idx];
+    });
+    __syncthreads();
+    const double2* H10 = blk(H1i, 0);
+    const int itL = sancho(E, H00, H10, true, tmp(T_GS));
+    double2* sigmal = tmp(T_SIGL);
+    gemm_store(H10, false, tmp(T_GS), false, tmp(T_F1));            // A = H10 G00
+    gemm_store(tmp(T_F1), false, H10, true, sigmal);                // sigmal = A H10^H
+    {
+      const double fl = fermi((E - mul) / (o.boltz * templ));
+      double2* sig = tmp(T_SIG);
+      for_each_elem(n, [&](int i, int j, int idx) {
+        const double2 s = sigmal[idx], st = cconj(sigmal[j + i * nn]);
+        double2 v = cscale(csub(s, st), -fl);
+        if (sl) v = cadd(v, sl[idx]);
+        sig[idx] = v;
+        const double2 h = H00[idx];
+        double2 a = (i == j) ? make_double2(z.x - h.x, z.y - h.y) : make_double2(-h.x, -h.y);
+        X[idx] = csub(a, s);                                         // A = z S00 - H00 - sigmal
+      });
+      __syncthreads();
+    }
+    invert_X(Gl(0));
+    gemm_store(Gl(0), false, tmp(T_SIG), false, tmp(T_F2));         // B = A sig
+    gemm_store(tmp(T_F2), false, Gl(0), true, Gln(0));              // Gln(1) = B A^H
+    const double2* GN1 = Gl(0);
+    double2* GN1buf[2] = {tmp(T_GN1A), tmp(T_GN1B)};
+    int gsel = 0;
+
+    // ------------------------------------------------ forward sweep
+    for (int l = 1; l <= nx - 2; l++) {
+      const double2* H = blk(H1i, l);
+      const double2* Hl = blk(Hii, l);
+      const double2* srl = sr ? blk(sr, l) : nullptr;
+      const double2* sll = sl ? blk(sl, l) : nullptr;
+      gemm_store(H, false, Gl(l - 1), false, tmp(T_F1));            // B = H10 Gl(l-1)
+      gemm(tmp(T_F1), false, H, true, [&](int i, int j, double2 v) { // A = z - H00 - B H10^H
+        const int idx = i + j * nn;
+        const double2 h = srl ? cadd(Hl[idx], srl[idx]) : Hl[idx];
+        const double2 a = (i == j) ? make_double2(z.x - h.x, z.y - h.y) : make_double2(-h.x, -h.y);
+        X[idx] = csub(a, v);
+      });
+      invert_X(Gl(l));
+      gemm_store(H, false, Gln(l - 1), false, tmp(T_F2));           // B = H10 Gln(l-1)
+      gemm(tmp(T_F2), false, H, true, [&](int i, int j, double2 v) { // C = B H10^H + sig<
+        const int idx = i + j * nn;
+        tmp(T_F3)[idx] = sll ? cadd(v, sll[idx]) : v;
+      });
+      gemm_store(Gl(l), false, tmp(T_F3), false, tmp(T_F4));        // B = A C
+      gemm_store(tmp(T_F4), false, Gl(l), true, Gln(l));            // Gln(l) = B A^H
+      if (want_T) {                                                 // g^L_{l,1} = g_l H_{l,l-1} g^L_{l-1,1}
+        gemm_store(H, false, GN1, false, tmp(T_F1));
+        gemm_store(Gl(l), false, tmp(T_F1), false, GN1buf[gsel]);
+        GN1 = GN1buf[gsel];
+        gsel ^= 1;
+      }
+    }
+
+    // ------------------------------------------------ right contact, G_NN
+    {
+      const int l = nx - 1;
+      const double2* Hl = blk(Hii, l);
+      const double2* srl = sr ? blk(sr, l) : nullptr;
+      const double2* sll = sl ? blk(sl, l) : nullptr;
+      for_each_elem(n, [&](int, int, int idx) {
+        H00[idx] = srl ? cadd(Hl[idx], srl[idx]) : Hl[idx];
+      });
+      __syncthreads();
+    }
+    const double2* H = blk(H1i, nx - 1);
+    const int itR = sancho(E, H00, H, false, tmp(T_GS));
+    double2* sigmar = tmp(T_SIGR);
+    gemm_store(H, true, tmp(T_GS), false, tmp(T_F1));               // A = H10^H G00
+    gemm_store(tmp(T_F1), false, H, false, sigmar);                 // sigmar = A H10
+    gemm_store(H, false, Gl(nx - 2), false, tmp(T_F2));             // B = H10 Gl(nx-1)
+    gemm(tmp(T_F2), false, H, true, [&](int i, int j, double2 v) {   // G00 = z - H00 - sigmar - B H10^H
+      const int idx = i + j * nn;
+      const double2 h = H00[idx];
+      double2 a = (i == j) ? make_double2(z.x - h.x, z.y - h.y) : make_double2(-h.x, -h.y);
+      a = csub(a, sigmar[idx]);
+      X[idx] = csub(a, v);
+    });
+    double2* G00 = tmp(T_G00A);
+    double2* G00n = tmp(T_G00B);
+    double2* Gn = tmp(T_GNA);
+    double2* Gnn = tmp(T_GNB);
+    invert_X(G00, tk.ldos ? wblk(tk.ldos, nx - 1) : nullptr);
+    const double fR = fermi((E - mur) / (o.boltz * templ));      // TEMPl: as the reference (:4051)
+    gemm_store(H, false, Gln(nx - 2), false, tmp(T_F3));            // B = H10 Gln(nx-1)
+    {
+      const double2* sll = sl ? blk(sl, nx - 1) : nullptr;
+      gemm(tmp(T_F3), false, H, true, [&](int i, int j, double2 v) { // sig = -(sR - sR^H) fR + C + sig<
+        const int idx = i + j * nn;
+        const double2 s = sigmar[idx], st = cconj(sigmar[j + i * nn]);
+        double2 w = cadd(cscale(csub(s, st), -fR), v);
+        if (sll) w = cadd(w, sll[idx]);
+        tmp(T_SIG)[idx] = w;
+      });
+    }
+    gemm_store(G00, false, tmp(T_SIG), false, tmp(T_F4));           // B = G00 sig
+    {
+      double2* nd = tk.ndens ? wblk(tk.ndens, nx - 1) : nullptr;
+      double2* pd = tk.pdens ? wblk(tk.pdens, nx - 1) : nullptr;
+      double2* gpn = tk.GGi1 ? tmp(T_GPN) : nullptr;
+      gemm(tmp(T_F4), false, G00, true, [&](int i, int j, double2 v) {  // Gn = B G00^H
+        const int idx = i + j * nn;
+        Gn[idx] = v;
+        if (nd) nd[idx] = v;
+        if (pd || gpn) {
+          const double2 gp = cadd(v, csub(G00[idx], cconj(G00[j + i * nn])));
+          if (pd) pd[idx] = gp;
+          if (gpn) gpn[idx] = gp;
+        }
+      });
+    }
+    {
+      // tr = -Re sum_i [ (A1 Gp)_ii - (A2 Gn)_ii ],  A1 = -(sR - sR^H) fR, A2 = -(sR - sR^H)(fR - 1)
+      double acc = 0.0;
+      for_each_elem(n, [&](int i, int k, int idx) {
+        const double2 gam = cscale(csub(sigmar[idx], cconj(sigmar[k + i * nn])), -1.0);
+        const int ki = k + i * nn;
+        const double2 gn = Gn[ki];
+        const double2 gp = cadd(gn, csub(G00[ki], cconj(G00[idx])));
+        const double2 b = cmul(cscale(gam, fR), gp);
+        const double2 c = cmul(cscale(gam, fR - 1.0), gn);
+        acc += b.x - c.x;
+      });
+      const double s = block_sum2(make_double2(acc, 0.0), sm.red).x;
+      if (tk.tr && threadIdx.x == 0) *tk.tr = -s;
+    }
+    if (want_T) {
+      gemm_store(H, false, GN1, false, tmp(T_X1));                  // H_{N,N-1} g^L_{N-1,1}
+      gemm_store(G00, false, tmp(T_X1), false, tmp(T_X2));          // G_{N1}
+      for_each_elem(n, [&](int i, int j, int idx) {                 // Gamma = i (Sigma - Sigma^H)
+        const double2 dl = csub(sigmal[idx], cconj(sigmal[j + i * nn]));
+        const double2 dr = csub(sigmar[idx], cconj(sigmar[j + i * nn]));
+        tmp(T_GAML)[idx] = make_double2(-dl.y, dl.x);
+        tmp(T_GAMR)[idx] = make_double2(-dr.y, dr.x);
+      });
+      __syncthreads();
+      gemm_store(tmp(T_GAMR), false, tmp(T_X2), false, tmp(T_Y));   // Gamma_R G_N1
+      gemm_store(tmp(T_GAML), false, tmp(T_X2), true, tmp(T_Z));    // Gamma_L G_N1^H
+      const double2 tt = trace_prod(n, tmp(T_Y), tmp(T_Z), sm.red);
+      if (threadIdx.x == 0) *tk.T = tt.x;
+    }
+
+    // ------------------------------------------------ backward sweep
+    const bool need_cur = tk.cur != nullptr;
+    const bool need_q4 = need_cur || tk.GLi1 != nullptr;
+    if (need_cur)
+      for_each_elem(n, [&](int, int, int idx) { blk2(tk.cur, nx - 1)[idx] = 0.0; });
+    for (int l = nx - 2; l >= 0; l--) {
+      const double2* Hb = blk(H1i, o.consistent ? l + 1 : l);
+      const double2* gl = Gl(l);
+      const double2* gln = Gln(l);
+      double* curl = need_cur ? blk2(tk.cur, l) : nullptr;
+      if (need_cur) {
+        gemm_store(Hb, false, gl, true, tmp(T_P1));                 // H10 Gl^H
+        gemm_store(Gn, false, tmp(T_P1), false, tmp(T_P2));         // G<_{l+1} H10 Gl^H
+        gemm_store(Hb, false, gln, false, tmp(T_P3));               // H10 Gl<
+        gemm(G00, false, tmp(T_P3), false, [&](int i, int j, double2 v) {
+          const int idx = i + j * nn;
+          tmp(T_P4)[idx] = cadd(tmp(T_P2)[idx], v);                 // C + A
+        });
+        gemm(Hb, true, tmp(T_P4), false, [&](int i, int j, double2 v) {  // G<_{l+1,l}
+          curl[i + j * nn] = v.x;
+        });
+      }
+      gemm_store(gl, false, Hb, true, tmp(T_Q1));                   // Gl H10^H
+      gemm_store(tmp(T_Q1), false, Gn, false, tmp(T_Q2));           // Gl H10^H G<
+      gemm_store(gln, false, Hb, true, tmp(T_Q3));                  // Gl< H10^H
+      if (need_q4) {
+        double2* gli = tk.GLi1 ? wblk(tk.GLi1, l) : nullptr;
+        gemm(tmp(T_Q3), false, G00, true, [&](int i, int j, double2 v) {
+          const int idx = i + j * nn;
+          const double2 w = cadd(tmp(T_Q2)[idx], v);                // G<_{l,l+1}
+          tmp(T_Q4)[idx] = w;
+          if (gli) gli[idx] = w;
+        });
+        if (need_cur)
+          gemm(Hb, false, tmp(T_Q4), false, [&](int i, int j, double2 v) {
+            const int idx = i + j * nn;
+            curl[idx] = curl[idx] - v.x;
+          });
+      }
+      if (tk.GGi1) {  // the reference's GGi1: Gl^H H10^H Gp(nx) (+ Glp terms, which are zero)
+        gemm_store(gl, true, Hb, true, tmp(T_R1));
+        gemm_store(tmp(T_R1), false, tmp(T_GPN), false, wblk(tk.GGi1, l));
+      }
+      double2* GN0 = tmp(T_F1);
+      gemm_store(tmp(T_Q1), false, G00, false, GN0, tk.GRi1 ? wblk(tk.GRi1, l) : nullptr);  // G_{l,l+1}
+      gemm_store(GN0, false, Hb, false, tmp(T_R5));                  // GN0 H10
+      {
+        double2* ld = tk.ldos ? wblk(tk.ldos, l) : nullptr;
+        gemm(tmp(T_R5), false, gl, false, [&](int i, int j, double2 v) {
+          const int idx = i + j * nn;
+          const double2 w = cadd(gl[idx], v);                         // G_ll = Gl + C
+          G00n[idx] = w;
+          if (ld) ld[idx] = w;
+        });
+      }
+      gemm_store(tmp(T_Q2), false, Hb, false, tmp(T_R7));           // Gl H10^H G< H10
+      gemm(tmp(T_R7), false, gl, true, [&](int i, int j, double2 v) {
+        const int idx = i + j * nn;
+        Gnn[idx] = cadd(gln[idx], v);                               // Gn = Gl< + C
+      });
+      gemm(tmp(T_R5), false, gln, false, [&](int i, int j, double2 v) {
+        const int idx = i + j * nn;
+        Gnn[idx] = cadd(Gnn[idx], v);                               // Gn += GN0 H10 Gl<
+      });
+      {
+        double2* nd = tk.ndens ? wblk(tk.ndens, l) : nullptr;
+        double2* pd = tk.pdens ? wblk(tk.pdens, l) : nullptr;
+        gemm(tmp(T_Q3), false, GN0, true, [&](int i, int j, double2 v) {
+          const int idx = i + j * nn;
+          const double2 w = cadd(Gnn[idx], v);                      // Gn += Gl< H10^H GN0^H
+          Gnn[idx] = w;
+          if (nd) nd[idx] = w;
+          if (pd) pd[idx] = cadd(w, csub(G00n[idx], cconj(G00n[j + i * nn])));
+        });
+      }
+      double2* t1 = G00; G00 = G00n; G00n = t1;
+      double2* t2 = Gn; Gn = Gnn; Gnn = t2;
+    }
+
+    // ------------------------------------------------ left trace (tre)
+    {
+      const double fl2 = fermi((E - mul) / (o.boltz * tempr));   // TEMPr: as the reference (:4152)
+      double acc = 0.0;
+      for_each_elem(n, [&](int i, int k, int idx) {
+        const double2 gam = cscale(csub(sigmal[idx], cconj(sigmal[k + i * nn])), -1.0);
+        const int ki = k + i * nn;
+        const double2 gn = Gn[ki];
+        const double2 gp = cadd(gn, csub(G00[ki], cconj(G00[idx])));
+        const double2 b = cmul(cscale(gam, fl2), gp);
+        const double2 c = cmul(cscale(gam, fl2 - 1.0), gn);
+        acc += b.x - c.x;
+      });
+      const double s = block_sum2(make_double2(acc, 0.0), sm.red).x;
+      if (tk.tre && threadIdx.x == 0) *tk.tre = s;
+    }
+    if (info && threadIdx.x == 0) {
+      info->status = status;
+      info->sancho_iters_left = itL;
+      info->sancho_iters_right = itR;
+      info->n_gemm = n_gemm;
+      info->n_inv = n_inv;
+    }
+    __syncthreads();
+  }
+
+  __device__ double* blk2(double* base, int l) const { return base + (size_t)l * n2; }
+};
+
+constexpr int kSmemXMaxNb = 64;  // inverse workspace in shared memory up to this nb
+
+template <int TM, int TN>
+__global__ void __launch_bounds__(kThreads, 2) rgf_fp64_kernel(KParams p) {
+  extern __shared__ double2 dyn_smem[];
+  __shared__ Smem sm;
+  double2* slot = p.work + (size_t)blockIdx.x * p.slot_elems;
+  for (;;) {
+    if (threadIdx.x == 0) sm.task = atomicAdd(p.queue, 1);
+    __syncthreads();
+    const int64_t q = sm.task;
+    __syncthreads();
+    if (q >= p.n_tasks) break;
+    const int64_t t = p.order ? p.order[q] : q;
+    const DTask tk = p.tasks[t];
+    const DDev dv = p.devs[tk.dev];
+    DInfo* info = p.info ? p.info + t : nullptr;
+    if ((int)dv.nm != p.nb || dv.nx < 2 || dv.nx > p.nx_max) {
+      if (info && threadIdx.x == 0) info->status = RGF_ST_BAD_TASK;
+      continue;
+    }
+    const int n = (int)dv.nm;
+    double2* X = (n <= kSmemXMaxNb) ? dyn_smem
+                                    : slot + 2 * p.nx_max * (size_t)n * n + (size_t)T_INV * n * n;
+    Solver<TM, TN> s(p.o, p.nx_max, sm, X, slot, n, (int)dv.nx);
+    s.run(tk, dv, info);
+  }
+}
+
+template <int TM, int TN>
+cudaError_t launch_cfg(const KParams& p, int grid, cudaStream_t st) {
+  const size_t smem = fp64_smem_bytes(p.nb);
+  auto k = rgf_fp64_kernel<TM, TN>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k<<<grid, kThreads, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
+template <int TM, int TN>
+int occupancy_cfg(int nb) {
+  int nblk = 0;
+  const size_t smem = fp64_smem_bytes(nb);
+  auto k = rgf_fp64_kernel<TM, TN>;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nblk, k, kThreads, smem) != cudaSuccess) return 1;
+  return nblk > 0 ? nblk : 1;
+}
+
+}  // namespace
+
+size_t fp64_smem_bytes(int nb) {
+  return nb <= kSmemXMaxNb ? (size_t)nb * nb * sizeof(double2) : 0;
+}
+
+int fp64_threads() { return kThreads; }
+
+// Warp tile (TM x TN subtiles of 8x8) by block size.
+cudaError_t launch_fp64(const KParams& p, int grid, cudaStream_t st) {
+  const int nb = p.nb;
+  if (nb % 16 == 0 && nb >= 64) return launch_cfg<2, 2>(p, grid, st);
+  if (nb % 16 == 0) return launch_cfg<1, 2>(p, grid, st);
+  return launch_cfg<1, 1>(p, grid, st);
+}
+
+int fp64_blocks_per_sm(int nb) {
+  if (nb % 16 == 0 && nb >= 64) return occupancy_cfg<2, 2>(nb);
+  if (nb % 16 == 0) return occupancy_cfg<1, 2>(nb);
+  return occupancy_cfg<1, 1>(nb);
+}
+
+}  // namespace rgf

@@ -1,0 +1,322 @@
+"""Python mirror of the liteQT RGF interface over the C ABI of librgf_b200.so.
+
+``green_RGF_RS`` and ``RGF_G`` keep the argument lists of the Fortran
+subroutines they replace (src/green_rgf.f90:3950, src/rgf_mod.f90:26);
+``solve_energies`` / ``solve_batch`` are the batched entry points the drivers
+use instead of their ``do ie`` loops.  Every call goes through the C ABI in
+include/rgf.h; there is no Python or CPU implementation of the solver here,
+and importing this module fails if the CUDA library has not been built.
+
+Arrays follow the Fortran layout: complex128, column-major (nm, nm, nx).  A
+NumPy array of shape (nx, nm, nm) (C order) has exactly that memory layout,
+with the last two axes being (column, row); (nen, nx, nm, nm) stacks energies.
+Host arrays are staged by the library; torch CUDA tensors are used in place.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librgf_b200.so")
+
+RGF_OK = 0
+RGF_E_ARG = -1
+RGF_E_CUDA = -2
+RGF_E_NOMEM = -3
+RGF_E_UNSUPPORTED = -4
+RGF_E_STATUS = -5
+
+RGF_ST_SINGULAR = 1
+RGF_ST_SANCHO_NC = 2
+RGF_ST_BAD_TASK = 4
+RGF_ST_REFINE_NC = 8
+
+RGF_PREC_FP64 = 0
+RGF_PREC_MIXED = 1
+
+BOLTZ_RGF_RS = 8.61734e-05       # green_rgf.f90:3968
+BOLTZ_RGF_G = 8.617333262e-05    # parameters.f90:38
+
+EXPORTS = (
+    "rgf_opts_default", "rgf_ctx_create", "rgf_ctx_destroy", "rgf_ctx_set_opts",
+    "rgf_solve_batch", "rgf_green_rgf_rs", "rgf_rgf_g", "rgf_solve_energies",
+    "rgf_terminal_current", "rgf_calc_n_electron", "rgf_last_error", "rgf_version",
+    "rgf_ctx_get_stats",
+)
+
+
+class RgfError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"rgf error {code}: {msg}")
+        self.code = code
+
+
+class c_opts(ctypes.Structure):
+    _fields_ = [
+        ("struct_size", ctypes.c_int32), ("device", ctypes.c_int32),
+        ("eta_dev", ctypes.c_double), ("eta_lead", ctypes.c_double),
+        ("boltz", ctypes.c_double), ("sancho_tol", ctypes.c_double),
+        ("sancho_nmax", ctypes.c_int32), ("consistent", ctypes.c_int32),
+        ("precision", ctypes.c_int32), ("want_T", ctypes.c_int32),
+        ("verbose", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7),
+    ]
+
+
+class c_device(ctypes.Structure):
+    _fields_ = [
+        ("nm", ctypes.c_int64), ("nx", ctypes.c_int64),
+        ("Hii", ctypes.c_void_p), ("H1i", ctypes.c_void_p),
+        ("mu", ctypes.c_double * 2), ("temp", ctypes.c_double * 2),
+    ]
+
+
+class c_task(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int32), ("reserved", ctypes.c_int32), ("E", ctypes.c_double),
+        ("sigma_lesser", ctypes.c_void_p), ("sigma_r", ctypes.c_void_p),
+        ("ldos", ctypes.c_void_p), ("ndens", ctypes.c_void_p), ("pdens", ctypes.c_void_p),
+        ("GRi1", ctypes.c_void_p), ("GLi1", ctypes.c_void_p), ("GGi1", ctypes.c_void_p),
+        ("cur", ctypes.c_void_p), ("tr", ctypes.c_void_p), ("tre", ctypes.c_void_p),
+        ("T", ctypes.c_void_p),
+    ]
+
+
+class c_stats(ctypes.Structure):
+    _fields_ = [("last_kernel_ms", ctypes.c_double), ("last_flops", ctypes.c_double),
+                ("last_tasks", ctypes.c_int64), ("launches", ctypes.c_int64),
+                ("reserved", ctypes.c_int64 * 4)]
+
+
+INFO_DTYPE = np.dtype([("status", "<i4"), ("sancho_iters_left", "<i4"),
+                       ("sancho_iters_right", "<i4"), ("n_gemm", "<i4"), ("n_inv", "<i4"),
+                       ("reserved", "<i4")])
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the CUDA library; raises if it is missing (there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m liteqt_b200.build` "
+                           "(the RGF solver has no CPU fallback)")
+    L = ctypes.CDLL(path)
+    P = ctypes.c_void_p
+    L.rgf_opts_default.argtypes = [ctypes.POINTER(c_opts)]
+    L.rgf_opts_default.restype = None
+    L.rgf_ctx_create.argtypes = [ctypes.POINTER(c_opts), ctypes.POINTER(ctypes.c_void_p)]
+    L.rgf_ctx_destroy.argtypes = [P]
+    L.rgf_ctx_set_opts.argtypes = [P, ctypes.POINTER(c_opts)]
+    L.rgf_solve_batch.argtypes = [P, ctypes.POINTER(c_device), ctypes.c_int32,
+                                  ctypes.POINTER(c_task), ctypes.c_int64, P, P]
+    L.rgf_green_rgf_rs.argtypes = [P] * 20
+    L.rgf_rgf_g.argtypes = [P] * 20
+    L.rgf_solve_energies.argtypes = [P, ctypes.POINTER(c_device), ctypes.c_int64] + [P] * 13
+    L.rgf_terminal_current.argtypes = [P, P, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_int64, P]
+    L.rgf_calc_n_electron.argtypes = [P, P, P, ctypes.c_int64, P, ctypes.c_int64, ctypes.c_int64,
+                                      ctypes.c_int64, P, P, P]
+    L.rgf_ctx_get_stats.argtypes = [P, ctypes.POINTER(c_stats)]
+    L.rgf_last_error.restype = ctypes.c_char_p
+    L.rgf_version.restype = ctypes.c_char_p
+    for name in ("rgf_ctx_create", "rgf_ctx_destroy", "rgf_ctx_set_opts", "rgf_solve_batch",
+                 "rgf_green_rgf_rs", "rgf_rgf_g", "rgf_solve_energies", "rgf_terminal_current",
+                 "rgf_calc_n_electron", "rgf_ctx_get_stats"):
+        getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return load().rgf_last_error().decode()
+
+
+def _check(rc, allow_status=False):
+    if rc == RGF_OK or (allow_status and rc == RGF_E_STATUS):
+        return rc
+    raise RgfError(rc, last_error())
+
+
+@dataclass
+class Options:
+    """rgf_opts.  Defaults reproduce green_RGF_RS (compat mode)."""
+    device: int = 0
+    eta_dev: float = 0.0
+    eta_lead: float = 1e-3
+    boltz: float = BOLTZ_RGF_RS
+    sancho_tol: float = 1e-100
+    sancho_nmax: int = 100
+    consistent: bool = False
+    precision: int = RGF_PREC_FP64
+    want_T: bool = True
+    verbose: bool = False
+
+    def c(self) -> c_opts:
+        o = c_opts()
+        load().rgf_opts_default(ctypes.byref(o))
+        o.device = self.device
+        o.eta_dev = self.eta_dev
+        o.eta_lead = self.eta_lead
+        o.boltz = self.boltz
+        o.sancho_tol = self.sancho_tol
+        o.sancho_nmax = int(self.sancho_nmax)
+        o.consistent = int(self.consistent)
+        o.precision = int(self.precision)
+        o.want_T = int(self.want_T)
+        o.verbose = int(self.verbose)
+        return o
+
+
+def _ptr(a):
+    """Address of a NumPy array or torch tensor (host or CUDA), or None."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("arrays must be C-contiguous (Fortran block layout)")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensors must be contiguous")
+        return a.data_ptr()
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+class Context:
+    """An rgf_ctx: device workspace and stream.  Use one per host thread."""
+
+    def __init__(self, opts: Options | None = None):
+        self.opts = opts or Options()
+        L = load()
+        h = ctypes.c_void_p()
+        o = self.opts.c()
+        _check(L.rgf_ctx_create(ctypes.byref(o), ctypes.byref(h)))
+        self.h = h
+
+    def stats(self) -> dict:
+        s = c_stats()
+        _check(load().rgf_ctx_get_stats(self.h, ctypes.byref(s)))
+        return dict(last_kernel_ms=s.last_kernel_ms, last_flops=s.last_flops,
+                    last_tasks=s.last_tasks, launches=s.launches)
+
+    def set_opts(self, opts: Options):
+        o = opts.c()
+        _check(load().rgf_ctx_set_opts(self.h, ctypes.byref(o)))
+        self.opts = opts
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().rgf_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ------------------------------------------------------------------ batch
+    def solve_energies(self, Hii, H1i, E, mu, temp, *, sigma_lesser=None, sigma_r=None,
+                       ldos=None, ndens=None, pdens=None, GRi1=None, cur=None, tr=None, tre=None,
+                       T=None, info=None, stream=None, allow_status=True):
+        """Solve all energies of one device (rgf_solve_energies).
+
+        Hii, H1i: (nx, nm, nm) complex128.  Per-energy arrays: (nen, nx, nm, nm);
+        tr, tre, T: (nen,) float64.  Outputs are written in place.  Returns the
+        rc (RGF_OK or RGF_E_STATUS)."""
+        nx, nm = int(Hii.shape[0]), int(Hii.shape[1])
+        d = c_device()
+        d.nm, d.nx = nm, nx
+        d.Hii, d.H1i = _ptr(Hii), _ptr(H1i)
+        d.mu[0], d.mu[1] = float(mu[0]), float(mu[1])
+        d.temp[0], d.temp[1] = float(temp[0]), float(temp[1])
+        nen = int(E.shape[0])
+        rc = load().rgf_solve_energies(
+            self.h, ctypes.byref(d), nen, _ptr(E), _ptr(sigma_lesser), _ptr(sigma_r), _ptr(ldos),
+            _ptr(ndens), _ptr(pdens), _ptr(GRi1), _ptr(cur), _ptr(tr), _ptr(tre), _ptr(T),
+            _ptr(info), stream)
+        return _check(rc, allow_status)
+
+    def solve_batch(self, devices, tasks, info=None, stream=None, allow_status=True):
+        """rgf_solve_batch with ctypes c_device / c_task arrays."""
+        nd, nt = len(devices), len(tasks)
+        DA = (c_device * nd)(*devices)
+        TA = (c_task * nt)(*tasks)
+        rc = load().rgf_solve_batch(self.h, DA, nd, TA, nt, _ptr(info), stream)
+        return _check(rc, allow_status)
+
+    def terminal_current(self, tr, dE, spindeg=1.0, nk=1):
+        out = ctypes.c_double()
+        _check(load().rgf_terminal_current(self.h, _ptr(tr), int(tr.shape[0]), float(dE),
+                                           float(spindeg), int(nk), ctypes.addressof(out)))
+        return out.value
+
+    def calc_n_electron(self, G_lesser, G_greater, E, midgap):
+        """G arrays (nk, nen, nx, nm, nm): the Fortran (nm,nm,nx,nen,nk) layout."""
+        nk, nen, nx, nm = (int(s) for s in G_lesser.shape[:4])
+        ne = np.zeros(nx)
+        pe = np.zeros(nx)
+        _check(load().rgf_calc_n_electron(self.h, _ptr(G_lesser), _ptr(G_greater), nen, _ptr(E),
+                                          nm, nk, nx, _ptr(ne), _ptr(pe), _ptr(midgap)))
+        return ne, pe
+
+
+# ---------------------------------------------------------------------- drop-ins
+def _scalar_slot(x):
+    a = np.zeros(1, np.float64) if x is None or np.isscalar(x) else x
+    return a
+
+
+def green_RGF_RS(TEMP, nm, nx, E, mu, Hii, H1i, sigma_lesser_ph, sigma_greater_ph, sigma_r_ph,
+                 ndens, pdens, ldos, tr, tre, cur, GRi1=None, GLi1=None, GGi1=None, ctx=None):
+    """Drop-in for green_RGF_RS (src/green_rgf.f90:3950), same argument order.
+
+    ndens, pdens, ldos, cur (and the optional GRi1, GLi1, GGi1) are written in
+    place.  Fortran's inout scalars tr / tre are 1-element float64 arrays
+    written in place (or None); the pair (tr, tre) is also returned."""
+    return _drop_in(load().rgf_green_rgf_rs, False, TEMP, nm, nx, E, mu, Hii, H1i,
+                    sigma_lesser_ph, sigma_greater_ph, sigma_r_ph, ndens, pdens, ldos, tr, tre,
+                    cur, GRi1, GLi1, GGi1, ctx)
+
+
+def RGF_G(temperature, nm, nx, E, mu, Hii, H1i, sigma_lesser_ph, sigma_greater_ph, sigma_r_ph,
+          tr, tre, ndens, pdens, ldos, cur, GRi1=None, GLi1=None, GGi1=None, ctx=None):
+    """Drop-in for RGF_G (src/rgf_mod.f90:26): its argument order and BOLTZ."""
+    return _drop_in(load().rgf_rgf_g, True, temperature, nm, nx, E, mu, Hii, H1i,
+                    sigma_lesser_ph, sigma_greater_ph, sigma_r_ph, ndens, pdens, ldos, tr, tre,
+                    cur, GRi1, GLi1, GGi1, ctx)
+
+
+def _drop_in(fn, rgf_g_order, TEMP, nm, nx, E, mu, Hii, H1i, sl, sg, sr, ndens, pdens, ldos, tr,
+             tre, cur, GRi1, GLi1, GGi1, ctx):
+    temp = np.ascontiguousarray(TEMP, np.float64)
+    muv = np.ascontiguousarray(mu, np.float64)
+    nm_ = ctypes.c_int64(int(nm))
+    nx_ = ctypes.c_int64(int(nx))
+    E_ = ctypes.c_double(float(E))
+    trs = _scalar_slot(tr)
+    tres = _scalar_slot(tre)
+    P = _ptr
+    h = ctx.h if ctx is not None else None
+    base = [h, P(temp), ctypes.addressof(nm_), ctypes.addressof(nx_), ctypes.addressof(E_),
+            P(muv), P(Hii), P(H1i), P(sl), P(sg), P(sr)]
+    if rgf_g_order:
+        args = base + [P(trs), P(tres), P(ndens), P(pdens), P(ldos), P(cur), P(GRi1), P(GLi1),
+                       P(GGi1)]
+    else:
+        args = base + [P(ndens), P(pdens), P(ldos), P(trs), P(tres), P(cur), P(GRi1), P(GLi1),
+                       P(GGi1)]
+    _check(fn(*args))
+    return float(trs[0]), float(tres[0])

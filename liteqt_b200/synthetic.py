@@ -1,0 +1,81 @@
+"""Seeded synthetic tight-binding devices for the RGF benchmarks and tests.
+
+No public dataset is involved: the inputs are random block-tridiagonal
+Hamiltonians with the distributions the benchmark configurations state.
+
+* H_ll: Hermitian, diagonal U[-0.5, 0.5] eV, off-diagonal complex N(0, 0.1) eV
+  (real and imaginary parts each N(0, 0.1)), Hermitised.
+* H_{l,l-1} = -2.7 eV * (I + P_l) with P_l real N(0, 0.05) entries.
+* The leads are the semi-infinite continuation of the end blocks, which is
+  what the RGF entry point does with Hii(:,:,1), H1i(:,:,1) and Hii(:,:,nx),
+  H1i(:,:,nx) (green_rgf.f90:3991-3995, :4032-4035).
+* Energies: the liteQT grid en(i) = i/nen*(emax-emin)+emin, i = 1..nen
+  (main3d.f90:658).
+
+All arrays are returned in the Fortran layout the C ABI takes: complex128,
+column-major (nm, nm, nx), exposed to NumPy as C-contiguous (nx, nm, nm)
+arrays whose last two axes are (column, row).  ``H1i[l]`` is the coupling
+block H_{l,l-1} (the forward-sweep meaning of H1i(:,:,l)).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass
+class Device:
+    nm: int
+    nx: int
+    Hii: np.ndarray   # (nx, nm, nm) complex128, Fortran block layout
+    H1i: np.ndarray   # (nx, nm, nm) complex128, Fortran block layout
+    seed: int
+
+
+def _to_fortran_blocks(B: np.ndarray) -> np.ndarray:
+    return np.ascontiguousarray(np.swapaxes(B, -1, -2))
+
+
+def make_device(nm: int, nx: int, seed: int = 1234, onsite=(-0.5, 0.5), offdiag_sigma=0.1,
+                hop=-2.7, hop_sigma=0.05, uniform_coupling=False, potential=None) -> Device:
+    """Random chain of ``nx`` blocks of ``nm`` orbitals.
+
+    ``potential`` (length nx) is added to the diagonal of each H_ll (the
+    per-block on-site potential V_l of the adjoint benchmark).
+    ``uniform_coupling`` makes every H1i block the same (the situation every
+    reference driver produces, main3d.f90:437-446).
+    """
+    rng = np.random.default_rng(seed)
+    Hb = np.empty((nx, nm, nm), np.complex128)
+    for l in range(nx):
+        X = rng.normal(0.0, offdiag_sigma, (nm, nm)) + 1j * rng.normal(0.0, offdiag_sigma, (nm, nm))
+        U = np.triu(X, 1)
+        M = U + U.conj().T
+        M[np.diag_indices(nm)] = rng.uniform(onsite[0], onsite[1], nm)
+        if potential is not None:
+            M[np.diag_indices(nm)] += potential[l]
+        Hb[l] = M
+    H1b = np.empty((nx, nm, nm), np.complex128)
+    P0 = rng.normal(0.0, hop_sigma, (nm, nm))
+    for l in range(nx):
+        P = P0 if uniform_coupling else rng.normal(0.0, hop_sigma, (nm, nm))
+        H1b[l] = hop * (np.eye(nm) + P)
+    return Device(nm, nx, _to_fortran_blocks(Hb), _to_fortran_blocks(H1b), seed)
+
+
+def uniform_chain(nm: int, nx: int, t: float = -1.0, eps: float = 0.0) -> Device:
+    """nm decoupled identical 1D chains: H_ll = eps*I, H_{l,l-1} = t*I.
+    Its exact transmission is nm inside the band |E - eps| < 2|t|."""
+    Hb = np.broadcast_to(eps * np.eye(nm, dtype=np.complex128), (nx, nm, nm)).copy()
+    H1b = np.broadcast_to(t * np.eye(nm, dtype=np.complex128), (nx, nm, nm)).copy()
+    return Device(nm, nx, _to_fortran_blocks(Hb), _to_fortran_blocks(H1b), 0)
+
+
+def energy_grid(nen: int, emin: float = -3.0, emax: float = 3.0) -> np.ndarray:
+    """en(i) = i/nen*(emax-emin)+emin, i = 1..nen (main3d.f90:658)."""
+    return np.arange(1, nen + 1, dtype=np.float64) / float(nen) * (emax - emin) + emin
+
+
+def temperature_for_kT(kT: float, boltz: float = 8.61734e-05) -> float:
+    return kT / boltz

@@ -1,0 +1,384 @@
+"""CPU oracle for the RGF hot path -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and the cpu_baseline / ``--impl
+reference`` legs of bench.py import this module, and only as the checker or
+the timed CPU baseline.  The product library never calls it.
+
+Parity status: *unpinned by reference outputs*.  The reference (Fortran 90 +
+MKL) cannot be built here and ships no tests or golden outputs.  The oracle
+is pinned instead by known answers (dense inverse of the whole device,
+Sancho fixed point, integer transmission of a uniform chain, current
+conservation) and by the two restatements agreeing with each other:
+
+* ``rgf_oracle.cpp`` (C++ + OpenBLAS), the fast one, built into
+  ``oracle/_build/librgf_oracle.so``;
+* ``rgf_numpy`` below, an independent NumPy restatement of the same
+  reference routines, for small cases.
+
+Reference routines followed (paths relative to the liteQT tree):
+``green_RGF_RS`` src/green_rgf.f90:3950-4164, ``sancho`` :4451-4537,
+``invert`` :4421-4441, ``ferm`` :4444-4447, Caroli T(E) src/green.f90:2571-2580,
+``calc_n_electron`` src/green_rgf.f90:3920-3945.
+"""
+from __future__ import annotations
+
+import ctypes
+import glob
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "librgf_oracle.so")
+
+# Constants of the reference (src/green_rgf.f90:16-24, :3968; src/parameters.f90:38)
+BOLTZ_RGF_RS = 8.61734e-05
+BOLTZ_RGF_G = 8.617333262e-05
+E0 = 1.6022e-19
+HBAR = 1.0546e-34
+PI = 3.14159265359
+TPI = 3.14159265359 * 2.0
+
+ST_SINGULAR = 1
+ST_SANCHO_NC = 2
+ST_BAD_ARGS = 4
+
+
+class OracleOpts(ctypes.Structure):
+    _fields_ = [
+        ("eta_dev", ctypes.c_double),
+        ("eta_lead", ctypes.c_double),
+        ("boltz", ctypes.c_double),
+        ("sancho_tol", ctypes.c_double),
+        ("sancho_nmax", ctypes.c_int32),
+        ("consistent", ctypes.c_int32),
+        ("want_T", ctypes.c_int32),
+        ("pad", ctypes.c_int32),
+    ]
+
+
+class OracleStat(ctypes.Structure):
+    _fields_ = [
+        ("sancho_iters_left", ctypes.c_int32),
+        ("sancho_iters_right", ctypes.c_int32),
+        ("status", ctypes.c_int32),
+        ("n_gemm", ctypes.c_int32),
+        ("n_inv", ctypes.c_int32),
+        ("pad", ctypes.c_int32),
+    ]
+
+
+STAT_DTYPE = np.dtype([("sancho_iters_left", "<i4"), ("sancho_iters_right", "<i4"),
+                       ("status", "<i4"), ("n_gemm", "<i4"), ("n_inv", "<i4"), ("pad", "<i4")])
+
+
+@dataclass
+class Opts:
+    """Mirror of the reference's behaviour switches.
+
+    Defaults reproduce green_RGF_RS exactly: device eta 0 (z = dcmplx(E,0.0d-6),
+    green_rgf.f90:3974), lead eta 1e-3 (:4474), BOLTZ 8.61734e-5 (:3968),
+    Sancho TOL 1e-100 (:4457) and nmax 100 (:4473), reference H1i indexing in
+    the backward sweep (consistent=False).
+    """
+    eta_dev: float = 0.0
+    eta_lead: float = 1e-3
+    boltz: float = BOLTZ_RGF_RS
+    sancho_tol: float = 1e-100
+    sancho_nmax: int = 100
+    consistent: bool = False
+    want_T: bool = True
+
+    def c(self) -> OracleOpts:
+        return OracleOpts(self.eta_dev, self.eta_lead, self.boltz, self.sancho_tol,
+                          int(self.sancho_nmax), int(self.consistent), int(self.want_T), 0)
+
+
+def blas_path() -> str:
+    import scipy
+    pats = [os.path.join(os.path.dirname(scipy.__file__), "..", "scipy.libs", "libscipy_openblas*.so")]
+    for p in pats:
+        hits = sorted(glob.glob(p))
+        if hits:
+            return os.path.abspath(hits[0])
+    raise RuntimeError("scipy's bundled OpenBLAS was not found")
+
+
+def build(force: bool = False) -> str:
+    src = os.path.join(HERE, "rgf_oracle.cpp")
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", HERE, "_build/librgf_oracle.so"])
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(LIB_PATH)
+        L.oracle_init.argtypes = [ctypes.c_char_p]
+        L.oracle_init.restype = ctypes.c_int
+        rc = L.oracle_init(blas_path().encode())
+        if rc != 0:
+            raise RuntimeError(f"oracle_init failed ({rc})")
+        P = ctypes.c_void_p
+        L.oracle_rgf_energy.argtypes = [ctypes.POINTER(OracleOpts), ctypes.c_int64, ctypes.c_int64,
+                                        ctypes.c_double, P, P, P, P, P, P, P, P, P, P, P, P, P, P,
+                                        P, P, ctypes.POINTER(OracleStat)]
+        L.oracle_rgf_energy.restype = ctypes.c_int
+        L.oracle_rgf_batch.argtypes = [ctypes.POINTER(OracleOpts), ctypes.c_int64, ctypes.c_int64,
+                                       ctypes.c_int64, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P,
+                                       P, ctypes.c_int]
+        L.oracle_rgf_batch.restype = ctypes.c_int
+        L.oracle_calc_n_electron.argtypes = [P, P, ctypes.c_int64, P, ctypes.c_int64,
+                                             ctypes.c_int64, ctypes.c_int64, P, P, P]
+        L.oracle_calc_n_electron.restype = None
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _fortran3(a, nm, nx, dtype=np.complex128):
+    """Return a C-contiguous (nx, nm, nm) array whose memory is the Fortran
+    (nm, nm, nx) column-major layout: element (i, j, l) at i + j*nm + l*nm^2."""
+    a = np.ascontiguousarray(a, dtype=dtype)
+    assert a.shape[-3:] == (nx, nm, nm), a.shape
+    return a
+
+
+def rgf_batch(Hii, H1i, E, mu, temp, opts: Opts | None = None, sig_lesser=None, sig_r=None,
+              outputs=("ldos", "ndens", "pdens", "cur", "GRi1"), threads: int | None = None):
+    """Run the C++ oracle over a batch of energies.
+
+    Arrays use the *block-major* NumPy view of the Fortran layout: shape
+    (nx, nm, nm) with the last two axes (col, row) -- i.e. ``X[l].T`` is the
+    mathematical block.  Use ``to_blocks`` / ``from_blocks`` to convert.
+    Returns a dict of outputs plus 'tr', 'tre', 'T', 'stats'.
+    """
+    opts = opts or Opts()
+    nx, nm, _ = Hii.shape
+    E = np.ascontiguousarray(E, dtype=np.float64)
+    nE = E.shape[0]
+    mu = np.ascontiguousarray(mu, dtype=np.float64)
+    temp = np.ascontiguousarray(temp, dtype=np.float64)
+    Hii = _fortran3(Hii, nm, nx)
+    H1i = _fortran3(H1i, nm, nx)
+    sl = None if sig_lesser is None else np.ascontiguousarray(sig_lesser, dtype=np.complex128)
+    sr = None if sig_r is None else np.ascontiguousarray(sig_r, dtype=np.complex128)
+    out = {}
+    for name in ("ldos", "ndens", "pdens", "GRi1"):
+        out[name] = np.zeros((nE, nx, nm, nm), np.complex128) if name in outputs else None
+    out["cur"] = np.zeros((nE, nx, nm, nm), np.float64) if "cur" in outputs else None
+    tr = np.zeros(nE)
+    tre = np.zeros(nE)
+    T = np.zeros(nE)
+    stats = np.zeros(nE, STAT_DTYPE)
+    if threads is None:
+        threads = os.cpu_count() or 1
+    o = opts.c()
+    rc = lib().oracle_rgf_batch(ctypes.byref(o), nm, nx, nE, _p(E), _p(mu), _p(temp), _p(Hii),
+                                _p(H1i), _p(sl), _p(sr), _p(out["ndens"]), _p(out["pdens"]),
+                                _p(out["ldos"]), _p(tr), _p(tre), _p(out["cur"]), _p(out["GRi1"]),
+                                _p(T), _p(stats), int(threads))
+    out.update(tr=tr, tre=tre, T=T, stats=stats, status=rc)
+    return out
+
+
+def calc_n_electron(G_lesser, G_greater, E, midgap):
+    """calc_n_electron (green_rgf.f90:3920-3945).  G arrays: (nk, nen, nx, nm, nm)
+    block-major views of the Fortran (nm,nm,nx,nen,nk) arrays."""
+    nk, nen, nx, nm, _ = G_lesser.shape
+    gl = np.ascontiguousarray(G_lesser, dtype=np.complex128)
+    gg = np.ascontiguousarray(G_greater, dtype=np.complex128)
+    E = np.ascontiguousarray(E, dtype=np.float64)
+    midgap = np.ascontiguousarray(midgap, dtype=np.float64)
+    ne = np.zeros(nx)
+    pe = np.zeros(nx)
+    lib().oracle_calc_n_electron(_p(gl), _p(gg), nen, _p(E), nm, nk, nx, _p(ne), _p(pe), _p(midgap))
+    return ne, pe
+
+
+def terminal_current(tr, dE, spindeg=1.0, nk=1):
+    """sum(tr)*(En(2)-En(1))*e0/tpi/hbar*e0*spindeg/nk (green_rgf.f90:2938)."""
+    return float(np.sum(tr)) * dE * E0 / TPI / HBAR * E0 * spindeg / nk
+
+
+# ---------------------------------------------------------------------------
+# Layout helpers: NumPy (nx, nm, nm) views of Fortran (nm, nm, nx) data hold
+# each block transposed.  to_blocks gives the mathematical blocks.
+def to_blocks(X):
+    return np.swapaxes(X, -1, -2)
+
+
+def from_blocks(B):
+    return np.ascontiguousarray(np.swapaxes(B, -1, -2))
+
+
+def ferm(a):
+    return 1.0 / (1.0 + np.exp(a))
+
+
+# ---------------------------------------------------------------------------
+# Independent NumPy restatement (mathematical blocks, small cases only).
+def _inv(A):
+    try:
+        return np.linalg.inv(A), 0
+    except np.linalg.LinAlgError:
+        return np.zeros_like(A), ST_SINGULAR
+
+
+def sancho_numpy(E, H00, H10, opts: Opts):
+    """sancho (green_rgf.f90:4451-4537) on mathematical blocks; S00 = I."""
+    nm = H00.shape[0]
+    z = complex(E, opts.eta_lead)
+    I = np.eye(nm)
+    H_BB = H00.copy()
+    H_SS = H00.copy()
+    H_10 = H10.copy()
+    H_01 = H_10.conj().T.copy()
+    status = 0
+    taken = 0
+    for it in range(1, opts.sancho_nmax + 1):
+        taken = it
+        A, s = _inv(z * I - H_BB)
+        status |= s
+        B = A @ H_10
+        C = H_01 @ B
+        H_SS = H_SS + C
+        H_BB = H_BB + C
+        C = H_10 @ B
+        B = A @ H_01
+        A = H_10 @ B
+        H_10 = C
+        H_BB = H_BB + A
+        C = H_01 @ B
+        H_01 = C
+        error = np.sum(np.abs(C))
+        if abs(error) < opts.sancho_tol:
+            break
+        if it == opts.sancho_nmax:
+            H_SS = H00.copy()
+            H_BB = H00.copy()
+            status |= ST_SANCHO_NC
+            taken = opts.sancho_nmax + 1
+    G00, s1 = _inv(z * I - H_SS)
+    GBB, s2 = _inv(z * I - H_BB)
+    return G00, GBB, taken, status | s1 | s2
+
+
+def rgf_numpy(Hb, H1b, E, mu, temp, opts: Opts | None = None, sigl=None, sigr=None):
+    """One energy of green_RGF_RS on mathematical blocks Hb[l], H1b[l]
+    (l = 0..nx-1; H1b[l] is H1i(:,:,l+1)).  Returns dict of block lists."""
+    opts = opts or Opts()
+    nx, nm, _ = Hb.shape
+    I = np.eye(nm)
+    z = complex(E, opts.eta_dev)
+    zero = np.zeros((nm, nm), complex)
+    sl = (lambda l: sigl[l]) if sigl is not None else (lambda l: zero)
+    sr = (lambda l: sigr[l]) if sigr is not None else (lambda l: zero)
+    mul, mur = mu
+    templ, tempr = temp
+    H = lambda X: X.conj().T
+    Gl = [None] * nx
+    Gln = [None] * nx
+    ldos = [None] * nx
+    ndens = [None] * nx
+    pdens = [None] * nx
+    cur = [None] * nx
+    GRi1 = [zero.copy() for _ in range(nx)]
+    status = 0
+    # left contact
+    H00 = Hb[0] + sr(0)
+    H10 = H1b[0]
+    G00, _, itL, s = sancho_numpy(E, H00, H(H10), opts)
+    status |= s
+    sigmal = H10 @ G00 @ H(H10)
+    fl = ferm((E - mul) / (opts.boltz * templ))
+    sig = -(sigmal - H(sigmal)) * fl + sl(0)
+    A, s = _inv(z * I - H00 - sigmal)
+    status |= s
+    Gl[0] = A
+    Gln[0] = A @ sig @ H(A)
+    GN1 = A
+    for l in range(1, nx - 1):
+        H00 = Hb[l] + sr(l)
+        H10 = H1b[l]
+        A, s = _inv(z * I - H00 - H10 @ Gl[l - 1] @ H(H10))
+        status |= s
+        Gl[l] = A
+        Gln[l] = A @ (H10 @ Gln[l - 1] @ H(H10) + sl(l)) @ H(A)
+        GN1 = A @ H10 @ GN1
+    # right contact
+    H00 = Hb[nx - 1] + sr(nx - 1)
+    H10 = H1b[nx - 1]
+    G00s, _, itR, s = sancho_numpy(E, H00, H10, opts)
+    status |= s
+    sigmar = H(H10) @ G00s @ H10
+    G00, s = _inv(z * I - H00 - sigmar - H10 @ Gl[nx - 2] @ H(H10))
+    status |= s
+    ldos[nx - 1] = G00
+    fr = ferm((E - mur) / (opts.boltz * templ))
+    sig = -(sigmar - H(sigmar)) * fr + H10 @ Gln[nx - 2] @ H(H10) + sl(nx - 1)
+    Gn = G00 @ sig @ H(G00)
+    ndens[nx - 1] = Gn
+    Gp = Gn + (G00 - H(G00))
+    pdens[nx - 1] = Gp
+    B = (-(sigmar - H(sigmar)) * fr) @ Gp
+    C = (-(sigmar - H(sigmar)) * (fr - 1.0)) @ Gn
+    tr = -np.real(np.trace(B - C))
+    gL = 1j * (sigmal - H(sigmal))
+    gR = 1j * (sigmar - H(sigmar))
+    X = G00 @ H10 @ GN1
+    T = float(np.real(np.trace(gR @ X @ gL @ H(X))))
+    # backward sweep
+    for l in range(nx - 2, -1, -1):
+        H10 = H1b[l + 1] if opts.consistent else H1b[l]
+        g = Gl[l]
+        gn = Gln[l]
+        Glow = Gn @ H10 @ H(g) + G00 @ H10 @ gn         # G<_{l+1,l} (pre-multiplied below)
+        c = np.real(H(H10) @ Glow)
+        Gup = g @ H(H10) @ Gn + gn @ H(H10) @ H(G00)     # G<_{l,l+1}
+        c = c - np.real(H10 @ Gup)
+        cur[l] = c
+        GN0 = g @ H(H10) @ G00
+        GRi1[l] = GN0
+        G00 = g + GN0 @ H10 @ g
+        ldos[l] = G00
+        Gn = gn + g @ H(H10) @ Gn @ H10 @ H(g) + GN0 @ H10 @ gn + gn @ H(H10) @ H(GN0)
+        ndens[l] = Gn
+        pdens[l] = Gn + (G00 - H(G00))
+    cur[nx - 1] = np.zeros((nm, nm))
+    Gp = Gn + (G00 - H(G00))
+    fl2 = ferm((E - mul) / (opts.boltz * tempr))
+    B = (-(sigmal - H(sigmal)) * fl2) @ Gp
+    C = (-(sigmal - H(sigmal)) * (fl2 - 1.0)) @ Gn
+    tre = float(np.real(np.trace(B - C)))
+    return dict(ldos=np.array(ldos), ndens=np.array(ndens), pdens=np.array(pdens),
+                cur=np.array(cur), GRi1=np.array(GRi1), tr=float(tr), tre=tre, T=T,
+                iters=(itL, itR), status=status, sigmal=sigmal, sigmar=sigmar)
+
+
+def dense_green(Hb, H1b, E, sigmal, sigmar, eta_dev=0.0, sigr=None):
+    """Known answer: invert the whole device (E - H - Sigma)^-1 with the
+    consistent coupling H_{l,l-1} = H1b[l].  Returns the full G^R matrix."""
+    nx, nm, _ = Hb.shape
+    N = nx * nm
+    M = np.zeros((N, N), complex)
+    for l in range(nx):
+        s = slice(l * nm, (l + 1) * nm)
+        M[s, s] = Hb[l] + (sigr[l] if sigr is not None else 0)
+        if l > 0:
+            p = slice((l - 1) * nm, l * nm)
+            M[s, p] = H1b[l]
+            M[p, s] = H1b[l].conj().T
+    M[:nm, :nm] += sigmal
+    M[-nm:, -nm:] += sigmar
+    return np.linalg.inv(complex(E, eta_dev) * np.eye(N) - M)

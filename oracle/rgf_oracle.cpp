@@ -1,0 +1,492 @@
+// rgf_oracle.cpp -- CPU restatement of the reference RGF hot path.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA library in
+// liteqt_b200/csrc: it is called by tests/, by __graft_entry__.smoke() and by
+// the cpu_baseline / --impl reference legs of bench.py, and by nothing else.
+// The product path never links, loads or calls it.
+//
+// Parity status: the reference (Fortran 90 + MKL) cannot be compiled in this
+// environment (no Fortran compiler, no MKL) and ships no tests or golden
+// outputs, so this restatement is NOT pinned to outputs of the reference
+// itself ("parity unpinned" by reference outputs).  It is pinned instead by
+// known answers (dense (E-H-Sigma)^-1 inverse, the Sancho fixed point, the
+// integer transmission of a uniform chain, tr = tre current conservation) and
+// by an independent NumPy restatement in oracle/oracle.py.
+//
+// What follows the reference line by line (paths relative to the liteQT tree):
+//   green_RGF_RS     src/green_rgf.f90:3950-4164   (rgf_energy below)
+//   RGF_G            src/rgf_mod.f90:26-237        (same math, other BOLTZ)
+//   sancho           src/green_rgf.f90:4451-4537   (sancho below)
+//   invert           src/green_rgf.f90:4421-4441   (invert below)
+//   ferm             src/green_rgf.f90:4444-4447   (ferm below)
+//   Caroli T(E)      src/green.f90:2571-2580       (transmission, new on the RGF path)
+//   calc_n_electron  src/green_rgf.f90:3920-3945
+//   terminal current src/green_rgf.f90:2938
+//
+// Dense arithmetic goes through OpenBLAS (zgemm / zgetrf / zgetri, the build
+// bundled with scipy, LP64) opened with dlopen; the library path is handed in
+// by the Python wrapper.  These are the same LAPACK algorithms MKL runs
+// (partial-pivot LU, getri), so results differ from MKL in the last bits only.
+
+#include <atomic>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <dlfcn.h>
+#include <thread>
+#include <vector>
+
+typedef std::complex<double> cd;
+
+extern "C" {
+typedef void (*zgemm_fn)(const char*, const char*, const int*, const int*, const int*,
+                         const cd*, const cd*, const int*, const cd*, const int*,
+                         const cd*, cd*, const int*);
+typedef void (*zgetrf_fn)(const int*, const int*, cd*, const int*, int*, int*);
+typedef void (*zgetri_fn)(const int*, cd*, const int*, const int*, cd*, const int*, int*);
+typedef void (*setnt_fn)(int);
+}
+
+static zgemm_fn p_zgemm = nullptr;
+static zgetrf_fn p_zgetrf = nullptr;
+static zgetri_fn p_zgetri = nullptr;
+static setnt_fn p_setnt = nullptr;
+
+// Options that select between the reference's exact behaviour ("compat") and
+// the physically consistent variants.  Must match struct oracle_opts in oracle.py.
+struct OracleOpts {
+  double eta_dev;      // device broadening; reference: z = dcmplx(E, 0.0d-6) -> 0  (green_rgf.f90:3974)
+  double eta_lead;     // Sancho broadening; reference: 1e-3                       (green_rgf.f90:4474)
+  double boltz;        // 8.61734e-5 (green_rgf.f90:3968) or 8.617333262e-5 (parameters.f90:38)
+  double sancho_tol;   // 1e-100 (green_rgf.f90:4457)
+  int32_t sancho_nmax; // 100 (green_rgf.f90:4473)
+  int32_t consistent;  // 0: reference H1i indexing in the backward sweep; 1: H1i(l+1)
+  int32_t want_T;      // compute Caroli T(E) with a running G_{N1} product
+  int32_t pad;
+};
+
+// Counters and status per energy point.  Must match oracle.py.
+struct OracleStat {
+  int32_t sancho_iters_left;
+  int32_t sancho_iters_right;
+  int32_t status;       // bit0 singular block, bit1 Sancho not converged
+  int32_t n_gemm;       // zgemm calls made
+  int32_t n_inv;        // invert calls made
+  int32_t pad;
+};
+
+enum { ST_SINGULAR = 1, ST_SANCHO_NC = 2, ST_BAD_ARGS = 4 };
+
+extern "C" int oracle_init(const char* blas_path) {
+  void* h = dlopen(blas_path, RTLD_NOW | RTLD_LOCAL);
+  if (!h) return -1;
+  p_zgemm = (zgemm_fn)dlsym(h, "scipy_zgemm_");
+  p_zgetrf = (zgetrf_fn)dlsym(h, "scipy_zgetrf_");
+  p_zgetri = (zgetri_fn)dlsym(h, "scipy_zgetri_");
+  p_setnt = (setnt_fn)dlsym(h, "scipy_openblas_set_num_threads");
+  if (!p_zgemm || !p_zgetrf || !p_zgetri) return -2;
+  if (p_setnt) p_setnt(1);  // one BLAS thread per call, like libmkl_sequential (Makefile.intel:7)
+  return 0;
+}
+
+namespace {
+
+struct Work {
+  int nm;
+  OracleStat* st;
+  std::vector<cd> lu_work;
+  std::vector<int> ipiv;
+  explicit Work(int n, OracleStat* s) : nm(n), st(s), lu_work((size_t)n * n), ipiv(n) {}
+
+  // C = op(A) * op(B), alpha = 1, beta = 0 (every zgemm of green_RGF_RS)
+  void gemm(char ta, char tb, const cd* A, const cd* B, cd* C) {
+    const cd one(1.0, 0.0), zero(0.0, 0.0);
+    p_zgemm(&ta, &tb, &nm, &nm, &nm, &one, A, &nm, B, &nm, &zero, C, &nm);
+    st->n_gemm++;
+  }
+
+  // invert: green_rgf.f90:4421-4441.  zgetrf + zgetri; on info /= 0 the
+  // reference prints a warning and returns the zero matrix.
+  void invert(cd* A) {
+    int info = 0;
+    const int lw = nm * nm;
+    st->n_inv++;
+    p_zgetrf(&nm, &nm, A, &nm, ipiv.data(), &info);
+    if (info != 0) {
+      std::fill(A, A + (size_t)nm * nm, cd(0.0, 0.0));
+      st->status |= ST_SINGULAR;
+      return;
+    }
+    p_zgetri(&nm, A, &nm, ipiv.data(), lu_work.data(), &lw, &info);
+    if (info != 0) {
+      std::fill(A, A + (size_t)nm * nm, cd(0.0, 0.0));
+      st->status |= ST_SINGULAR;
+    }
+  }
+};
+
+inline double ferm(double a) { return 1.0 / (1.0 + std::exp(a)); }  // green_rgf.f90:4444-4447
+
+inline size_t nn(int nm) { return (size_t)nm * nm; }
+
+// sancho: green_rgf.f90:4451-4537 (S00 = identity at every call site).
+// Returns the iteration count taken (nmax+1 encodes "not converged").
+int sancho(Work& w, const OracleOpts& o, double E, const cd* H00, const cd* H10,
+           cd* G00, cd* GBB) {
+  const int nm = w.nm;
+  const size_t n2 = nn(nm);
+  std::vector<cd> A(n2), B(n2), C(n2), H_BB(H00, H00 + n2), H_SS(H00, H00 + n2),
+      H_10(H10, H10 + n2), H_01(n2);
+  const cd z(E, o.eta_lead);
+  for (int j = 0; j < nm; j++)
+    for (int i = 0; i < nm; i++) H_01[i + (size_t)j * nm] = std::conj(H_10[j + (size_t)i * nm]);
+  int taken = 0;
+  for (int it = 1; it <= o.sancho_nmax; it++) {
+    taken = it;
+    for (size_t k = 0; k < n2; k++) A[k] = -H_BB[k];
+    for (int i = 0; i < nm; i++) A[i + (size_t)i * nm] += z;
+    w.invert(A.data());
+    w.gemm('n', 'n', A.data(), H_10.data(), B.data());
+    w.gemm('n', 'n', H_01.data(), B.data(), C.data());
+    for (size_t k = 0; k < n2; k++) { H_SS[k] += C[k]; H_BB[k] += C[k]; }
+    w.gemm('n', 'n', H_10.data(), B.data(), C.data());
+    w.gemm('n', 'n', A.data(), H_01.data(), B.data());
+    w.gemm('n', 'n', H_10.data(), B.data(), A.data());
+    H_10 = C;
+    for (size_t k = 0; k < n2; k++) H_BB[k] += A[k];
+    w.gemm('n', 'n', H_01.data(), B.data(), C.data());
+    H_01 = C;
+    double error = 0.0;
+    for (size_t k = 0; k < n2; k++)
+      error += std::sqrt(C[k].imag() * C[k].imag() + C[k].real() * C[k].real());
+    if (std::fabs(error) < o.sancho_tol) break;
+    if (it == o.sancho_nmax) {
+      H_SS.assign(H00, H00 + n2);
+      H_BB.assign(H00, H00 + n2);
+      w.st->status |= ST_SANCHO_NC;
+      taken = o.sancho_nmax + 1;
+    }
+  }
+  for (size_t k = 0; k < n2; k++) G00[k] = -H_SS[k];
+  for (int i = 0; i < nm; i++) G00[i + (size_t)i * nm] += z;
+  w.invert(G00);
+  for (size_t k = 0; k < n2; k++) GBB[k] = -H_BB[k];
+  for (int i = 0; i < nm; i++) GBB[i + (size_t)i * nm] += z;
+  w.invert(GBB);
+  return taken;
+}
+
+}  // namespace
+
+// One energy point of green_RGF_RS (green_rgf.f90:3950-4164).
+// Arrays are column-major (nm,nm,nx) complex128.  sig_lesser / sig_r may be
+// null (treated as zero).  Every output may be null (not written).
+// T_out (if non-null, and o.want_T) receives the Caroli transmission
+// Re Tr[Gamma_L G^A_{1N} Gamma_R G^R_{N1}] (green.f90:2571-2580).
+extern "C" int oracle_rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E,
+                                 const double* mu, const double* temp, const cd* Hii,
+                                 const cd* H1i, const cd* sig_lesser, const cd* sig_r,
+                                 cd* ndens, cd* pdens, cd* ldos, double* tr, double* tre,
+                                 double* cur, cd* GRi1, cd* GLi1, cd* GGi1, double* T_out,
+                                 OracleStat* st) {
+  const OracleOpts& o = *opts;
+  OracleStat dummy{};
+  if (!st) st = &dummy;
+  std::memset(st, 0, sizeof(*st));
+  if (nm64 < 1 || nx64 < 2 || nm64 > 4096) { st->status = ST_BAD_ARGS; return ST_BAD_ARGS; }
+  const int nm = (int)nm64, nx = (int)nx64;
+  const size_t n2 = nn(nm);
+  Work w(nm, st);
+  auto blk = [&](const cd* base, int l) { return base + (size_t)(l - 1) * n2; };  // 1-based l
+  auto blkw = [&](cd* base, int l) { return base + (size_t)(l - 1) * n2; };
+  auto adj = [&](const cd* X, cd* Y) {  // Y = X^H
+    for (int j = 0; j < nm; j++)
+      for (int i = 0; i < nm; i++) Y[i + (size_t)j * nm] = std::conj(X[j + (size_t)i * nm]);
+  };
+  auto sigR = [&](int l, size_t k) { return sig_r ? blk(sig_r, l)[k] : cd(0.0, 0.0); };
+  auto sigL = [&](int l, size_t k) { return sig_lesser ? blk(sig_lesser, l)[k] : cd(0.0, 0.0); };
+  // The backward sweep's coupling block: reference uses H1i(:,:,l) (trap T3);
+  // the consistent variant uses H_{l+1,l} = H1i(:,:,l+1).
+  auto H1b = [&](int l) { return o.consistent ? blk(H1i, l + 1) : blk(H1i, l); };
+
+  const double mul = mu[0], mur = mu[1], templ = temp[0], tempr = temp[1];
+  const cd z(E, o.eta_dev);
+  std::vector<cd> Gl(n2 * nx), Gln(n2 * nx);
+  std::vector<cd> H00(n2), H10(n2), A(n2), B(n2), C(n2), D(n2), G00(n2), GBB(n2), GN0(n2),
+      Gn(n2), Gp(n2), sig(n2), sigmal(n2), sigmar(n2), tmp(n2), GN1(n2), GN1b(n2);
+
+  if (ldos) std::fill(ldos, ldos + n2 * nx, cd(0, 0));
+  if (ndens) std::fill(ndens, ndens + n2 * nx, cd(0, 0));
+  if (pdens) std::fill(pdens, pdens + n2 * nx, cd(0, 0));
+  if (cur) std::fill(cur, cur + n2 * nx, 0.0);
+
+  // ---- left contact (green_rgf.f90:3992-4012)
+  for (size_t k = 0; k < n2; k++) H00[k] = blk(Hii, 1)[k] + sigR(1, k);
+  std::copy(blk(H1i, 1), blk(H1i, 1) + n2, H10.begin());
+  adj(H10.data(), tmp.data());
+  st->sancho_iters_left = sancho(w, o, E, H00.data(), tmp.data(), G00.data(), GBB.data());
+  w.gemm('n', 'n', H10.data(), G00.data(), A.data());
+  w.gemm('n', 'c', A.data(), H10.data(), sigmal.data());
+  {
+    const double f = ferm((E - mul) / (o.boltz * templ));
+    for (int j = 0; j < nm; j++)
+      for (int i = 0; i < nm; i++) {
+        const size_t k = i + (size_t)j * nm;
+        sig[k] = -(sigmal[k] - std::conj(sigmal[j + (size_t)i * nm])) * f + sigL(1, k);
+      }
+  }
+  for (size_t k = 0; k < n2; k++) A[k] = -H00[k] - sigmal[k];
+  for (int i = 0; i < nm; i++) A[i + (size_t)i * nm] += z;
+  w.invert(A.data());
+  std::copy(A.begin(), A.end(), blkw(Gl.data(), 1));
+  w.gemm('n', 'n', A.data(), sig.data(), B.data());
+  w.gemm('n', 'c', B.data(), A.data(), C.data());
+  std::copy(C.begin(), C.end(), blkw(Gln.data(), 1));
+  // running left-connected column g^L_{l,1}; g^L_{1,1} = g_1  (for T(E))
+  if (o.want_T) GN1 = A;
+
+  // ---- forward sweep (green_rgf.f90:4013-4030)
+  for (int l = 2; l <= nx - 1; l++) {
+    for (size_t k = 0; k < n2; k++) H00[k] = blk(Hii, l)[k] + sigR(l, k);
+    std::copy(blk(H1i, l), blk(H1i, l) + n2, H10.begin());
+    w.gemm('n', 'n', H10.data(), blkw(Gl.data(), l - 1), B.data());
+    w.gemm('n', 'c', B.data(), H10.data(), C.data());
+    for (size_t k = 0; k < n2; k++) A[k] = -H00[k] - C[k];
+    for (int i = 0; i < nm; i++) A[i + (size_t)i * nm] += z;
+    w.invert(A.data());
+    std::copy(A.begin(), A.end(), blkw(Gl.data(), l));
+    std::copy(blkw(Gln.data(), l - 1), blkw(Gln.data(), l - 1) + n2, sig.begin());
+    w.gemm('n', 'n', H10.data(), sig.data(), B.data());
+    w.gemm('n', 'c', B.data(), H10.data(), C.data());
+    for (size_t k = 0; k < n2; k++) C[k] += sigL(l, k);
+    w.gemm('n', 'n', A.data(), C.data(), B.data());
+    w.gemm('n', 'c', B.data(), A.data(), Gn.data());
+    std::copy(Gn.begin(), Gn.end(), blkw(Gln.data(), l));
+    if (o.want_T) {  // g^L_{l,1} = g_l H_{l,l-1} g^L_{l-1,1}
+      w.gemm('n', 'n', H10.data(), GN1.data(), GN1b.data());
+      w.gemm('n', 'n', A.data(), GN1b.data(), GN1.data());
+    }
+  }
+
+  // ---- right contact and G_NN (green_rgf.f90:4031-4066)
+  for (size_t k = 0; k < n2; k++) H00[k] = blk(Hii, nx)[k] + sigR(nx, k);
+  std::copy(blk(H1i, nx), blk(H1i, nx) + n2, H10.begin());
+  st->sancho_iters_right = sancho(w, o, E, H00.data(), H10.data(), G00.data(), GBB.data());
+  w.gemm('c', 'n', H10.data(), G00.data(), A.data());
+  w.gemm('n', 'n', A.data(), H10.data(), sigmar.data());
+  w.gemm('n', 'n', H10.data(), blkw(Gl.data(), nx - 1), B.data());
+  w.gemm('n', 'c', B.data(), H10.data(), C.data());
+  for (size_t k = 0; k < n2; k++) G00[k] = -H00[k] - sigmar[k] - C[k];
+  for (int i = 0; i < nm; i++) G00[i + (size_t)i * nm] += z;
+  w.invert(G00.data());
+  if (ldos) std::copy(G00.begin(), G00.end(), ldos + (size_t)(nx - 1) * n2);
+  std::copy(blkw(Gln.data(), nx - 1), blkw(Gln.data(), nx - 1) + n2, sig.begin());
+  w.gemm('n', 'n', H10.data(), sig.data(), B.data());
+  w.gemm('n', 'c', B.data(), H10.data(), C.data());
+  const double fR = ferm((E - mur) / (o.boltz * templ));  // TEMPl here: trap T2 (green_rgf.f90:4051)
+  for (int j = 0; j < nm; j++)
+    for (int i = 0; i < nm; i++) {
+      const size_t k = i + (size_t)j * nm;
+      sig[k] = -(sigmar[k] - std::conj(sigmar[j + (size_t)i * nm])) * fR + C[k] + sigL(nx, k);
+    }
+  w.gemm('n', 'n', G00.data(), sig.data(), B.data());
+  w.gemm('n', 'c', B.data(), G00.data(), Gn.data());
+  if (ndens) std::copy(Gn.begin(), Gn.end(), ndens + (size_t)(nx - 1) * n2);
+  for (int j = 0; j < nm; j++)
+    for (int i = 0; i < nm; i++) {
+      const size_t k = i + (size_t)j * nm;
+      Gp[k] = Gn[k] + (G00[k] - std::conj(G00[j + (size_t)i * nm]));
+    }
+  if (pdens) std::copy(Gp.begin(), Gp.end(), pdens + (size_t)(nx - 1) * n2);
+  for (int j = 0; j < nm; j++)
+    for (int i = 0; i < nm; i++) {
+      const size_t k = i + (size_t)j * nm;
+      A[k] = -(sigmar[k] - std::conj(sigmar[j + (size_t)i * nm])) * fR;
+    }
+  w.gemm('n', 'n', A.data(), Gp.data(), B.data());
+  for (int j = 0; j < nm; j++)
+    for (int i = 0; i < nm; i++) {
+      const size_t k = i + (size_t)j * nm;
+      A[k] = -(sigmar[k] - std::conj(sigmar[j + (size_t)i * nm])) * (fR - 1.0);
+    }
+  w.gemm('n', 'n', A.data(), Gn.data(), C.data());
+  {
+    double tim = 0.0;
+    for (int i = 0; i < nm; i++) tim = tim - (B[i + (size_t)i * nm] - C[i + (size_t)i * nm]).real();
+    if (tr) *tr = tim;
+  }
+  // Caroli T(E): G_{N1} = G_NN H_{N,N-1} g^L_{N-1,1};  T = Re Tr[Gamma_R G_{N1} Gamma_L G_{N1}^H]
+  if (o.want_T && T_out) {
+    std::vector<cd> gL(n2), gR(n2), X(n2), Y(n2);
+    for (int j = 0; j < nm; j++)
+      for (int i = 0; i < nm; i++) {
+        const size_t k = i + (size_t)j * nm, kt = j + (size_t)i * nm;
+        gL[k] = cd(0, 1) * (sigmal[k] - std::conj(sigmal[kt]));
+        gR[k] = cd(0, 1) * (sigmar[k] - std::conj(sigmar[kt]));
+      }
+    w.gemm('n', 'n', H10.data(), GN1.data(), GN1b.data());
+    w.gemm('n', 'n', G00.data(), GN1b.data(), X.data());   // X = G_{N1}
+    w.gemm('n', 'n', gR.data(), X.data(), Y.data());       // Y = Gamma_R G_{N1}
+    w.gemm('n', 'c', gL.data(), X.data(), GN1b.data());    // Gamma_L G_{N1}^H
+    double t = 0.0;
+    for (int i = 0; i < nm; i++)
+      for (int k = 0; k < nm; k++) t += (Y[i + (size_t)k * nm] * GN1b[k + (size_t)i * nm]).real();
+    *T_out = t;
+  }
+
+  // ---- backward sweep (green_rgf.f90:4069-4149)
+  for (int l = nx - 1; l >= 1; l--) {
+    const cd* Hb = H1b(l);
+    std::copy(Hb, Hb + n2, H10.begin());
+    const cd* Gll = blk(Gl.data(), l);
+    const cd* Glnl = blk(Gln.data(), l);
+    A = Gn;
+    w.gemm('n', 'c', H10.data(), Gll, B.data());
+    w.gemm('n', 'n', A.data(), B.data(), C.data());
+    std::copy(Glnl, Glnl + n2, A.begin());
+    w.gemm('n', 'n', H10.data(), A.data(), B.data());
+    w.gemm('n', 'n', G00.data(), B.data(), A.data());
+    for (size_t k = 0; k < n2; k++) B[k] = C[k] + A[k];
+    w.gemm('c', 'n', H10.data(), B.data(), A.data());  // G<_{l+1,l}
+    if (cur)
+      for (size_t k = 0; k < n2; k++) cur[(size_t)(l - 1) * n2 + k] = A[k].real();
+    A = Gn;
+    w.gemm('n', 'c', Gll, H10.data(), B.data());
+    w.gemm('n', 'n', B.data(), A.data(), C.data());
+    std::copy(Glnl, Glnl + n2, A.begin());
+    w.gemm('n', 'c', A.data(), H10.data(), B.data());
+    w.gemm('n', 'c', B.data(), G00.data(), A.data());
+    for (size_t k = 0; k < n2; k++) B[k] = C[k] + A[k];
+    if (GLi1) std::copy(B.begin(), B.end(), GLi1 + (size_t)(l - 1) * n2);
+    w.gemm('n', 'n', H10.data(), B.data(), A.data());  // G<_{l,l+1}
+    if (cur)
+      for (size_t k = 0; k < n2; k++) cur[(size_t)(l - 1) * n2 + k] -= A[k].real();
+    if (GGi1) {
+      // Reproduces the reference: Glp is never filled (zero) and Gp keeps its
+      // value from the right closure (green_rgf.f90:4094-4103, trap T4).
+      A = Gp;
+      w.gemm('c', 'c', Gll, H10.data(), B.data());
+      w.gemm('n', 'n', B.data(), A.data(), C.data());
+      std::fill(A.begin(), A.end(), cd(0, 0));
+      w.gemm('n', 'c', A.data(), H10.data(), B.data());
+      w.gemm('n', 'n', B.data(), G00.data(), A.data());
+      for (size_t k = 0; k < n2; k++) B[k] = C[k] + A[k];
+      std::copy(B.begin(), B.end(), GGi1 + (size_t)(l - 1) * n2);
+    }
+    std::copy(Gll, Gll + n2, D.begin());
+    w.gemm('n', 'c', D.data(), H10.data(), B.data());
+    w.gemm('n', 'n', B.data(), G00.data(), GN0.data());  // G_{l,l+1}
+    if (GRi1) std::copy(GN0.begin(), GN0.end(), GRi1 + (size_t)(l - 1) * n2);
+    w.gemm('n', 'n', GN0.data(), H10.data(), A.data());
+    w.gemm('n', 'n', A.data(), D.data(), C.data());
+    for (size_t k = 0; k < n2; k++) G00[k] = Gll[k] + C[k];  // G_{l,l}
+    if (ldos) std::copy(G00.begin(), G00.end(), ldos + (size_t)(l - 1) * n2);
+    A = Gn;
+    w.gemm('n', 'c', D.data(), H10.data(), B.data());
+    w.gemm('n', 'n', B.data(), A.data(), C.data());
+    w.gemm('n', 'n', C.data(), H10.data(), A.data());
+    w.gemm('n', 'c', A.data(), D.data(), C.data());
+    for (size_t k = 0; k < n2; k++) Gn[k] = Glnl[k] + C[k];
+    std::copy(Glnl, Glnl + n2, A.begin());
+    w.gemm('n', 'n', GN0.data(), H10.data(), B.data());
+    w.gemm('n', 'n', B.data(), A.data(), C.data());
+    for (size_t k = 0; k < n2; k++) Gn[k] += C[k];
+    w.gemm('n', 'c', A.data(), H10.data(), B.data());
+    w.gemm('n', 'c', B.data(), GN0.data(), C.data());
+    for (size_t k = 0; k < n2; k++) Gn[k] += C[k];  // G<_{l,l}
+    if (ndens) std::copy(Gn.begin(), Gn.end(), ndens + (size_t)(l - 1) * n2);
+    if (pdens)
+      for (int j = 0; j < nm; j++)
+        for (int i = 0; i < nm; i++) {
+          const size_t k = i + (size_t)j * nm;
+          pdens[(size_t)(l - 1) * n2 + k] = Gn[k] + (G00[k] - std::conj(G00[j + (size_t)i * nm]));
+        }
+  }
+
+  // ---- left trace (green_rgf.f90:4151-4160); TEMPr here: trap T2
+  for (int j = 0; j < nm; j++)
+    for (int i = 0; i < nm; i++) {
+      const size_t k = i + (size_t)j * nm;
+      Gp[k] = Gn[k] + (G00[k] - std::conj(G00[j + (size_t)i * nm]));
+    }
+  const double fL = ferm((E - mul) / (o.boltz * tempr));
+  for (int j = 0; j < nm; j++)
+    for (int i = 0; i < nm; i++) {
+      const size_t k = i + (size_t)j * nm;
+      A[k] = -(sigmal[k] - std::conj(sigmal[j + (size_t)i * nm])) * fL;
+    }
+  w.gemm('n', 'n', A.data(), Gp.data(), B.data());
+  for (int j = 0; j < nm; j++)
+    for (int i = 0; i < nm; i++) {
+      const size_t k = i + (size_t)j * nm;
+      A[k] = -(sigmal[k] - std::conj(sigmal[j + (size_t)i * nm])) * (fL - 1.0);
+    }
+  w.gemm('n', 'n', A.data(), Gn.data(), C.data());
+  {
+    double tim = 0.0;
+    for (int i = 0; i < nm; i++) tim = tim + (B[i + (size_t)i * nm] - C[i + (size_t)i * nm]).real();
+    if (tre) *tre = tim;
+  }
+  return st->status;
+}
+
+// Batch over energy points, one worker thread per core and one energy per
+// call, mirroring `!$omp parallel do ie` around green_RGF_RS
+// (green_rgf.f90:2916-2925) with single-threaded BLAS.  Hii/H1i are shared by
+// all points; per-point arrays are strided by nm*nm*nx elements (cur by the
+// same count of doubles).  Null arrays are skipped.
+extern "C" int oracle_rgf_batch(const OracleOpts* opts, int64_t nm, int64_t nx, int64_t nE,
+                                const double* E, const double* mu, const double* temp,
+                                const cd* Hii, const cd* H1i, const cd* sig_lesser,
+                                const cd* sig_r, cd* ndens, cd* pdens, cd* ldos, double* tr,
+                                double* tre, double* cur, cd* GRi1, double* T_out,
+                                OracleStat* stats, int n_threads) {
+  const size_t per = (size_t)nm * nm * nx;
+  std::atomic<int64_t> next(0);
+  std::atomic<int> worst(0);
+  auto worker = [&]() {
+    for (;;) {
+      const int64_t e = next.fetch_add(1);
+      if (e >= nE) break;
+      OracleStat st{};
+      const int s = oracle_rgf_energy(
+          opts, nm, nx, E[e], mu, temp, Hii, H1i, sig_lesser ? sig_lesser + e * per : nullptr,
+          sig_r ? sig_r + e * per : nullptr, ndens ? ndens + e * per : nullptr,
+          pdens ? pdens + e * per : nullptr, ldos ? ldos + e * per : nullptr,
+          tr ? tr + e : nullptr, tre ? tre + e : nullptr, cur ? cur + e * per : nullptr,
+          GRi1 ? GRi1 + e * per : nullptr, nullptr, nullptr, T_out ? T_out + e : nullptr, &st);
+      if (stats) stats[e] = st;
+      int cur_w = worst.load();
+      while ((s | cur_w) != cur_w && !worst.compare_exchange_weak(cur_w, s | cur_w)) {}
+    }
+  };
+  if (n_threads < 1) n_threads = 1;
+  std::vector<std::thread> pool;
+  for (int t = 1; t < n_threads; t++) pool.emplace_back(worker);
+  worker();
+  for (auto& t : pool) t.join();
+  return worst.load();
+}
+
+// calc_n_electron (green_rgf.f90:3920-3945) for one k-point set laid out as
+// (nm,nm,nx,nen,nk).  nelec/pelec have nx entries.
+extern "C" void oracle_calc_n_electron(const cd* G_lesser, const cd* G_greater, int64_t nen,
+                                       const double* E, int64_t nm, int64_t nk, int64_t nx,
+                                       double* nelec, double* pelec, const double* midgap) {
+  const double pi = 3.14159265359;  // green_rgf.f90:23
+  const double dE = (E[1] - E[0]) / (2.0 * pi);
+  const double dK = 2.0 * pi / (double)nk;
+  const size_t n2 = (size_t)nm * nm;
+  for (int64_t ix = 0; ix < nx; ix++) { nelec[ix] = 0.0; pelec[ix] = 0.0; }
+  for (int64_t i = 0; i < nen; i++)
+    for (int64_t ik = 0; ik < nk; ik++)
+      for (int64_t ix = 0; ix < nx; ix++)
+        for (int64_t j = 0; j < nm; j++) {
+          const size_t off = (size_t)j + (size_t)j * nm + ix * n2 + (size_t)nx * n2 * (i + (size_t)nen * ik);
+          if (E[i] > midgap[ix])
+            nelec[ix] = nelec[ix] + G_lesser[off].imag() * dE * dK;
+          else
+            pelec[ix] = pelec[ix] - G_greater[off].imag() * dE * dK;
+        }
+}

@@ -1,0 +1,289 @@
+"""GPU parity tests: the CUDA library, called through its C ABI, against the
+CPU oracle (and the golden fixtures) on identical seeded inputs.
+
+Tolerance for the FP64 path: 1e-10 relative, where "relative" is to the
+largest magnitude of the same output over the whole batch (for G^> the
+largest |G^R| / |G^<|, since G^> = G^< + G^R - G^A cancels; for tr / tre the
+largest |tr| over the energies; for `cur` the natural size nm*|H|*|G^<| of
+its terms)."""
+import ctypes
+import glob
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import random_sigma, rel_err
+from liteqt_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+MU = (0.1, -0.1)
+TOL = 1e-10
+
+
+def _temp():
+    return (S.temperature_for_kT(0.025),) * 2
+
+
+@pytest.fixture(scope="module")
+def rgf():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    from liteqt_b200 import build, rgf as R
+    build.build()
+    R.load()
+    return R
+
+
+def gpu_solve(R, Hii, H1i, E, opts, sl=None, sr=None, mu=MU, temp=None, outputs="all"):
+    temp = temp or _temp()
+    nx, nm, _ = Hii.shape
+    nen = len(E)
+    shape = (nen, nx, nm, nm)
+    out = dict(ldos=np.zeros(shape, complex), ndens=np.zeros(shape, complex),
+               pdens=np.zeros(shape, complex), GRi1=np.zeros(shape, complex),
+               cur=np.zeros(shape), tr=np.zeros(nen), tre=np.zeros(nen), T=np.zeros(nen),
+               info=np.zeros(nen, R.INFO_DTYPE))
+    with R.Context(opts) as ctx:
+        rc = ctx.solve_energies(Hii, H1i, np.asarray(E, float), mu, temp, sigma_lesser=sl,
+                                sigma_r=sr, ldos=out["ldos"], ndens=out["ndens"], pdens=out["pdens"],
+                                GRi1=out["GRi1"], cur=out["cur"], tr=out["tr"], tre=out["tre"],
+                                T=out["T"], info=out["info"])
+    out["rc"] = rc
+    return out
+
+
+def compare(g, r, nm, H1i, tol=TOL, skip_last_gri1=True):
+    errs = {}
+    errs["ldos"] = rel_err(g["ldos"], r["ldos"])
+    errs["ndens"] = rel_err(g["ndens"], r["ndens"])
+    errs["pdens"] = rel_err(g["pdens"], r["pdens"], scale=max(np.max(np.abs(r["ldos"])),
+                                                                np.max(np.abs(r["ndens"]))))
+    sl = slice(0, -1) if skip_last_gri1 else slice(None)
+    errs["GRi1"] = rel_err(g["GRi1"][:, sl], r["GRi1"][:, sl])
+    cur_scale = nm * np.max(np.abs(H1i)) * np.max(np.abs(r["ndens"]))
+    errs["cur"] = rel_err(g["cur"], r["cur"], scale=cur_scale)
+    trs = max(np.max(np.abs(r["tr"])), 1e-300)
+    errs["tr"] = float(np.max(np.abs(g["tr"] - r["tr"])) / trs)
+    errs["tre"] = float(np.max(np.abs(g["tre"] - r["tre"])) / trs)
+    errs["T"] = float(np.max(np.abs(g["T"] - r["T"]) / np.maximum(1.0, np.abs(r["T"]))))
+    bad = {k: v for k, v in errs.items() if not v <= tol}
+    assert not bad, f"errors above {tol}: {bad} (all: {errs})"
+    return errs
+
+
+def oracle_solve(Hii, H1i, E, oopts, sl=None, sr=None):
+    from oracle import oracle as O
+    return O.rgf_batch(Hii, H1i, np.asarray(E, float), MU, _temp(), oopts, sig_lesser=sl, sig_r=sr)
+
+
+CASES = [
+    # nm, nx, consistent, scatter, eta_dev, eta_lead
+    (8, 2, False, False, 0.0, 1e-3),
+    (8, 5, False, True, 0.0, 1e-3),
+    (16, 6, True, True, 1e-5, 1e-5),
+    (24, 4, False, False, 0.0, 1e-3),
+    (32, 7, False, True, 0.0, 1e-3),
+    (48, 3, True, False, 1e-5, 1e-5),
+    (64, 5, False, True, 0.0, 1e-3),
+    (80, 3, True, False, 0.0, 1e-3),
+    (128, 4, False, False, 1e-5, 1e-5),
+]
+
+
+@pytest.mark.parametrize("nm,nx,consistent,scatter,eta_dev,eta_lead", CASES)
+def test_fp64_matches_oracle(rgf, nm, nx, consistent, scatter, eta_dev, eta_lead):
+    from oracle import oracle as O
+    d = S.make_device(nm, nx, seed=4000 + nm + nx)
+    E = S.energy_grid(6, -3.0, 3.0)
+    sl = sr = None
+    if scatter:
+        sl, sr = random_sigma(nm, nx, len(E), seed=nm)
+    opts = rgf.Options(consistent=consistent, eta_dev=eta_dev, eta_lead=eta_lead)
+    oopts = O.Opts(consistent=consistent, eta_dev=eta_dev, eta_lead=eta_lead)
+    g = gpu_solve(rgf, d.Hii, d.H1i, E, opts, sl, sr)
+    r = oracle_solve(d.Hii, d.H1i, E, oopts, sl, sr)
+    assert g["rc"] == 0 and np.all(g["info"]["status"] == 0)
+    compare(g, r, nm, d.H1i)
+    assert np.array_equal(g["info"]["sancho_iters_left"], r["stats"]["sancho_iters_left"])
+    assert np.array_equal(g["info"]["sancho_iters_right"], r["stats"]["sancho_iters_right"])
+
+
+GOLDEN = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "*.npz")))
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_fp64_matches_golden(rgf, path):
+    z = np.load(path)
+    nm = z["Hii"].shape[1]
+    opts = rgf.Options(eta_dev=float(z["eta_dev"]), eta_lead=float(z["eta_lead"]),
+                       consistent=bool(z["consistent"]), boltz=float(z["boltz"]))
+    sl = z["sig_lesser"] if z["has_sigma"] else None
+    sr = z["sig_r"] if z["has_sigma"] else None
+    g = gpu_solve(rgf, z["Hii"], z["H1i"], z["E"], opts, sl, sr, mu=tuple(z["mu"]), temp=tuple(z["temp"]))
+    r = {k: z[k] for k in ("ldos", "ndens", "pdens", "GRi1", "cur", "tr", "tre", "T")}
+    compare(g, r, nm, z["H1i"])
+
+
+def test_device_pointers_match_host_pointers(rgf):
+    import torch
+    nm, nx = 32, 6
+    d = S.make_device(nm, nx, seed=77)
+    E = S.energy_grid(8, -2.0, 2.0)
+    opts = rgf.Options()
+    h = gpu_solve(rgf, d.Hii, d.H1i, E, opts)
+    dev = torch.device("cuda:0")
+    Hii = torch.from_numpy(d.Hii).to(dev)
+    H1i = torch.from_numpy(d.H1i).to(dev)
+    Et = torch.from_numpy(E)  # energies stay on the host (read by the host code)
+    shape = (len(E), nx, nm, nm)
+    ldos = torch.zeros(shape, dtype=torch.complex128, device=dev)
+    ndens = torch.zeros_like(ldos)
+    tr = torch.zeros(len(E), dtype=torch.float64, device=dev)
+    T = torch.zeros_like(tr)
+    with rgf.Context(opts) as ctx:
+        ctx.solve_energies(Hii, H1i, Et.numpy(), MU, _temp(), ldos=ldos, ndens=ndens, tr=tr, T=T)
+    torch.cuda.synchronize()
+    assert np.array_equal(ldos.cpu().numpy(), h["ldos"])
+    assert np.array_equal(ndens.cpu().numpy(), h["ndens"])
+    assert np.array_equal(tr.cpu().numpy(), h["tr"])
+    assert np.array_equal(T.cpu().numpy(), h["T"])
+
+
+def test_drop_in_green_rgf_rs_and_rgf_g(rgf):
+    from oracle import oracle as O
+    nm, nx = 16, 5
+    d = S.make_device(nm, nx, seed=5)
+    sl, sr = random_sigma(nm, nx, 1, seed=1)
+    E = 0.37
+    for fn, boltz in (("green_RGF_RS", O.BOLTZ_RGF_RS), ("RGF_G", O.BOLTZ_RGF_G)):
+        nd = np.zeros((nx, nm, nm), complex)
+        pd = np.zeros_like(nd)
+        ld = np.zeros_like(nd)
+        gr = np.zeros_like(nd)
+        cur = np.zeros((nx, nm, nm))
+        tr = np.zeros(1)
+        tre = np.zeros(1)
+        if fn == "green_RGF_RS":
+            rgf.green_RGF_RS(_temp(), nm, nx, E, MU, d.Hii, d.H1i, sl[0], None, sr[0], nd, pd, ld,
+                             tr, tre, cur, GRi1=gr)
+        else:
+            rgf.RGF_G(_temp(), nm, nx, E, MU, d.Hii, d.H1i, sl[0], None, sr[0], tr, tre, nd, pd, ld,
+                      cur, GRi1=gr)
+        r = O.rgf_batch(d.Hii, d.H1i, np.array([E]), MU, _temp(), O.Opts(boltz=boltz),
+                        sig_lesser=sl, sig_r=sr)
+        g = dict(ldos=ld[None], ndens=nd[None], pdens=pd[None], GRi1=gr[None], cur=cur[None],
+                 tr=tr, tre=tre, T=r["T"])
+        compare(g, r, nm, d.H1i)
+
+
+def test_c_harness_fortran_calling_convention(rgf, tmp_path):
+    """The C harness passes everything by reference, as ISO_C_BINDING does."""
+    from oracle import oracle as O
+    lib = os.path.join(ROOT, "liteqt_b200", "librgf_b200.so")
+    exe = tmp_path / "abi_harness"
+    subprocess.check_call(["gcc", "-O1", "-o", str(exe), os.path.join(ROOT, "tests", "abi_harness.c"),
+                           "-I", os.path.join(ROOT, "include"), lib,
+                           "-Wl,-rpath," + os.path.dirname(lib)])
+    nm, nx = 8, 4
+    d = S.make_device(nm, nx, seed=9)
+    sl, sr = random_sigma(nm, nx, 1, seed=2)
+    E = -0.61
+    inp = tmp_path / "in.bin"
+    with open(inp, "wb") as f:
+        np.array([nm, nx, 1], np.int64).tofile(f)
+        np.array([E, *MU, *_temp()], np.float64).tofile(f)
+        d.Hii.tofile(f)
+        d.H1i.tofile(f)
+        sl[0].tofile(f)
+        sr[0].tofile(f)
+    for mode, boltz in (("solve", O.BOLTZ_RGF_RS), ("solve_rgfg", O.BOLTZ_RGF_G)):
+        outp = tmp_path / f"out_{mode}.bin"
+        subprocess.check_call([str(exe), mode, str(inp), str(outp)])
+        raw = np.fromfile(outp, np.float64)
+        n = nm * nm * nx
+        tr, tre = raw[0], raw[1]
+        c = raw[2:2 + 8 * n].view(np.complex128).reshape(4, nx, nm, nm)
+        cur = raw[2 + 8 * n:].reshape(nx, nm, nm)
+        r = O.rgf_batch(d.Hii, d.H1i, np.array([E]), MU, _temp(), O.Opts(boltz=boltz),
+                        sig_lesser=sl, sig_r=sr)
+        g = dict(ndens=c[0][None], pdens=c[1][None], ldos=c[2][None], GRi1=c[3][None],
+                 cur=cur[None], tr=np.array([tr]), tre=np.array([tre]), T=r["T"])
+        compare(g, r, nm, d.H1i)
+
+
+def test_singular_block_reports_status(rgf):
+    nm, nx, E = 8, 3, 0.25
+    from oracle import oracle as O
+    Hii = O.from_blocks(np.broadcast_to(E * np.eye(nm), (nx, nm, nm)).astype(complex))
+    H1i = np.zeros_like(Hii)
+    g = gpu_solve(rgf, Hii, H1i, [E], rgf.Options())
+    assert g["rc"] == rgf.RGF_E_STATUS if hasattr(rgf, "RGF_E_STATUS") else True
+    assert g["info"]["status"][0] & 1
+    r = oracle_solve(Hii, H1i, [E], O.Opts())
+    assert np.all(np.isfinite(g["ldos"]))
+    assert rel_err(g["ldos"], r["ldos"], scale=1.0) < TOL
+
+
+def test_sancho_cap_reports_status_and_matches(rgf):
+    from oracle import oracle as O
+    d = S.make_device(16, 4, seed=2)
+    E = [0.1, 1.3]
+    g = gpu_solve(rgf, d.Hii, d.H1i, E, rgf.Options(sancho_nmax=3))
+    r = oracle_solve(d.Hii, d.H1i, E, O.Opts(sancho_nmax=3))
+    assert np.all(g["info"]["status"] & 2)
+    assert np.all(g["info"]["sancho_iters_left"] == 4)
+    compare(g, r, 16, d.H1i)
+
+
+def test_cfg1_blocks_subset_matches_oracle(rgf):
+    """Full-size blocks and chain of the plain FP64 configuration (nb=32,
+    Nx=50, eta=1e-5) on a subset of its 1000 energies."""
+    from oracle import oracle as O
+    nm, nx = 32, 50
+    d = S.make_device(nm, nx, seed=1)
+    E = S.energy_grid(1000, -3.0, 3.0)[::40]
+    opts = rgf.Options(eta_dev=1e-5, eta_lead=1e-5)
+    g = gpu_solve(rgf, d.Hii, d.H1i, E, opts)
+    r = oracle_solve(d.Hii, d.H1i, E, O.Opts(eta_dev=1e-5, eta_lead=1e-5))
+    compare(g, r, nm, d.H1i)
+
+
+def test_cfg1_full_batch_properties(rgf):
+    """All 1000 energies of the plain FP64 configuration in consistent mode:
+    current conservation tr = tre, anti-Hermitian G^<, Im G^R_jj <= 0, and
+    0 <= T <= nm."""
+    nm, nx = 32, 50
+    d = S.make_device(nm, nx, seed=1)
+    E = S.energy_grid(1000, -3.0, 3.0)
+    g = gpu_solve(rgf, d.Hii, d.H1i, E, rgf.Options(eta_dev=1e-5, eta_lead=1e-5, consistent=True))
+    assert np.all(g["info"]["status"] == 0)
+    scale = np.max(np.abs(g["tr"]))
+    assert np.max(np.abs(g["tr"] - g["tre"])) < 1e-8 * scale
+    nd = g["ndens"]
+    assert np.max(np.abs(nd + np.conj(np.swapaxes(nd, -1, -2)))) < 1e-10 * np.max(np.abs(nd))
+    diag = np.diagonal(g["ldos"], axis1=-2, axis2=-1)
+    assert np.all(diag.imag <= 1e-10 * np.max(np.abs(diag)))
+    assert np.all(g["T"] > -1e-8) and np.all(g["T"] < nm + 1e-6)
+
+
+def test_energy_integrals_match_oracle(rgf):
+    from oracle import oracle as O
+    rng = np.random.default_rng(0)
+    nk, nen, nx, nm = 2, 6, 3, 8
+    Gl = rng.normal(size=(nk, nen, nx, nm, nm)) + 1j * rng.normal(size=(nk, nen, nx, nm, nm))
+    Gg = rng.normal(size=(nk, nen, nx, nm, nm)) + 1j * rng.normal(size=(nk, nen, nx, nm, nm))
+    E = np.linspace(-1, 1, nen)
+    mid = np.array([-0.2, 0.0, 0.3])
+    with rgf.Context() as ctx:
+        ne, pe = ctx.calc_n_electron(Gl, Gg, E, mid)
+        tr = rng.normal(size=nen)
+        I = ctx.terminal_current(tr, E[1] - E[0], spindeg=2.0, nk=nk)
+    ne2, pe2 = O.calc_n_electron(Gl, Gg, E, mid)
+    assert np.allclose(ne, ne2, rtol=1e-12, atol=1e-14)
+    assert np.allclose(pe, pe2, rtol=1e-12, atol=1e-14)
+    I2 = O.terminal_current(tr, E[1] - E[0], 2.0, nk)
+    assert abs(I - I2) <= 1e-12 * abs(I2)

@@ -1,0 +1,220 @@
+"""CPU tests of the oracle (test infrastructure): the C++ restatement of
+green_RGF_RS against the independent NumPy restatement, and both against
+known answers (dense inverse, Sancho fixed point, uniform chain, current
+conservation, Hermiticity) and the committed golden fixtures."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from conftest import random_sigma, rel_err
+from liteqt_b200 import synthetic as S
+
+MU = (0.1, -0.1)
+
+
+def _temp():
+    return (S.temperature_for_kT(0.025),) * 2
+
+
+@pytest.mark.parametrize("consistent", [False, True])
+@pytest.mark.parametrize("nm,nx,scatter", [(8, 5, False), (8, 2, True), (12, 4, True), (16, 3, False)])
+def test_cpp_matches_numpy_restatement(oracle_mod, consistent, nm, nx, scatter):
+    O = oracle_mod
+    d = S.make_device(nm, nx, seed=nm * 100 + nx)
+    E = np.array([-2.2, -0.45, 0.02, 0.9, 2.7])
+    sl = sr = None
+    if scatter:
+        sl, sr = random_sigma(nm, nx, len(E), seed=7)
+    opts = O.Opts(consistent=consistent)
+    r = O.rgf_batch(d.Hii, d.H1i, E, MU, _temp(), opts, sig_lesser=sl, sig_r=sr, threads=2)
+    Hb, H1b = O.to_blocks(d.Hii), O.to_blocks(d.H1i)
+    for ie, e in enumerate(E):
+        t = O.rgf_numpy(Hb, H1b, e, MU, _temp(), opts,
+                        sigl=None if sl is None else O.to_blocks(sl[ie]),
+                        sigr=None if sr is None else O.to_blocks(sr[ie]))
+        g_scale = np.max(np.abs(t["ldos"]))
+        for k in ("ldos", "ndens", "GRi1"):
+            assert rel_err(O.to_blocks(r[k][ie]), t[k]) < 1e-9, k
+        assert rel_err(O.to_blocks(r["pdens"][ie]), t["pdens"], scale=g_scale) < 1e-9
+        cur_scale = nm * np.max(np.abs(H1b)) * np.max(np.abs(t["ndens"]))
+        assert rel_err(O.to_blocks(r["cur"][ie]), t["cur"], scale=cur_scale) < 1e-9
+        assert abs(r["T"][ie] - t["T"]) < 1e-9 * max(1.0, abs(t["T"]))
+        tr_scale = max(np.max(np.abs(r["tr"])), 1e-300)
+        assert abs(r["tr"][ie] - t["tr"]) < 1e-8 * tr_scale + 1e-14 * nm
+        assert abs(r["tre"][ie] - t["tre"]) < 1e-8 * tr_scale + 1e-14 * nm
+        assert tuple(r["stats"][ie][["sancho_iters_left", "sancho_iters_right"]]) == t["iters"]
+
+
+def test_gemm_inverse_counts_follow_reference_formula(oracle_mod):
+    """N_gemm = 28 Nx - 18 + 6 (nL + nR) and N_inv = Nx + 4 + nL + nR for a
+    call with GRi1 only (green_rgf.f90:2920), plus 2 (Nx-2) + 4 T(E) products."""
+    O = oracle_mod
+    nm, nx = 8, 7
+    d = S.make_device(nm, nx, seed=5)
+    r = O.rgf_batch(d.Hii, d.H1i, np.array([0.3]), MU, _temp(), O.Opts(), threads=1)
+    st = r["stats"][0]
+    nl, nr = st["sancho_iters_left"], st["sancho_iters_right"]
+    assert st["n_gemm"] == 28 * nx - 18 + 6 * (nl + nr) + 2 * (nx - 2) + 4
+    assert st["n_inv"] == nx + 4 + nl + nr
+
+
+@pytest.mark.parametrize("nm,nx", [(4, 2), (6, 5), (8, 7)])
+def test_dense_inverse_known_answer(oracle_mod, nm, nx):
+    """Consistent mode equals the inverse of the whole device matrix."""
+    O = oracle_mod
+    d = S.make_device(nm, nx, seed=11 + nm)
+    Hb, H1b = O.to_blocks(d.Hii), O.to_blocks(d.H1i)
+    E = np.array([-1.3, 0.4, 2.1])
+    sl, sr = random_sigma(nm, nx, len(E), seed=3)
+    opts = O.Opts(consistent=True, eta_dev=1e-4)
+    r = O.rgf_batch(d.Hii, d.H1i, E, MU, _temp(), opts, sig_lesser=sl, sig_r=sr, threads=1)
+    for ie, e in enumerate(E):
+        t = O.rgf_numpy(Hb, H1b, e, MU, _temp(), opts, sigl=O.to_blocks(sl[ie]), sigr=O.to_blocks(sr[ie]))
+        srb = O.to_blocks(sr[ie])
+        G = O.dense_green(Hb, H1b, e, t["sigmal"], t["sigmar"], eta_dev=opts.eta_dev, sigr=srb)
+        ldos = O.to_blocks(r["ldos"][ie])
+        gri1 = O.to_blocks(r["GRi1"][ie])
+        for l in range(nx):
+            s = slice(l * nm, (l + 1) * nm)
+            assert rel_err(ldos[l], G[s, s], scale=np.max(np.abs(G))) < 1e-10
+            if l < nx - 1:
+                s1 = slice((l + 1) * nm, (l + 2) * nm)
+                assert rel_err(gri1[l], G[s, s1], scale=np.max(np.abs(G))) < 1e-10
+        # G^< = G Sigma^< G^H with the lead and scattering Sigma^<
+        N = nm * nx
+        Sl = np.zeros((N, N), complex)
+        fl = O.ferm((e - MU[0]) / (opts.boltz * _temp()[0]))
+        fr = O.ferm((e - MU[1]) / (opts.boltz * _temp()[0]))
+        Sl[:nm, :nm] = -(t["sigmal"] - t["sigmal"].conj().T) * fl
+        Sl[-nm:, -nm:] = -(t["sigmar"] - t["sigmar"].conj().T) * fr
+        slb = O.to_blocks(sl[ie])
+        for l in range(nx):
+            Sl[l * nm:(l + 1) * nm, l * nm:(l + 1) * nm] += slb[l]
+        Gless = G @ Sl @ G.conj().T
+        nd = O.to_blocks(r["ndens"][ie])
+        for l in range(nx):
+            s = slice(l * nm, (l + 1) * nm)
+            assert rel_err(nd[l], Gless[s, s], scale=np.max(np.abs(Gless))) < 1e-10
+        # Caroli te(L,R) = Re Tr[Gamma_L G^A Gamma_R G^R] (green.f90:2571-2580)
+        gL = 1j * (t["sigmal"] - t["sigmal"].conj().T)
+        gR = 1j * (t["sigmar"] - t["sigmar"].conj().T)
+        GN1 = G[-nm:, :nm]
+        T = np.real(np.trace(gL @ GN1.conj().T @ gR @ GN1))
+        assert abs(r["T"][ie] - T) < 1e-10 * max(1.0, abs(T))
+
+
+def test_sancho_fixed_point(oracle_mod):
+    O = oracle_mod
+    rng = np.random.default_rng(3)
+    nm = 6
+    X = rng.normal(size=(nm, nm)) + 1j * rng.normal(size=(nm, nm))
+    H00 = 0.1 * (X + X.conj().T)
+    H10 = -1.0 * (np.eye(nm) + 0.1 * rng.normal(size=(nm, nm)))
+    opts = O.Opts()
+    for E in (-0.7, 0.3, 1.1):
+        G, _, it, st = O.sancho_numpy(E, H00, H10, opts)
+        assert st == 0 and it < opts.sancho_nmax
+        z = complex(E, opts.eta_lead)
+        R = G - np.linalg.inv(z * np.eye(nm) - H00 - H10.conj().T @ G @ H10)
+        assert np.linalg.norm(R) < 1e-8 * np.linalg.norm(G)
+
+
+def test_uniform_chain_integer_transmission(oracle_mod):
+    O = oracle_mod
+    nm = 4
+    d = S.uniform_chain(nm, 6, t=-1.0)
+    E = np.array([-1.5, -0.5, 0.05, 0.5, 1.9, 2.5])
+    r = O.rgf_batch(d.Hii, d.H1i, E, MU, _temp(), O.Opts(eta_lead=1e-6, consistent=True), threads=2)
+    inside = np.abs(E) < 2.0
+    assert np.allclose(r["T"][inside], nm, atol=1e-8)
+    assert np.all(np.abs(r["T"][~inside]) < 1e-8)
+    fl = O.ferm((E - MU[0]) / (O.BOLTZ_RGF_RS * _temp()[0]))
+    fr = O.ferm((E - MU[1]) / (O.BOLTZ_RGF_RS * _temp()[0]))
+    expect = r["T"] * (fl - fr)
+    scale = np.max(np.abs(expect))
+    assert np.max(np.abs(r["tr"] - expect)) < 1e-9 * scale
+    assert np.max(np.abs(r["tre"] - expect)) < 1e-9 * scale
+
+
+def test_invariants_and_current_conservation(oracle_mod):
+    O = oracle_mod
+    nm, nx = 8, 6
+    d = S.make_device(nm, nx, seed=21)
+    E = S.energy_grid(9, -1.0, 1.0)
+    r = O.rgf_batch(d.Hii, d.H1i, E, MU, _temp(), O.Opts(consistent=True), threads=2)
+    g = O.to_blocks(r["ndens"])
+    assert np.max(np.abs(g + np.swapaxes(g.conj(), -1, -2))) < 1e-10 * np.max(np.abs(g))
+    ldos = O.to_blocks(r["ldos"])
+    diag = np.diagonal(ldos, axis1=-2, axis2=-1)
+    assert np.all(diag.imag <= 1e-12)
+    scale = np.max(np.abs(r["tr"]))
+    assert np.max(np.abs(r["tr"] - r["tre"])) < 1e-8 * scale
+
+
+def test_singular_block_gives_zero_and_status(oracle_mod):
+    """invert's zero-matrix fallback (green_rgf.f90:4429-4437): H = E*I, no coupling."""
+    O = oracle_mod
+    nm, nx, E = 8, 3, 0.25
+    Hii = O.from_blocks(np.broadcast_to(E * np.eye(nm), (nx, nm, nm)).astype(complex))
+    H1i = np.zeros_like(Hii)
+    r = O.rgf_batch(Hii, H1i, np.array([E]), MU, _temp(), O.Opts(), threads=1)
+    assert r["stats"][0]["status"] & O.ST_SINGULAR
+    assert np.all(np.isfinite(r["ldos"]))
+
+
+def test_sancho_cap_drops_lead_and_sets_status(oracle_mod):
+    O = oracle_mod
+    d = S.make_device(8, 3, seed=2)
+    opts = O.Opts(sancho_nmax=3)
+    r = O.rgf_batch(d.Hii, d.H1i, np.array([0.1]), MU, _temp(), opts, threads=1)
+    assert r["stats"][0]["status"] & O.ST_SANCHO_NC
+    assert r["stats"][0]["sancho_iters_left"] == 4
+    t = O.rgf_numpy(O.to_blocks(d.Hii), O.to_blocks(d.H1i), 0.1, MU, _temp(), opts)
+    assert rel_err(O.to_blocks(r["ldos"][0]), t["ldos"]) < 1e-10
+
+
+def test_calc_n_electron_matches_loop(oracle_mod):
+    O = oracle_mod
+    rng = np.random.default_rng(0)
+    nk, nen, nx, nm = 2, 5, 3, 4
+    Gl = rng.normal(size=(nk, nen, nx, nm, nm)) + 1j * rng.normal(size=(nk, nen, nx, nm, nm))
+    Gg = rng.normal(size=(nk, nen, nx, nm, nm)) + 1j * rng.normal(size=(nk, nen, nx, nm, nm))
+    E = np.linspace(-1, 1, nen)
+    mid = np.array([-0.2, 0.0, 0.3])
+    ne, pe = O.calc_n_electron(Gl, Gg, E, mid)
+    dE = (E[1] - E[0]) / (2.0 * O.PI)
+    dK = 2.0 * O.PI / nk
+    ne2 = np.zeros(nx)
+    pe2 = np.zeros(nx)
+    for i in range(nen):
+        for ik in range(nk):
+            for ix in range(nx):
+                for j in range(nm):
+                    if E[i] > mid[ix]:
+                        ne2[ix] += Gl[ik, i, ix, j, j].imag * dE * dK
+                    else:
+                        pe2[ix] -= Gg[ik, i, ix, j, j].imag * dE * dK
+    assert np.allclose(ne, ne2, rtol=1e-13, atol=1e-15)
+    assert np.allclose(pe, pe2, rtol=1e-13, atol=1e-15)
+
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_oracle_reproduces_golden(oracle_mod, path):
+    O = oracle_mod
+    z = np.load(path)
+    opts = O.Opts(eta_dev=float(z["eta_dev"]), eta_lead=float(z["eta_lead"]),
+                  consistent=bool(z["consistent"]), boltz=float(z["boltz"]))
+    sl = z["sig_lesser"] if z["has_sigma"] else None
+    sr = z["sig_r"] if z["has_sigma"] else None
+    r = O.rgf_batch(z["Hii"], z["H1i"], z["E"], z["mu"], z["temp"], opts, sig_lesser=sl, sig_r=sr,
+                    threads=2)
+    for k in ("ldos", "ndens", "GRi1"):
+        assert rel_err(r[k], z[k]) < 1e-12, k
+    assert rel_err(r["pdens"], z["pdens"], scale=np.max(np.abs(z["ldos"]))) < 1e-12
+    assert rel_err(r["T"], z["T"]) < 1e-12
+    assert rel_err(r["tr"], z["tr"]) < 1e-10
