@@ -133,7 +133,7 @@ def lib():
         L.oracle_rgf_energy.restype = ctypes.c_int
         L.oracle_rgf_batch.argtypes = [ctypes.POINTER(OracleOpts), ctypes.c_int64, ctypes.c_int64,
                                        ctypes.c_int64, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P,
-                                       P, ctypes.c_int]
+                                       P, ctypes.c_int, ctypes.c_int]
         L.oracle_rgf_batch.restype = ctypes.c_int
         L.oracle_calc_n_electron.argtypes = [P, P, ctypes.c_int64, P, ctypes.c_int64,
                                              ctypes.c_int64, ctypes.c_int64, P, P, P]
@@ -155,8 +155,13 @@ def _fortran3(a, nm, nx, dtype=np.complex128):
 
 
 def rgf_batch(Hii, H1i, E, mu, temp, opts: Opts | None = None, sig_lesser=None, sig_r=None,
-              outputs=("ldos", "ndens", "pdens", "cur", "GRi1"), threads: int | None = None):
+              outputs=("ldos", "ndens", "pdens", "cur", "GRi1"), threads: int | None = None,
+              extended: bool = False):
     """Run the C++ oracle over a batch of energies.
+
+    extended=False: FP64 with OpenBLAS, the reference's arithmetic.
+    extended=True: the same algorithm in x87 80-bit long double with plain
+    loops (ground truth for accuracy statements; small cases only).
 
     Arrays use the *block-major* NumPy view of the Fortran layout: shape
     (nx, nm, nm) with the last two axes (col, row) -- i.e. ``X[l].T`` is the
@@ -187,7 +192,7 @@ def rgf_batch(Hii, H1i, E, mu, temp, opts: Opts | None = None, sig_lesser=None, 
     rc = lib().oracle_rgf_batch(ctypes.byref(o), nm, nx, nE, _p(E), _p(mu), _p(temp), _p(Hii),
                                 _p(H1i), _p(sl), _p(sr), _p(out["ndens"]), _p(out["pdens"]),
                                 _p(out["ldos"]), _p(tr), _p(tre), _p(out["cur"]), _p(out["GRi1"]),
-                                _p(T), _p(stats), int(threads))
+                                _p(T), _p(stats), int(threads), int(extended))
     out.update(tr=tr, tre=tre, T=T, stats=stats, status=rc)
     return out
 

@@ -34,6 +34,7 @@
 #include <cstdint>
 #include <cstring>
 #include <dlfcn.h>
+#include <type_traits>
 #include <thread>
 #include <vector>
 
@@ -92,53 +93,113 @@ extern "C" int oracle_init(const char* blas_path) {
 
 namespace {
 
+// Dense kernels on one scalar type.  double: OpenBLAS zgemm / zgetrf / zgetri
+// (the reference's MKL calls).  long double (x87, 64-bit mantissa): plain
+// loops and Gauss-Jordan with partial pivoting -- the extended-precision
+// ground truth the FP64 results are measured against.
+template <typename R>
 struct Work {
+  typedef std::complex<R> C;
   int nm;
   OracleStat* st;
   std::vector<cd> lu_work;
   std::vector<int> ipiv;
   explicit Work(int n, OracleStat* s) : nm(n), st(s), lu_work((size_t)n * n), ipiv(n) {}
 
+  static C opel(const C* X, char t, int n, int i, int j) {  // op(X)[i][j]
+    if (t == 'n') return X[i + (size_t)j * n];
+    if (t == 'c') return std::conj(X[j + (size_t)i * n]);
+    return X[j + (size_t)i * n];  // 't'
+  }
+
   // C = op(A) * op(B), alpha = 1, beta = 0 (every zgemm of green_RGF_RS)
-  void gemm(char ta, char tb, const cd* A, const cd* B, cd* C) {
-    const cd one(1.0, 0.0), zero(0.0, 0.0);
-    p_zgemm(&ta, &tb, &nm, &nm, &nm, &one, A, &nm, B, &nm, &zero, C, &nm);
+  void gemm(char ta, char tb, const C* A, const C* B, C* Cm) {
     st->n_gemm++;
+    if constexpr (std::is_same<R, double>::value) {
+      const cd one(1.0, 0.0), zero(0.0, 0.0);
+      p_zgemm(&ta, &tb, &nm, &nm, &nm, &one, A, &nm, B, &nm, &zero, Cm, &nm);
+    } else {
+      const int n = nm;
+      std::vector<C> At((size_t)n * n), Bt((size_t)n * n);
+      for (int i = 0; i < n; i++)
+        for (int k = 0; k < n; k++) At[k + (size_t)i * n] = opel(A, ta, n, i, k);  // row i contiguous
+      for (int j = 0; j < n; j++)
+        for (int k = 0; k < n; k++) Bt[k + (size_t)j * n] = opel(B, tb, n, k, j);  // col j contiguous
+      for (int j = 0; j < n; j++)
+        for (int i = 0; i < n; i++) {
+          C acc(0, 0);
+          const C* a = &At[(size_t)i * n];
+          const C* b = &Bt[(size_t)j * n];
+          for (int k = 0; k < n; k++) acc += a[k] * b[k];
+          Cm[i + (size_t)j * n] = acc;
+        }
+    }
   }
 
   // invert: green_rgf.f90:4421-4441.  zgetrf + zgetri; on info /= 0 the
   // reference prints a warning and returns the zero matrix.
-  void invert(cd* A) {
-    int info = 0;
-    const int lw = nm * nm;
+  void invert(C* A) {
     st->n_inv++;
-    p_zgetrf(&nm, &nm, A, &nm, ipiv.data(), &info);
-    if (info != 0) {
-      std::fill(A, A + (size_t)nm * nm, cd(0.0, 0.0));
-      st->status |= ST_SINGULAR;
-      return;
-    }
-    p_zgetri(&nm, A, &nm, ipiv.data(), lu_work.data(), &lw, &info);
-    if (info != 0) {
-      std::fill(A, A + (size_t)nm * nm, cd(0.0, 0.0));
-      st->status |= ST_SINGULAR;
+    const int n = nm;
+    if constexpr (std::is_same<R, double>::value) {
+      int info = 0;
+      const int lw = n * n;
+      p_zgetrf(&nm, &nm, A, &nm, ipiv.data(), &info);
+      if (info == 0) p_zgetri(&nm, A, &nm, ipiv.data(), lu_work.data(), &lw, &info);
+      if (info != 0) {
+        std::fill(A, A + (size_t)n * n, C(0, 0));
+        st->status |= ST_SINGULAR;
+      }
+    } else {
+      std::vector<int> perm(n);
+      for (int k = 0; k < n; k++) {
+        int p = k;
+        R best = -1;
+        for (int i = k; i < n; i++) {
+          const R v = std::fabs(A[i + (size_t)k * n].real()) + std::fabs(A[i + (size_t)k * n].imag());
+          if (v > best) { best = v; p = i; }
+        }
+        perm[k] = p;
+        if (best == 0) {
+          std::fill(A, A + (size_t)n * n, C(0, 0));
+          st->status |= ST_SINGULAR;
+          return;
+        }
+        if (p != k)
+          for (int j = 0; j < n; j++) std::swap(A[k + (size_t)j * n], A[p + (size_t)j * n]);
+        const C pinv = C(1, 0) / A[k + (size_t)k * n];
+        A[k + (size_t)k * n] = C(1, 0);
+        for (int j = 0; j < n; j++) A[k + (size_t)j * n] *= pinv;
+        for (int i = 0; i < n; i++) {
+          if (i == k) continue;
+          const C f = A[i + (size_t)k * n];
+          A[i + (size_t)k * n] = C(0, 0);
+          for (int j = 0; j < n; j++) A[i + (size_t)j * n] -= f * A[k + (size_t)j * n];
+        }
+      }
+      for (int k = n - 1; k >= 0; k--)
+        if (perm[k] != k)
+          for (int i = 0; i < n; i++) std::swap(A[i + (size_t)k * n], A[i + (size_t)perm[k] * n]);
     }
   }
 };
 
-inline double ferm(double a) { return 1.0 / (1.0 + std::exp(a)); }  // green_rgf.f90:4444-4447
+template <typename R>
+inline R ferm(R a) { return R(1) / (R(1) + std::exp(a)); }  // green_rgf.f90:4444-4447
 
 inline size_t nn(int nm) { return (size_t)nm * nm; }
 
 // sancho: green_rgf.f90:4451-4537 (S00 = identity at every call site).
 // Returns the iteration count taken (nmax+1 encodes "not converged").
-int sancho(Work& w, const OracleOpts& o, double E, const cd* H00, const cd* H10,
-           cd* G00, cd* GBB) {
+template <typename R>
+int sancho(Work<R>& w, const OracleOpts& o, R E, const std::complex<R>* H00,
+           const std::complex<R>* H10, std::complex<R>* G00, std::complex<R>* GBB) {
+  typedef std::complex<R> cd;
   const int nm = w.nm;
   const size_t n2 = nn(nm);
   std::vector<cd> A(n2), B(n2), C(n2), H_BB(H00, H00 + n2), H_SS(H00, H00 + n2),
       H_10(H10, H10 + n2), H_01(n2);
-  const cd z(E, o.eta_lead);
+  const cd z(E, (R)o.eta_lead);
   for (int j = 0; j < nm; j++)
     for (int i = 0; i < nm; i++) H_01[i + (size_t)j * nm] = std::conj(H_10[j + (size_t)i * nm]);
   int taken = 0;
@@ -157,7 +218,7 @@ int sancho(Work& w, const OracleOpts& o, double E, const cd* H00, const cd* H10,
     for (size_t k = 0; k < n2; k++) H_BB[k] += A[k];
     w.gemm('n', 'n', H_01.data(), B.data(), C.data());
     H_01 = C;
-    double error = 0.0;
+    R error = 0;
     for (size_t k = 0; k < n2; k++)
       error += std::sqrt(C[k].imag() * C[k].imag() + C[k].real() * C[k].real());
     if (std::fabs(error) < o.sancho_tol) break;
@@ -184,20 +245,49 @@ int sancho(Work& w, const OracleOpts& o, double E, const cd* H00, const cd* H10,
 // null (treated as zero).  Every output may be null (not written).
 // T_out (if non-null, and o.want_T) receives the Caroli transmission
 // Re Tr[Gamma_L G^A_{1N} Gamma_R G^R_{N1}] (green.f90:2571-2580).
-extern "C" int oracle_rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E,
-                                 const double* mu, const double* temp, const cd* Hii,
-                                 const cd* H1i, const cd* sig_lesser, const cd* sig_r,
-                                 cd* ndens, cd* pdens, cd* ldos, double* tr, double* tre,
-                                 double* cur, cd* GRi1, cd* GLi1, cd* GGi1, double* T_out,
-                                 OracleStat* st) {
+namespace {
+
+template <typename R>
+int rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E_in, const double* mu,
+               const double* temp, const cd* Hii_in, const cd* H1i_in, const cd* sig_lesser_in,
+               const cd* sig_r_in, cd* ndens_out, cd* pdens_out, cd* ldos_out, double* tr,
+               double* tre, double* cur_out, cd* GRi1_out, cd* GLi1_out, cd* GGi1_out,
+               double* T_out, OracleStat* st) {
+  typedef std::complex<R> cd;
+  typedef std::complex<double> cdd;
   const OracleOpts& o = *opts;
+  const R E = (R)E_in;
   OracleStat dummy{};
   if (!st) st = &dummy;
   std::memset(st, 0, sizeof(*st));
   if (nm64 < 1 || nx64 < 2 || nm64 > 4096) { st->status = ST_BAD_ARGS; return ST_BAD_ARGS; }
   const int nm = (int)nm64, nx = (int)nx64;
   const size_t n2 = nn(nm);
-  Work w(nm, st);
+  Work<R> w(nm, st);
+  // inputs and outputs in the working precision
+  const size_t nall = n2 * (size_t)nx;
+  std::vector<cd> Hii_v(Hii_in, Hii_in + nall), H1i_v(H1i_in, H1i_in + nall);
+  std::vector<cd> sl_v, sr_v, nd_v, pd_v, ld_v, gr_v, gl_v, gg_v;
+  std::vector<R> cur_v;
+  if (sig_lesser_in) sl_v.assign(sig_lesser_in, sig_lesser_in + nall);
+  if (sig_r_in) sr_v.assign(sig_r_in, sig_r_in + nall);
+  auto outbuf = [&](cdd* p, std::vector<cd>& v) -> cd* {
+    if (!p) return nullptr;
+    v.assign(p, p + nall);  // keep the caller's values where nothing is written
+    return v.data();
+  };
+  const cd* Hii = Hii_v.data();
+  const cd* H1i = H1i_v.data();
+  const cd* sig_lesser = sig_lesser_in ? sl_v.data() : nullptr;
+  const cd* sig_r = sig_r_in ? sr_v.data() : nullptr;
+  cd* ndens = outbuf(ndens_out, nd_v);
+  cd* pdens = outbuf(pdens_out, pd_v);
+  cd* ldos = outbuf(ldos_out, ld_v);
+  cd* GRi1 = outbuf(GRi1_out, gr_v);
+  cd* GLi1 = outbuf(GLi1_out, gl_v);
+  cd* GGi1 = outbuf(GGi1_out, gg_v);
+  R* cur = nullptr;
+  if (cur_out) { cur_v.assign(cur_out, cur_out + nall); cur = cur_v.data(); }
   auto blk = [&](const cd* base, int l) { return base + (size_t)(l - 1) * n2; };  // 1-based l
   auto blkw = [&](cd* base, int l) { return base + (size_t)(l - 1) * n2; };
   auto adj = [&](const cd* X, cd* Y) {  // Y = X^H
@@ -210,8 +300,8 @@ extern "C" int oracle_rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t n
   // the consistent variant uses H_{l+1,l} = H1i(:,:,l+1).
   auto H1b = [&](int l) { return o.consistent ? blk(H1i, l + 1) : blk(H1i, l); };
 
-  const double mul = mu[0], mur = mu[1], templ = temp[0], tempr = temp[1];
-  const cd z(E, o.eta_dev);
+  const R mul = mu[0], mur = mu[1], templ = temp[0], tempr = temp[1];
+  const cd z(E, (R)o.eta_dev);
   std::vector<cd> Gl(n2 * nx), Gln(n2 * nx);
   std::vector<cd> H00(n2), H10(n2), A(n2), B(n2), C(n2), D(n2), G00(n2), GBB(n2), GN0(n2),
       Gn(n2), Gp(n2), sig(n2), sigmal(n2), sigmar(n2), tmp(n2), GN1(n2), GN1b(n2);
@@ -219,7 +309,7 @@ extern "C" int oracle_rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t n
   if (ldos) std::fill(ldos, ldos + n2 * nx, cd(0, 0));
   if (ndens) std::fill(ndens, ndens + n2 * nx, cd(0, 0));
   if (pdens) std::fill(pdens, pdens + n2 * nx, cd(0, 0));
-  if (cur) std::fill(cur, cur + n2 * nx, 0.0);
+  if (cur) std::fill(cur, cur + n2 * nx, R(0));
 
   // ---- left contact (green_rgf.f90:3992-4012)
   for (size_t k = 0; k < n2; k++) H00[k] = blk(Hii, 1)[k] + sigR(1, k);
@@ -229,7 +319,7 @@ extern "C" int oracle_rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t n
   w.gemm('n', 'n', H10.data(), G00.data(), A.data());
   w.gemm('n', 'c', A.data(), H10.data(), sigmal.data());
   {
-    const double f = ferm((E - mul) / (o.boltz * templ));
+    const R f = ferm<R>((E - mul) / ((R)o.boltz * templ));
     for (int j = 0; j < nm; j++)
       for (int i = 0; i < nm; i++) {
         const size_t k = i + (size_t)j * nm;
@@ -284,7 +374,7 @@ extern "C" int oracle_rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t n
   std::copy(blkw(Gln.data(), nx - 1), blkw(Gln.data(), nx - 1) + n2, sig.begin());
   w.gemm('n', 'n', H10.data(), sig.data(), B.data());
   w.gemm('n', 'c', B.data(), H10.data(), C.data());
-  const double fR = ferm((E - mur) / (o.boltz * templ));  // TEMPl here: trap T2 (green_rgf.f90:4051)
+  const R fR = ferm<R>((E - mur) / ((R)o.boltz * templ));  // TEMPl here: trap T2 (green_rgf.f90:4051)
   for (int j = 0; j < nm; j++)
     for (int i = 0; i < nm; i++) {
       const size_t k = i + (size_t)j * nm;
@@ -312,9 +402,9 @@ extern "C" int oracle_rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t n
     }
   w.gemm('n', 'n', A.data(), Gn.data(), C.data());
   {
-    double tim = 0.0;
+    R tim = 0;
     for (int i = 0; i < nm; i++) tim = tim - (B[i + (size_t)i * nm] - C[i + (size_t)i * nm]).real();
-    if (tr) *tr = tim;
+    if (tr) *tr = (double)tim;
   }
   // Caroli T(E): G_{N1} = G_NN H_{N,N-1} g^L_{N-1,1};  T = Re Tr[Gamma_R G_{N1} Gamma_L G_{N1}^H]
   if (o.want_T && T_out) {
@@ -329,10 +419,10 @@ extern "C" int oracle_rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t n
     w.gemm('n', 'n', G00.data(), GN1b.data(), X.data());   // X = G_{N1}
     w.gemm('n', 'n', gR.data(), X.data(), Y.data());       // Y = Gamma_R G_{N1}
     w.gemm('n', 'c', gL.data(), X.data(), GN1b.data());    // Gamma_L G_{N1}^H
-    double t = 0.0;
+    R t = 0;
     for (int i = 0; i < nm; i++)
       for (int k = 0; k < nm; k++) t += (Y[i + (size_t)k * nm] * GN1b[k + (size_t)i * nm]).real();
-    *T_out = t;
+    *T_out = (double)t;
   }
 
   // ---- backward sweep (green_rgf.f90:4069-4149)
@@ -410,7 +500,7 @@ extern "C" int oracle_rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t n
       const size_t k = i + (size_t)j * nm;
       Gp[k] = Gn[k] + (G00[k] - std::conj(G00[j + (size_t)i * nm]));
     }
-  const double fL = ferm((E - mul) / (o.boltz * tempr));
+  const R fL = ferm<R>((E - mul) / ((R)o.boltz * tempr));
   for (int j = 0; j < nm; j++)
     for (int i = 0; i < nm; i++) {
       const size_t k = i + (size_t)j * nm;
@@ -424,11 +514,47 @@ extern "C" int oracle_rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t n
     }
   w.gemm('n', 'n', A.data(), Gn.data(), C.data());
   {
-    double tim = 0.0;
+    R tim = 0;
     for (int i = 0; i < nm; i++) tim = tim + (B[i + (size_t)i * nm] - C[i + (size_t)i * nm]).real();
-    if (tre) *tre = tim;
+    if (tre) *tre = (double)tim;
   }
+  auto back = [&](const std::vector<cd>& v, cdd* p) {
+    if (p)
+      for (size_t k = 0; k < nall; k++) p[k] = cdd((double)v[k].real(), (double)v[k].imag());
+  };
+  back(nd_v, ndens_out);
+  back(pd_v, pdens_out);
+  back(ld_v, ldos_out);
+  back(gr_v, GRi1_out);
+  back(gl_v, GLi1_out);
+  back(gg_v, GGi1_out);
+  if (cur_out)
+    for (size_t k = 0; k < nall; k++) cur_out[k] = (double)cur_v[k];
   return st->status;
+}
+
+}  // namespace
+
+extern "C" int oracle_rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E,
+                                 const double* mu, const double* temp, const cd* Hii,
+                                 const cd* H1i, const cd* sig_lesser, const cd* sig_r,
+                                 cd* ndens, cd* pdens, cd* ldos, double* tr, double* tre,
+                                 double* cur, cd* GRi1, cd* GLi1, cd* GGi1, double* T_out,
+                                 OracleStat* st) {
+  return rgf_energy<double>(opts, nm64, nx64, E, mu, temp, Hii, H1i, sig_lesser, sig_r, ndens,
+                            pdens, ldos, tr, tre, cur, GRi1, GLi1, GGi1, T_out, st);
+}
+
+// The same computation in x87 extended precision (64-bit mantissa) with
+// plain loops: the ground truth that FP64 results are measured against.
+extern "C" int oracle_rgf_energy_ld(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E,
+                                    const double* mu, const double* temp, const cd* Hii,
+                                    const cd* H1i, const cd* sig_lesser, const cd* sig_r,
+                                    cd* ndens, cd* pdens, cd* ldos, double* tr, double* tre,
+                                    double* cur, cd* GRi1, cd* GLi1, cd* GGi1, double* T_out,
+                                    OracleStat* st) {
+  return rgf_energy<long double>(opts, nm64, nx64, E, mu, temp, Hii, H1i, sig_lesser, sig_r,
+                                 ndens, pdens, ldos, tr, tre, cur, GRi1, GLi1, GGi1, T_out, st);
 }
 
 // Batch over energy points, one worker thread per core and one energy per
@@ -441,7 +567,7 @@ extern "C" int oracle_rgf_batch(const OracleOpts* opts, int64_t nm, int64_t nx, 
                                 const cd* Hii, const cd* H1i, const cd* sig_lesser,
                                 const cd* sig_r, cd* ndens, cd* pdens, cd* ldos, double* tr,
                                 double* tre, double* cur, cd* GRi1, double* T_out,
-                                OracleStat* stats, int n_threads) {
+                                OracleStat* stats, int n_threads, int extended) {
   const size_t per = (size_t)nm * nm * nx;
   std::atomic<int64_t> next(0);
   std::atomic<int> worst(0);
@@ -450,7 +576,7 @@ extern "C" int oracle_rgf_batch(const OracleOpts* opts, int64_t nm, int64_t nx, 
       const int64_t e = next.fetch_add(1);
       if (e >= nE) break;
       OracleStat st{};
-      const int s = oracle_rgf_energy(
+      const int s = (extended ? oracle_rgf_energy_ld : oracle_rgf_energy)(
           opts, nm, nx, E[e], mu, temp, Hii, H1i, sig_lesser ? sig_lesser + e * per : nullptr,
           sig_r ? sig_r + e * per : nullptr, ndens ? ndens + e * per : nullptr,
           pdens ? pdens + e * per : nullptr, ldos ? ldos + e * per : nullptr,

