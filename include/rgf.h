@@ -191,6 +191,37 @@ RGF_API int rgf_calc_n_electron(rgf_ctx* ctx, const rgf_c16* G_lesser, const rgf
                         int64_t nen, const double* E, int64_t nm, int64_t nk, int64_t nx,
                         double* nelec, double* pelec, const double* midgap);
 
+/* Batched FP64 solve that allocates no device memory.  No counterpart in the
+ * reference: it exists for callers that cannot let a library call cudaMalloc
+ * -- host codes whose own memory pool owns all of HBM, or that call the solver
+ * inside a loop where cudaMalloc's implicit device synchronisation is not
+ * acceptable.  Same meaning as rgf_solve_energies, except:
+ *   - every array (device->Hii, H1i and all inputs / outputs) must be device
+ *     memory; E (nen energies) and info (nen entries, may be NULL) are host
+ *     memory; there is no context: options come per call, `stream` is a
+ *     cudaStream_t (NULL = the default stream), and the call returns when the
+ *     results are written;
+ *   - its workspace is a fixed 256 MiB array inside the library, reserved on
+ *     every GPU that loads the library until the process exits; problems
+ *     whose one solver slot plus task tables exceed it ((2 nx + 32) nm^2 * 16
+ *     bytes + about 200 bytes per energy) are rejected with RGF_E_ARG;
+ *   - the first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current, so make that first
+ *     call before any stream capture;
+ *   - all calls share the array, which keeps the last call's contents; calls
+ *     from one process are serialised by a lock, and calls whose GPU work
+ *     overlaps (for example from several processes sharing a device through
+ *     MPS, which each see their own copy) must not be assumed to be
+ *     independent of that.
+ * The error text of a failed call is rgf_noalloc_last_error(). */
+RGF_API int rgf_solve_energies_noalloc(const rgf_opts* opts, const rgf_device* device,
+                                       int64_t nen, const double* E,
+                                       const rgf_c16* sigma_lesser, const rgf_c16* sigma_r,
+                                       rgf_c16* ldos, rgf_c16* ndens, rgf_c16* pdens,
+                                       rgf_c16* GRi1, double* cur, double* tr, double* tre,
+                                       double* T, rgf_task_info* info, void* stream);
+RGF_API const char* rgf_noalloc_last_error(void);
+
 /* Last error message of the calling thread ("" if none). */
 RGF_API const char* rgf_last_error(void);
 
