@@ -23,9 +23,11 @@
 //     of GGi1 (:4094-4103) are skipped.
 // The result is the same function of the inputs up to rounding.
 #include <cstdio>
+#include <type_traits>
 
 #include "rgf_device.cuh"
 #include "rgf_internal.h"
+#include "rgf_staged.cuh"
 
 namespace rgf {
 
@@ -34,7 +36,7 @@ namespace {
 enum TmpBlock {
   T_H00 = 0, T_SA, T_SB, T_HBB, T_HSS, T_H10A, T_H10B, T_H01A, T_H01B, T_GS,
   T_SIGL, T_SIGR, T_SIG, T_F1, T_F2, T_F3, T_F4, T_GN1A, T_GN1B, T_G00A,
-  T_G00B, T_GNA, T_GNB, T_Q1, T_Q2, T_Q3, T_Q4, T_R5, T_INV,
+  T_G00B, T_GNA, T_GNB, T_Q1, T_Q2, T_Q3, T_Q4, T_R5, T_INV, T_RT,
   T_COUNT,
   // aliases (lifetimes do not overlap)
   T_R7 = T_F4, T_P1 = T_F1, T_P2 = T_F2, T_P3 = T_F3, T_P4 = T_SIG,
@@ -49,20 +51,63 @@ struct Smem {
   int64_t task;
 };
 
+constexpr int kSmemXMaxNb = 64;  // generic path: inverse workspace in shared memory up to this nb
+
+// Any nb that is a multiple of 8: register-direct DMMA GEMM (warp tiles of
+// TM x TN 8x8 subtiles), unblocked Gauss-Jordan.
 template <int TM, int TN>
+struct GenericOps {
+  static constexpr int kMinBlocks = 2;
+  static size_t smem_bytes(int nb) { return nb <= kSmemXMaxNb ? (size_t)nb * nb * sizeof(double2) : 0; }
+  SmemInv& inv;
+  double2* X;
+  __device__ GenericOps(SmemInv& i, double2* dyn, double2* slot_inv, double2*, int n)
+      : inv(i), X(n <= kSmemXMaxNb ? dyn : slot_inv) {}
+  template <class Epi>
+  __device__ void gemm(int n, const double2* A, bool cA, const double2* B, bool cB, Epi&& epi) {
+    cgemm<TM, TN>(n, A, cA, B, cB, epi);
+  }
+  __device__ int invert(int n, double2* dst, double2* dst2) { return gj_invert(n, X, dst, dst2, inv); }
+};
+
+// nb = 32, 64, 128, 256: shared-memory-staged GEMM; inverse in shared memory
+// (nb <= 64) or blocked with shared-memory panels.
+template <int NB>
+struct StagedOps {
+  static constexpr int kMinBlocks = 2;
+  static size_t smem_bytes(int) { return StagedCfg<NB>::SMEM; }
+  SmemInv& inv;
+  double2* dyn;
+  double2* X;
+  double2* Rt;
+  __device__ StagedOps(SmemInv& i, double2* dyn_, double2* slot_inv, double2* slot_rt, int)
+      : inv(i), dyn(dyn_), X(StagedCfg<NB>::SMEM_INV ? dyn_ : slot_inv), Rt(slot_rt) {}
+  template <class Epi>
+  __device__ void gemm(int, const double2* A, bool cA, const double2* B, bool cB, Epi&& epi) {
+    gemm_staged<NB>(NB, NB, NB, A, NB, cA, B, NB, cB, dyn, epi);
+  }
+  __device__ int invert(int, double2* dst, double2* dst2) {
+    if constexpr (StagedCfg<NB>::SMEM_INV) return gj_invert(NB, X, dst, dst2, inv);
+    else return gj_invert_blocked<NB>(X, dst, dst2, Rt, dyn, dyn, inv);
+  }
+};
+
+template <class Ops>
 struct Solver {
   KOpts o;
   int64_t nx_max;
   Smem& sm;
-  double2* X;       // inverse workspace (shared memory if it fits, else a slot block)
+  Ops& ops;
+  double2* X;       // the matrix to invert is assembled here
   double2* slot;
   int n, nx;
   size_t n2;
   int status = 0, n_gemm = 0, n_inv = 0;
 
-  __device__ Solver(const KOpts& o_, int64_t nx_max_, Smem& sm_, double2* X_, double2* slot_,
+  __device__ Solver(const KOpts& o_, int64_t nx_max_, Smem& sm_, Ops& ops_, double2* slot_,
                     int n_, int nx_)
-      : o(o_), nx_max(nx_max_), sm(sm_), X(X_), slot(slot_), n(n_), nx(nx_), n2((size_t)n_ * n_) {}
+      : o(o_), nx_max(nx_max_), sm(sm_), ops(ops_), X(ops_.X), slot(slot_), n(n_), nx(nx_),
+        n2((size_t)n_ * n_) {}
 
   __device__ double2* tmp(int k) const { return slot + 2 * nx_max * n2 + (size_t)k * n2; }
   __device__ double2* Gl(int l) const { return slot + (size_t)l * n2; }
@@ -70,7 +115,7 @@ struct Solver {
 
   template <class Epi>
   __device__ void gemm(const double2* A, bool cA, const double2* B, bool cB, Epi&& epi) {
-    cgemm<TM, TN>(n, A, cA, B, cB, epi);
+    ops.gemm(n, A, cA, B, cB, epi);
     n_gemm++;
     __syncthreads();
   }
@@ -86,7 +131,7 @@ struct Solver {
   // X holds the matrix; dst (and dst2) receive its inverse.
   __device__ void invert_X(double2* dst, double2* dst2 = nullptr) {
     n_inv++;
-    if (gj_invert(n, X, dst, dst2, sm.inv)) status |= RGF_ST_SINGULAR;
+    if (ops.invert(n, dst, dst2)) status |= RGF_ST_SINGULAR;
   }
 
   // sancho (green_rgf.f90:4451-4537) with S00 = I.  H00 is a slot block; the
@@ -423,11 +468,9 @@ struct Solver {
   __device__ double* blk2(double* base, int l) const { return base + (size_t)l * n2; }
 };
 
-constexpr int kSmemXMaxNb = 64;  // inverse workspace in shared memory up to this nb
-
-template <int TM, int TN>
+template <class Ops>
 __global__ void __launch_bounds__(kThreads, 2) rgf_fp64_kernel(KParams p) {
-  extern __shared__ double2 dyn_smem[];
+  extern __shared__ __align__(16) double2 dyn_smem[];
   __shared__ Smem sm;
   double2* slot = p.work + (size_t)blockIdx.x * p.slot_elems;
   for (;;) {
@@ -445,53 +488,64 @@ __global__ void __launch_bounds__(kThreads, 2) rgf_fp64_kernel(KParams p) {
       continue;
     }
     const int n = (int)dv.nm;
-    double2* X = (n <= kSmemXMaxNb) ? dyn_smem
-                                    : slot + 2 * p.nx_max * (size_t)n * n + (size_t)T_INV * n * n;
-    Solver<TM, TN> s(p.o, p.nx_max, sm, X, slot, n, (int)dv.nx);
+    const size_t n2 = (size_t)n * n;
+    double2* temps = slot + 2 * p.nx_max * n2;
+    Ops ops(sm.inv, dyn_smem, temps + (size_t)T_INV * n2, temps + (size_t)T_RT * n2, n);
+    Solver<Ops> s(p.o, p.nx_max, sm, ops, slot, n, (int)dv.nx);
     s.run(tk, dv, info);
   }
 }
 
-template <int TM, int TN>
+template <class Ops>
 cudaError_t launch_cfg(const KParams& p, int grid, cudaStream_t st) {
-  const size_t smem = fp64_smem_bytes(p.nb);
-  auto k = rgf_fp64_kernel<TM, TN>;
+  const size_t smem = Ops::smem_bytes(p.nb);
+  auto k = rgf_fp64_kernel<Ops>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   k<<<grid, kThreads, smem, st>>>(p);
   return cudaGetLastError();
 }
 
-template <int TM, int TN>
+template <class Ops>
 int occupancy_cfg(int nb) {
   int nblk = 0;
-  const size_t smem = fp64_smem_bytes(nb);
-  auto k = rgf_fp64_kernel<TM, TN>;
+  const size_t smem = Ops::smem_bytes(nb);
+  auto k = rgf_fp64_kernel<Ops>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nblk, k, kThreads, smem) != cudaSuccess) return 1;
   return nblk > 0 ? nblk : 1;
 }
 
+// Dispatch on the block size: the staged kernels for the benchmark sizes, the
+// generic one for any other multiple of 8.
+template <class F>
+auto dispatch(int nb, F&& f) {
+  switch (nb) {
+    case 32: return f((StagedOps<32>*)nullptr);
+    case 64: return f((StagedOps<64>*)nullptr);
+    case 128: return f((StagedOps<128>*)nullptr);
+    case 256: return f((StagedOps<256>*)nullptr);
+    default: break;
+  }
+  if (nb % 16 == 0 && nb >= 64) return f((GenericOps<2, 2>*)nullptr);
+  if (nb % 16 == 0) return f((GenericOps<1, 2>*)nullptr);
+  return f((GenericOps<1, 1>*)nullptr);
+}
+
 }  // namespace
 
 size_t fp64_smem_bytes(int nb) {
-  return nb <= kSmemXMaxNb ? (size_t)nb * nb * sizeof(double2) : 0;
+  return dispatch(nb, [&](auto* tag) { return std::remove_pointer_t<decltype(tag)>::smem_bytes(nb); });
 }
 
 int fp64_threads() { return kThreads; }
 
-// Warp tile (TM x TN subtiles of 8x8) by block size.
 cudaError_t launch_fp64(const KParams& p, int grid, cudaStream_t st) {
-  const int nb = p.nb;
-  if (nb % 16 == 0 && nb >= 64) return launch_cfg<2, 2>(p, grid, st);
-  if (nb % 16 == 0) return launch_cfg<1, 2>(p, grid, st);
-  return launch_cfg<1, 1>(p, grid, st);
+  return dispatch(p.nb, [&](auto* tag) { return launch_cfg<std::remove_pointer_t<decltype(tag)>>(p, grid, st); });
 }
 
 int fp64_blocks_per_sm(int nb) {
-  if (nb % 16 == 0 && nb >= 64) return occupancy_cfg<2, 2>(nb);
-  if (nb % 16 == 0) return occupancy_cfg<1, 2>(nb);
-  return occupancy_cfg<1, 1>(nb);
+  return dispatch(nb, [&](auto* tag) { return occupancy_cfg<std::remove_pointer_t<decltype(tag)>>(nb); });
 }
 
 }  // namespace rgf

@@ -15,7 +15,8 @@ accepts an output whose distance to the x87 80-bit evaluation of the same
 algorithm (the exact answer to ~1e-18) is within 4x the FP64 oracle's own
 distance to it, up to 8x (the spread seen between independent FP64
 implementations of the same algorithm): the GPU result is then as exact as
-the reference's."""
+the reference's.  (At nb = 128 with eta = 1e-5 the FP64 oracle itself is
+3e-8 from the exact answer; no output may ever be more than 1e-6 from it.)"""
 import ctypes
 import glob
 import os
@@ -93,7 +94,7 @@ def compare(g, r, nm, H1i, tol=TOL, truth=None, skip_last_gri1=True):
     e_gt = errors(g, truth, nm, H1i, skip_last_gri1)
     e_rt = errors(r, truth, nm, H1i, skip_last_gri1)
     bad = {k: (e_go[k], e_gt[k], e_rt[k]) for k in e_go
-           if not (e_go[k] <= tol or e_gt[k] <= 8.0 * e_rt[k] + 1e-12) or not e_gt[k] < 1e-7}
+           if not (e_go[k] <= tol or e_gt[k] <= 8.0 * e_rt[k] + 1e-12) or not e_gt[k] < 1e-6}
     assert not bad, f"(gpu-oracle, gpu-exact, oracle-exact) failing: {bad}"
     return e_go
 
@@ -319,3 +320,28 @@ def test_energy_integrals_match_oracle(rgf):
     assert np.allclose(pe, pe2, rtol=1e-12, atol=1e-14)
     I2 = O.terminal_current(tr, E[1] - E[0], 2.0, nk)
     assert abs(I - I2) <= 1e-12 * abs(I2)
+
+
+def test_fp64_nb256_matches_oracle(rgf):
+    """The largest block size (the mixed-precision configuration's nb) at the
+    reference's own settings.  At nb = 256 two faithful FP64 restatements (the
+    C++ oracle and the NumPy one) already differ by ~3e-10, and the 80-bit
+    evaluation takes minutes, so the bound is 1e-10 or 3x that C++/NumPy
+    distance, whichever is larger."""
+    from oracle import oracle as O
+    nm, nx = 256, 2
+    d = S.make_device(nm, nx, seed=256)
+    E = np.array([-1.1, 0.35])
+    g = gpu_solve(rgf, d.Hii, d.H1i, E, rgf.Options())
+    r = oracle_solve(d.Hii, d.H1i, E, O.Opts())
+    assert np.all(g["info"]["status"] == 0)
+    Hb, H1b = O.to_blocks(d.Hii), O.to_blocks(d.H1i)
+    tw = [O.rgf_numpy(Hb, H1b, e, MU, _temp(), O.Opts()) for e in E]
+    twin = {k: np.stack([O.from_blocks(t[k]) for t in tw]) for k in ("ldos", "ndens", "pdens", "GRi1")}
+    twin["cur"] = np.stack([O.from_blocks(t["cur"]) for t in tw])
+    for k in ("tr", "tre", "T"):
+        twin[k] = np.array([t[k] for t in tw])
+    e_twin = errors(twin, r, nm, d.H1i)
+    e_gpu = errors(g, r, nm, d.H1i)
+    bad = {k: (e_gpu[k], e_twin[k]) for k in e_gpu if not e_gpu[k] <= max(TOL, 3.0 * e_twin[k])}
+    assert not bad, f"(gpu-oracle, numpy-oracle) failing: {bad}"
