@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-threads", type=int, default=0)
+    p.add_argument("--single", action="store_true",
+                   help="one device-resident solve and exit (for profiler captures; prints no JSON)")
     return p.parse_args()
 
 
@@ -360,9 +362,30 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_single(args):
+    """One device-resident batched solve of the workload (profiler captures)."""
+    import torch
+    from liteqt_b200 import rgf
+    d, E, temp = workload(args)
+    dev = torch.device("cuda", 0)
+    Hii = torch.from_numpy(d.Hii).to(dev)
+    H1i = torch.from_numpy(d.H1i).to(dev)
+    shape = (args.nen, args.nx, args.nb, args.nb)
+    ldos = torch.empty(shape, dtype=torch.complex128, device=dev)
+    ndens = torch.empty_like(ldos)
+    T = torch.empty(args.nen, dtype=torch.float64, device=dev)
+    with rgf.Context(rgf.Options(eta_dev=ETA, eta_lead=ETA)) as ctx:
+        ctx.solve_energies(Hii, H1i, E, MU, temp, ldos=ldos, ndens=ndens, T=T)
+        st = ctx.stats()
+    print(f"single solve nb={args.nb} nx={args.nx} nen={args.nen}: kernel {st['last_kernel_ms']:.1f} ms, "
+          f"{st['last_flops'] / st['last_kernel_ms'] / 1e9:.2f} TFLOP/s executed")
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.single:
+        run_single(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
