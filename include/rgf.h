@@ -180,6 +180,25 @@ RGF_API int rgf_solve_energies(rgf_ctx* ctx, const rgf_device* device, int64_t n
                        rgf_c16* ndens, rgf_c16* pdens, rgf_c16* GRi1, double* cur, double* tr,
                        double* tre, double* T, rgf_task_info* info, void* stream);
 
+/* Adjoint RGF (no counterpart in the reference; the Jacobian a Newton-Poisson
+ * loop needs).  For every energy of one ballistic device (no scattering
+ * self-energy) it returns the Caroli transmission T(E) and its derivatives
+ *   dTdV[e*nx + l] = dT(E_e)/dV_l,  V_l adding V_l * I to Hii(:,:,l+1)
+ *                    (the end blocks also shift their semi-infinite leads,
+ *                    which are the continuation of Hii(:,:,1) / Hii(:,:,nx));
+ *   dTds[e]        = dT(E_e)/ds,    s scaling the interior couplings
+ *                    H1i(:,:,m), m = 2..nx-1 (1-based),
+ * from one reverse sweep with sqrt(nx) checkpoints of the left-connected
+ * Green's functions.  If dIdV (nx values) / dIds (1 value) are non-NULL they
+ * receive the derivatives of the Landauer current
+ *   I = spindeg * e0^2/(2 pi hbar) * dE * sum_e T(E_e) (f_L(E_e) - f_R(E_e)),
+ * with dE = E[1] - E[0] and the constants of green_rgf.f90:18-24.  T, dTdV and
+ * dTds may be host or device memory; E, dIdV and dIds are host memory. */
+RGF_API int rgf_adjoint_energies(rgf_ctx* ctx, const rgf_device* device, int64_t nen,
+                                 const double* E, double* T, double* dTdV, double* dTds,
+                                 double spindeg, double* dIdV, double* dIds,
+                                 rgf_task_info* info, void* stream);
+
 /* Terminal current of one energy sweep: sum(tr)*dE*e0/tpi/hbar*e0*spindeg/nk
  * (green_rgf.f90:2938), summed on the device in a fixed order. */
 RGF_API int rgf_terminal_current(rgf_ctx* ctx, const double* tr, int64_t nen, double dE, double spindeg,
@@ -221,6 +240,17 @@ RGF_API int rgf_solve_energies_noalloc(const rgf_opts* opts, const rgf_device* d
                                        rgf_c16* GRi1, double* cur, double* tr, double* tre,
                                        double* T, rgf_task_info* info, void* stream);
 RGF_API const char* rgf_noalloc_last_error(void);
+
+/* Bond current between the sub-blocks of every block (calc_block_current,
+ * green_rgf.f90:4602-4640): nm = nb*ns orbitals per block as ns sub-blocks
+ * of nb; tot_cur / tot_ecur (nb,nb,nx*ns) are the energy sums of the current
+ * and energy current, jdens (nb,nb,nx*ns,nen) the energy-resolved current
+ * (tot_ecur, jdens may be NULL).  The last sub-block of each block repeats
+ * the previous sub-block's value, as in the reference.  Host outputs. */
+RGF_API int rgf_calc_block_current(rgf_ctx* ctx, const rgf_c16* H, const rgf_c16* G_lesser,
+                                   int64_t nen, const double* E, double spindeg, int64_t nb,
+                                   int64_t ns, int64_t nm, int64_t nx, double* tot_cur,
+                                   double* tot_ecur, double* jdens);
 
 /* Last error message of the calling thread ("" if none). */
 RGF_API const char* rgf_last_error(void);

@@ -6,6 +6,7 @@
 // happens on the host, and there is no CPU fallback: if the CUDA path cannot
 // run, the call fails with RGF_E_CUDA / RGF_E_UNSUPPORTED.
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -425,6 +426,146 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
         printf(" SEVERE warning: nmax reached in sancho!!! task %lld\n", (long long)t);
     }
   }
+  if (worst & RGF_ST_BAD_TASK) return fail(RGF_E_ARG, "a task was rejected on the device");
+  return worst ? RGF_E_STATUS : RGF_OK;
+}
+
+// ------------------------------------------------------------------ adjoint
+extern "C" int rgf_adjoint_energies(rgf_ctx* c, const rgf_device* v, int64_t nen, const double* E,
+                                    double* T, double* dTdV, double* dTds, double spindeg,
+                                    double* dIdV, double* dIds, rgf_task_info* info, void* stream_) {
+  if (!c || !v || !E || nen < 1) return fail(RGF_E_ARG, "invalid argument");
+  if (v->nm < 8 || v->nm > kMaxNb || v->nm % 8 != 0)
+    return fail(RGF_E_UNSUPPORTED, "nm=%lld unsupported (multiple of 8 in [8,%d])", (long long)v->nm, kMaxNb);
+  if (v->nx < 2) return fail(RGF_E_ARG, "nx < 2");
+  if (!v->Hii || !v->H1i) return fail(RGF_E_ARG, "Hii/H1i is NULL");
+  if (!(v->temp[0] > 0.0) || !(v->temp[1] > 0.0)) return fail(RGF_E_ARG, "temperature must be > 0");
+  if ((dIdV || dIds) && nen < 2) return fail(RGF_E_ARG, "the current needs at least two energies");
+  RGF_CUDA(cudaSetDevice(c->device));
+  cudaStream_t st = stream_ ? (cudaStream_t)stream_ : c->stream;
+  const int64_t nx = v->nx, nm = v->nm;
+  // staging: H (in), T / dTdV / dTds (out)
+  Stage sg;
+  const size_t hb = sizeof(rgf_c16) * (size_t)nm * nm * nx;
+  sg.add(v->Hii, hb, true, false);
+  sg.add(v->H1i, hb, true, false);
+  sg.add(T, sizeof(double) * nen, false, true);
+  sg.add(dTdV, sizeof(double) * nen * nx, false, true);
+  sg.add(dTds, sizeof(double) * nen, false, true);
+  sg.layout();
+  int rc = c->stage.reserve(std::max<size_t>(sg.total, 256));
+  if (rc) return rc;
+  char* sbase = (char*)c->stage.p;
+  for (const auto& s : sg.segs)
+    if (s.copy_in) RGF_CUDA(cudaMemcpyAsync(sbase + s.off, s.host, s.bytes, cudaMemcpyHostToDevice, st));
+  // the gradients are always produced on the device (the current needs them)
+  const size_t grad_bytes = sizeof(double) * (size_t)nen * (nx + 2);
+  double* dT_d = dTdV ? (double*)sg.resolve(dTdV, sbase) : nullptr;
+  DDev dd;
+  dd.nm = nm;
+  dd.nx = nx;
+  dd.Hii = (const double2*)sg.resolve(v->Hii, sbase);
+  dd.H1i = (const double2*)sg.resolve(v->H1i, sbase);
+  for (int i = 0; i < 2; i++) { dd.mu[i] = v->mu[i]; dd.temp[i] = v->temp[i]; }
+  if ((rc = c->devs.reserve(sizeof(DDev)))) return rc;
+  if ((rc = c->tasks.reserve(sizeof(DAdj) * nen + grad_bytes))) return rc;
+  if ((rc = c->info.reserve(sizeof(DInfo) * nen))) return rc;
+  if ((rc = c->queue.reserve(sizeof(int32_t) * 64))) return rc;
+  char* tb = (char*)c->tasks.p;
+  double* scratch = (double*)(tb + sizeof(DAdj) * nen);  // dTdV (if not given), T, dTds
+  if (!dT_d) dT_d = scratch;
+  double* T_d = T ? (double*)sg.resolve(T, sbase) : scratch + (size_t)nen * nx;
+  double* ds_d = dTds ? (double*)sg.resolve(dTds, sbase) : scratch + (size_t)nen * nx + nen;
+  std::vector<DAdj> tasks(nen);
+  for (int64_t e = 0; e < nen; e++) {
+    DAdj& a = tasks[e];
+    a.dev = 0;
+    a.pad = 0;
+    a.E = E[e];
+    a.T = T_d + e;
+    a.dTdV = dT_d + e * nx;
+    a.dTds = ds_d + e;
+  }
+  RGF_CUDA(cudaMemcpyAsync(c->devs.p, &dd, sizeof(DDev), cudaMemcpyHostToDevice, st));
+  RGF_CUDA(cudaMemcpyAsync(tb, tasks.data(), sizeof(DAdj) * nen, cudaMemcpyHostToDevice, st));
+  RGF_CUDA(cudaMemsetAsync(c->info.p, 0, sizeof(DInfo) * nen, st));
+  RGF_CUDA(cudaMemsetAsync(c->queue.p, 0, sizeof(int32_t), st));
+  const int nb = (int)nm;
+  int grid = std::max(1, c->sm_count * fp64_blocks_per_sm(nb));
+  if ((int64_t)grid > nen) grid = (int)nen;
+  const int64_t slot = slot_elems_for(nm, nx);
+  if ((rc = c->work.reserve(sizeof(double2) * (size_t)slot * grid))) return rc;
+  KParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.o.eta_dev = c->opts.eta_dev;
+  p.o.eta_lead = c->opts.eta_lead;
+  p.o.boltz = c->opts.boltz;
+  p.o.sancho_tol = c->opts.sancho_tol;
+  p.o.sancho_nmax = c->opts.sancho_nmax;
+  p.o.consistent = c->opts.consistent;
+  p.o.want_T = 1;
+  p.devs = (const DDev*)c->devs.p;
+  p.n_tasks = nen;
+  p.queue = (int32_t*)c->queue.p;
+  p.work = (double2*)c->work.p;
+  p.slot_elems = slot;
+  p.nx_max = nx;
+  p.nb = nb;
+  p.info = (DInfo*)c->info.p;
+  p.adj = (const DAdj*)tb;
+  RGF_CUDA(cudaEventRecord(c->ev0, st));
+  cudaError_t e = launch_fp64(p, grid, st);
+  if (e != cudaSuccess) return fail(RGF_E_CUDA, "adjoint launch failed: %s", cudaGetErrorString(e));
+  c->stats.launches++;
+  RGF_CUDA(cudaEventRecord(c->ev1, st));
+  // current derivatives: weighted energy sums on the device (fixed order)
+  std::vector<double> w;
+  if (dIdV || dIds) {
+    const double kE0 = 1.6022e-19, kHbar = 1.0546e-34, kTpi = 3.14159265359 * 2.0;
+    const double dE = E[1] - E[0];
+    w.resize(nen);
+    for (int64_t k = 0; k < nen; k++) {
+      const double fl = 1.0 / (1.0 + std::exp((E[k] - v->mu[0]) / (c->opts.boltz * v->temp[0])));
+      const double fr = 1.0 / (1.0 + std::exp((E[k] - v->mu[1]) / (c->opts.boltz * v->temp[1])));
+      w[k] = (fl - fr) * dE * kE0 / kTpi / kHbar * kE0 * spindeg;
+    }
+  }
+  for (const auto& sgm : sg.segs)
+    if (sgm.copy_out)
+      RGF_CUDA(cudaMemcpyAsync(const_cast<char*>(sgm.host), sbase + sgm.off, sgm.bytes, cudaMemcpyDeviceToHost, st));
+  std::vector<double> hgrad;
+  std::vector<double> hds;
+  if (dIdV || dIds) {
+    hgrad.resize((size_t)nen * nx);
+    hds.resize(nen);
+    RGF_CUDA(cudaMemcpyAsync(hgrad.data(), dT_d, sizeof(double) * nen * nx, cudaMemcpyDeviceToHost, st));
+    RGF_CUDA(cudaMemcpyAsync(hds.data(), ds_d, sizeof(double) * nen, cudaMemcpyDeviceToHost, st));
+  }
+  std::vector<DInfo> hinfo(nen);
+  RGF_CUDA(cudaMemcpyAsync(hinfo.data(), c->info.p, sizeof(DInfo) * nen, cudaMemcpyDeviceToHost, st));
+  RGF_CUDA(cudaStreamSynchronize(st));
+  float kms = 0.0f;
+  RGF_CUDA(cudaEventElapsedTime(&kms, c->ev0, c->ev1));
+  c->stats.last_kernel_ms = kms;
+  c->stats.last_tasks = nen;
+  double flops = 0.0;
+  int worst = 0;
+  for (int64_t k = 0; k < nen; k++) {
+    worst |= hinfo[k].status;
+    flops += 8.0 * (double)nm * nm * nm * (double)(hinfo[k].n_gemm + hinfo[k].n_inv);
+  }
+  c->stats.last_flops = flops;
+  // energy sums in a fixed order (energies outermost, as the reference's loops)
+  if (dIdV) {
+    for (int64_t l = 0; l < nx; l++) dIdV[l] = 0.0;
+    for (int64_t k = 0; k < nen; k++)
+      for (int64_t l = 0; l < nx; l++) dIdV[l] += w[k] * hgrad[(size_t)k * nx + l];
+  }
+  if (dIds) {
+    *dIds = 0.0;
+    for (int64_t k = 0; k < nen; k++) *dIds += w[k] * hds[k];
+  }
+  if (info) std::memcpy(info, hinfo.data(), sizeof(DInfo) * nen);
   if (worst & RGF_ST_BAD_TASK) return fail(RGF_E_ARG, "a task was rejected on the device");
   return worst ? RGF_E_STATUS : RGF_OK;
 }

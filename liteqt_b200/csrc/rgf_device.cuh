@@ -84,6 +84,31 @@ __device__ __forceinline__ void for_each_elem(int n, F&& body) {
   }
 }
 
+// One complex 8x8x4 step on TM x TN subtiles: Cr += Ar Br - Ai Bi,
+// Ci += Ar Bi + Ai Br as four rounds of real DMMAs, each round over all
+// subtiles, so that consecutive MMAs on one accumulator are TM*TN apart.
+template <int TM, int TN>
+__device__ __forceinline__ void cmma_step(double (&cr)[TM][TN][2], double (&ci)[TM][TN][2],
+                                          const double2 (&av)[TM], const double2 (&bv)[TN],
+                                          double a_sg, double b_sg) {
+#pragma unroll
+  for (int a = 0; a < TM; a++)
+#pragma unroll
+    for (int b = 0; b < TN; b++) dmma884(cr[a][b][0], cr[a][b][1], av[a].x, bv[b].x);
+#pragma unroll
+  for (int a = 0; a < TM; a++)
+#pragma unroll
+    for (int b = 0; b < TN; b++) dmma884(ci[a][b][0], ci[a][b][1], av[a].x, bv[b].y * b_sg);
+#pragma unroll
+  for (int a = 0; a < TM; a++)
+#pragma unroll
+    for (int b = 0; b < TN; b++) dmma884(cr[a][b][0], cr[a][b][1], -av[a].y * a_sg, bv[b].y * b_sg);
+#pragma unroll
+  for (int a = 0; a < TM; a++)
+#pragma unroll
+    for (int b = 0; b < TN; b++) dmma884(ci[a][b][0], ci[a][b][1], av[a].y * a_sg, bv[b].x);
+}
+
 // ---------------------------------------------------------------- GEMM
 // C = op(A) * op(B) for n x n complex blocks, op = identity or conjugate
 // transpose (cA / cB).  The result is not stored: epi(i, j, value) is called
@@ -120,18 +145,7 @@ __device__ __forceinline__ void cgemm(int n, const double2* A, bool cA, const do
       for (int a = 0; a < TM; a++) av[a] = Ap[a][k0 * a_sk];
 #pragma unroll
       for (int b = 0; b < TN; b++) bv[b] = Bp[b][k0 * b_sk];
-#pragma unroll
-      for (int a = 0; a < TM; a++) {
-        const double ar = av[a].x, ai = av[a].y * a_sg;
-#pragma unroll
-        for (int b = 0; b < TN; b++) {
-          const double br = bv[b].x, bi = bv[b].y * b_sg;
-          dmma884(cr[a][b][0], cr[a][b][1], ar, br);
-          dmma884(cr[a][b][0], cr[a][b][1], -ai, bi);
-          dmma884(ci[a][b][0], ci[a][b][1], ar, bi);
-          dmma884(ci[a][b][0], ci[a][b][1], ai, br);
-        }
-      }
+      cmma_step<TM, TN>(cr, ci, av, bv, a_sg, b_sg);
     }
 #pragma unroll
     for (int a = 0; a < TM; a++)
@@ -144,12 +158,14 @@ __device__ __forceinline__ void cgemm(int n, const double2* A, bool cA, const do
 }
 
 // ---------------------------------------------------------------- inverse
+// Pivot bookkeeping of the inverse (the row / column vectors of the current
+// elimination step live in dynamic shared memory, see gj_invert).
 struct SmemInv {
-  double2 rowk[kMaxNb];
-  double2 fcol[kMaxNb];
-  int perm[kMaxNb];
-  int colsrc[kMaxNb];
+  int16_t perm[kMaxNb];
+  int16_t colsrc[kMaxNb];
+  int16_t rmap[kMaxNb];  // row map of the current panel (outside the GEMM staging area)
   double2 pivval;
+  double2 akc;  // the pivot column's entry in row k before the interchange
   int piv;
   int singular;
 };
@@ -161,7 +177,9 @@ struct SmemInv {
 // result the zero block (the reference's `invert` fallback,
 // green_rgf.f90:4429-4437) and the return value 1.
 // Preconditions: X holds the matrix and is visible to all threads.
-__device__ __noinline__ static int gj_invert(int n, double2* X, double2* dst, double2* dst2, SmemInv& s) {
+// rowk, fcol: shared scratch of n complex values each.
+__device__ __noinline__ static int gj_invert(int n, double2* X, double2* dst, double2* dst2, SmemInv& s,
+                                             double2* rowk, double2* fcol) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s.singular = 0;
   for (int k = 0; k < n; k++) {
@@ -181,7 +199,7 @@ __device__ __noinline__ static int gj_invert(int n, double2* X, double2* dst, do
       if (lane == 0) {
         s.piv = bi;
         s.pivval = X[bi + k * n];
-        s.perm[k] = bi;
+        s.perm[k] = (int16_t)bi;
         if (best == 0.0) s.singular = 1;
       }
     }
@@ -196,17 +214,17 @@ __device__ __noinline__ static int gj_invert(int n, double2* X, double2* dst, do
       if (p != k) X[p + j * n] = a;
       const double2 r = (j == k) ? pinv : cmul(b, pinv);
       X[k + j * n] = r;
-      s.rowk[j] = r;
+      rowk[j] = r;
     }
     __syncthreads();
-    for (int i = tid; i < n; i += kThreads) s.fcol[i] = (i == k) ? czero() : X[i + k * n];
+    for (int i = tid; i < n; i += kThreads) fcol[i] = (i == k) ? czero() : X[i + k * n];
     __syncthreads();
     // X[i][j] -= f_i * rowk[j] for i != k, with X[i][k] treated as 0
     for_each_elem(n, [&](int i, int j, int idx) {
       if (i == k) return;
-      const double2 f = s.fcol[i];
+      const double2 f = fcol[i];
       const double2 x = (j == k) ? czero() : X[idx];
-      const double2 r = s.rowk[j];
+      const double2 r = rowk[j];
       X[idx] = make_double2(x.x - (f.x * r.x - f.y * r.y), x.y - (f.x * r.y + f.y * r.x));
     });
     __syncthreads();
@@ -221,10 +239,10 @@ __device__ __noinline__ static int gj_invert(int n, double2* X, double2* dst, do
     return 1;
   }
   if (tid == 0) {
-    for (int j = 0; j < n; j++) s.colsrc[j] = j;
+    for (int j = 0; j < n; j++) s.colsrc[j] = (int16_t)j;
     for (int k = n - 1; k >= 0; k--) {
       const int q = s.perm[k];
-      if (q != k) { const int tmp = s.colsrc[k]; s.colsrc[k] = s.colsrc[q]; s.colsrc[q] = tmp; }
+      if (q != k) { const int16_t tmp = s.colsrc[k]; s.colsrc[k] = s.colsrc[q]; s.colsrc[q] = tmp; }
     }
   }
   __syncthreads();

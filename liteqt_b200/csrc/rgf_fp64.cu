@@ -58,16 +58,22 @@ constexpr int kSmemXMaxNb = 64;  // generic path: inverse workspace in shared me
 template <int TM, int TN>
 struct GenericOps {
   static constexpr int kMinBlocks = 2;
-  static size_t smem_bytes(int nb) { return nb <= kSmemXMaxNb ? (size_t)nb * nb * sizeof(double2) : 0; }
+  static size_t smem_bytes(int nb) {
+    return ((nb <= kSmemXMaxNb ? (size_t)nb * nb : 0) + 2 * (size_t)nb) * sizeof(double2);
+  }
   SmemInv& inv;
   double2* X;
+  double2* rowk;
   __device__ GenericOps(SmemInv& i, double2* dyn, double2* slot_inv, double2*, int n)
-      : inv(i), X(n <= kSmemXMaxNb ? dyn : slot_inv) {}
+      : inv(i), X(n <= kSmemXMaxNb ? dyn : slot_inv),
+        rowk(dyn + (n <= kSmemXMaxNb ? (size_t)n * n : 0)) {}
   template <class Epi>
   __device__ void gemm(int n, const double2* A, bool cA, const double2* B, bool cB, Epi&& epi) {
     cgemm<TM, TN>(n, A, cA, B, cB, epi);
   }
-  __device__ int invert(int n, double2* dst, double2* dst2) { return gj_invert(n, X, dst, dst2, inv); }
+  __device__ int invert(int n, double2* dst, double2* dst2) {
+    return gj_invert(n, X, dst, dst2, inv, rowk, rowk + n);
+  }
 };
 
 // nb = 32, 64, 128, 256: shared-memory-staged GEMM; inverse in shared memory
@@ -87,8 +93,9 @@ struct StagedOps {
     gemm_staged<NB>(NB, NB, NB, A, NB, cA, B, NB, cB, dyn, epi);
   }
   __device__ int invert(int, double2* dst, double2* dst2) {
-    if constexpr (StagedCfg<NB>::SMEM_INV) return gj_invert(NB, X, dst, dst2, inv);
-    else return gj_invert_blocked<NB>(X, dst, dst2, Rt, dyn, dyn, inv);
+    if constexpr (StagedCfg<NB>::SMEM_INV)
+      return gj_invert(NB, X, dst, dst2, inv, dyn + (size_t)NB * NB, dyn + (size_t)NB * NB + NB);
+    else return gj_invert_blocked<NB>(X, Rt, dst, dst2, dyn, dyn, inv);
   }
 };
 
@@ -465,6 +472,259 @@ struct Solver {
     __syncthreads();
   }
 
+
+  // ------------------------------------------------------------------ adjoint
+  // Stein doubling for X = Q + P X R with Q = -g g, P = g H^H, R = H g: the
+  // energy derivative of a Sancho-Rubio surface Green's function g that
+  // satisfies g = (z - H00 - H^H g H)^-1 (H = the coupling argument).
+  // Result in out.  Uses temps T_F1..T_F4, T_Q1..T_Q3.
+  // conj_h: the coupling argument is Hc^H (left lead).
+  __device__ void dg_dE(const double2* g, const double2* Hc, bool conj_h, double2* out) {
+    const int nn = n;
+    double2 *P = tmp(T_Q1), *R = tmp(T_Q2), *P2 = tmp(T_Q3), *R2 = tmp(T_F4), *Y = tmp(T_F3);
+    gemm_store(g, false, Hc, !conj_h, P);                            // P = g H^H
+    gemm_store(Hc, conj_h, g, false, R);                             // R = H g
+    gemm(g, false, g, false, [&](int i, int j, double2 v) { out[i + j * nn] = make_double2(-v.x, -v.y); });
+    for (int it = 0; it < 4 * o.sancho_nmax; it++) {
+      gemm_store(P, false, out, false, Y);                           // P X
+      double dsum = 0.0, xsum = 0.0;
+      gemm(Y, false, R, false, [&](int i, int j, double2 v) {        // X += P X R
+        const int idx = i + j * nn;
+        const double2 x = cadd(out[idx], v);
+        out[idx] = x;
+        dsum += fabs(v.x) + fabs(v.y);
+        xsum += fabs(x.x) + fabs(x.y);
+      });
+      const double2 sums = block_sum2(make_double2(dsum, xsum), sm.red);
+      if (!(sums.x > 1e-17 * sums.y)) break;
+      gemm_store(P, false, P, false, P2);
+      gemm_store(R, false, R, false, R2);
+      double2* t1 = P; P = P2; P2 = t1;
+      double2* t2 = R; R = R2; R2 = t2;
+    }
+  }
+
+  // T(E), dT/dV_l (l = 0..nx-1) and dT/ds for one energy of a ballistic
+  // device (no scattering self-energy).  V_l adds V_l * I to H_ll; the two
+  // end blocks also shift their semi-infinite leads (the leads are the
+  // continuation of Hii(:,:,1) / Hii(:,:,nx), as in green_RGF_RS), which
+  // enters through dSigma/dE.  s scales the interior couplings H1i(:,:,m),
+  // m = 2..nx-1 (1-based).  Reverse sweep with sqrt(nx) checkpoints of the
+  // left-connected g_l and of the running column c_l = g^L_{l,1}.
+  __device__ void run_adjoint(const DAdj& tk, const DDev& dv, DInfo* info) {
+    const int nn = n;
+    const double E = tk.E;
+    const double2 z = make_double2(E, o.eta_dev);
+    const double2* Hii = dv.Hii;
+    const double2* H1i = dv.H1i;
+    auto blk = [&](const double2* base, int l) { return base + (size_t)l * n2; };
+    const int nl = nx - 1;                     // blocks of the left-connected chain: 0..nx-2
+    int S = nl;                                // segment length
+    if (nl > 16) { S = 1; while (S * S < nl) S++; }
+    const int nseg = (nl + S - 1) / S;
+    // storage in the Gl / Gln regions: [checkpoints (nseg) | segment (S)]
+    const int cko = nseg > 1 ? nseg : 0;
+    auto ckg = [&](int q) { return Gl(q); };
+    auto ckc = [&](int q) { return Gln(q); };
+    auto sgg = [&](int q) { return Gl(cko + q); };
+    auto sgc = [&](int q) { return Gln(cko + q); };
+    double2* H00 = tmp(T_H00);
+    // ---- left lead
+    for_each_elem(n, [&](int, int, int idx) { H00[idx] = Hii[idx]; });
+    __syncthreads();
+    const int itL = sancho(E, H00, blk(H1i, 0), true, tmp(T_GS));
+    double2* sigmal = tmp(T_SIGL);
+    gemm_store(blk(H1i, 0), false, tmp(T_GS), false, tmp(T_F1));
+    gemm_store(tmp(T_F1), false, blk(H1i, 0), true, sigmal);
+    double2* dSL = tmp(T_Q4);                                        // -dSigma_L/dE
+    dg_dE(tmp(T_GS), blk(H1i, 0), true, tmp(T_F2));                 // coupling argument H1i(1)^H
+    gemm_store(blk(H1i, 0), false, tmp(T_F2), false, tmp(T_F1));
+    gemm(tmp(T_F1), false, blk(H1i, 0), true, [&](int i, int j, double2 v) {
+      dSL[i + j * nn] = make_double2(-v.x, -v.y);
+    });
+    // ---- forward sweep with checkpoints
+    double2* gprev = tmp(T_GN1A);  // rolling g_{l-1}, c_{l-1} when checkpointing
+    double2* cprev = tmp(T_GN1B);
+    auto store_state = [&](int l, const double2* g, const double2* c) {
+      if (nseg == 1) {
+        if (g != sgg(l)) for_each_elem(n, [&](int, int, int idx) { sgg(l)[idx] = g[idx]; sgc(l)[idx] = c[idx]; });
+        else for_each_elem(n, [&](int, int, int idx) { sgc(l)[idx] = c[idx]; });
+        __syncthreads();
+      } else if (l % S == 0) {
+        for_each_elem(n, [&](int, int, int idx) { ckg(l / S)[idx] = g[idx]; ckc(l / S)[idx] = c[idx]; });
+        __syncthreads();
+      }
+    };
+    // g_0
+    for_each_elem(n, [&](int i, int j, int idx) {
+      const double2 h = Hii[idx];
+      const double2 a = (i == j) ? make_double2(z.x - h.x, z.y - h.y) : make_double2(-h.x, -h.y);
+      X[idx] = csub(a, sigmal[idx]);
+    });
+    __syncthreads();
+    double2* g0 = nseg == 1 ? sgg(0) : gprev;
+    invert_X(g0);
+    store_state(0, g0, g0);
+    if (nseg > 1) for_each_elem(n, [&](int, int, int idx) { cprev[idx] = g0[idx]; });
+    __syncthreads();
+    const double2* gl = g0;
+    const double2* cl = nseg == 1 ? sgc(0) : cprev;
+    // forward step from (g_{l-1}, c_{l-1}) to (g_l, c_l) into (gout, cout)
+    auto fwd_step = [&](int l, const double2* gp, const double2* cp, double2* gout, double2* cout) {
+      const double2* Hc = blk(H1i, l);
+      const double2* Hl = blk(Hii, l);
+      gemm_store(Hc, false, gp, false, tmp(T_F1));
+      gemm(tmp(T_F1), false, Hc, true, [&](int i, int j, double2 v) {
+        const int idx = i + j * nn;
+        const double2 h = Hl[idx];
+        const double2 a = (i == j) ? make_double2(z.x - h.x, z.y - h.y) : make_double2(-h.x, -h.y);
+        X[idx] = csub(a, v);
+      });
+      invert_X(gout);
+      gemm_store(Hc, false, cp, false, tmp(T_F1));
+      gemm_store(gout, false, tmp(T_F1), false, cout);               // c_l = g_l H_{l,l-1} c_{l-1}
+    };
+    for (int l = 1; l <= nx - 2; l++) {
+      if (nseg == 1) {
+        fwd_step(l, sgg(l - 1), sgc(l - 1), sgg(l), sgc(l));
+        gl = sgg(l);
+        cl = sgc(l);
+      } else {
+        double2* gn = tmp(T_G00A);
+        double2* cn = tmp(T_G00B);
+        fwd_step(l, gprev, cprev, gn, cn);
+        store_state(l, gn, cn);
+        for_each_elem(n, [&](int, int, int idx) { gprev[idx] = gn[idx]; cprev[idx] = cn[idx]; });
+        __syncthreads();
+        gl = gprev;
+        cl = cprev;
+      }
+    }
+    // ---- right lead, G_NN, X = G_{N1}, T, W
+    const double2* Hr = blk(H1i, nx - 1);
+    for_each_elem(n, [&](int, int, int idx) { H00[idx] = blk(Hii, nx - 1)[idx]; });
+    __syncthreads();
+    const int itR = sancho(E, H00, Hr, false, tmp(T_GS));
+    double2* sigmar = tmp(T_SIGR);
+    gemm_store(Hr, true, tmp(T_GS), false, tmp(T_F1));
+    gemm_store(tmp(T_F1), false, Hr, false, sigmar);
+    double2* dSR = tmp(T_R5);                                        // -dSigma_R/dE
+    dg_dE(tmp(T_GS), Hr, false, tmp(T_F2));
+    gemm_store(Hr, true, tmp(T_F2), false, tmp(T_F1));
+    gemm(tmp(T_F1), false, Hr, false, [&](int i, int j, double2 v) { dSR[i + j * nn] = make_double2(-v.x, -v.y); });
+    gemm_store(Hr, false, gl, false, tmp(T_F1));
+    gemm(tmp(T_F1), false, Hr, true, [&](int i, int j, double2 v) {
+      const int idx = i + j * nn;
+      const double2 h = H00[idx];
+      double2 a = (i == j) ? make_double2(z.x - h.x, z.y - h.y) : make_double2(-h.x, -h.y);
+      a = csub(a, sigmar[idx]);
+      X[idx] = csub(a, v);
+    });
+    double2* GNN = tmp(T_G00A);  // gn of the checkpointed forward loop is dead here
+    invert_X(GNN);
+    double2* XN1 = tmp(T_X2);
+    gemm_store(Hr, false, cl, false, tmp(T_F1));
+    gemm_store(GNN, false, tmp(T_F1), false, XN1);                    // X = G_NN H c_{N-2}
+    double2* gamL = tmp(T_GAML);
+    double2* gamR = tmp(T_GAMR);
+    double2* dgL = tmp(T_H10B);
+    double2* dgR = tmp(T_H01A);
+    for_each_elem(n, [&](int i, int j, int idx) {
+      const double2 dl = csub(sigmal[idx], cconj(sigmal[j + i * nn]));
+      const double2 dr = csub(sigmar[idx], cconj(sigmar[j + i * nn]));
+      gamL[idx] = make_double2(-dl.y, dl.x);
+      gamR[idx] = make_double2(-dr.y, dr.x);
+      const double2 el = csub(dSL[idx], cconj(dSL[j + i * nn]));     // i (S' - S'^H)
+      const double2 er = csub(dSR[idx], cconj(dSR[j + i * nn]));
+      dgL[idx] = make_double2(-el.y, el.x);
+      dgR[idx] = make_double2(-er.y, er.x);
+    });
+    __syncthreads();
+    double2* W = tmp(T_SIG);
+    gemm_store(gamL, false, XN1, true, tmp(T_F1));                    // Gamma_L X^H
+    gemm_store(tmp(T_F1), false, gamR, false, W);                     // W = Gamma_L X^H Gamma_R
+    double2* XGX = tmp(T_F3);
+    gemm_store(gamR, false, XN1, false, tmp(T_F1));                   // Gamma_R X
+    gemm_store(XN1, false, gamL, false, tmp(T_F2));                   // X Gamma_L
+    gemm_store(tmp(T_F2), false, XN1, true, XGX);                     // X Gamma_L X^H
+    const double T = trace_prod(n, gamR, XGX, sm.red).x;
+    // lead terms: Tr[Gamma_R X dGamma_L X^H] and Tr[dGamma_R X Gamma_L X^H]
+    gemm_store(tmp(T_F1), false, dgL, false, tmp(T_F2));              // Gamma_R X dGamma_L
+    gemm_store(tmp(T_F2), false, XN1, true, tmp(T_F4));
+    double leadL = 0.0, leadR = 0.0;
+    {
+      double acc = 0.0;
+      for (int i = threadIdx.x; i < n; i += kThreads) acc += tmp(T_F4)[i + i * nn].x;
+      leadL = block_sum2(make_double2(acc, 0.0), sm.red).x;
+    }
+    leadR = trace_prod(n, dgR, XGX, sm.red).x;
+    // ---- reverse sweep
+    double2 *r1 = tmp(T_Q1), *r0 = tmp(T_Q2), *k1 = tmp(T_Q3), *k0 = tmp(T_GNA);
+    double2 *y1 = tmp(T_H01B), *y0 = tmp(T_HSS), *tA = tmp(T_F1), *tB = tmp(T_F2);
+    // l = nx-1: r = G_NN, k = X
+    for_each_elem(n, [&](int, int, int idx) { r1[idx] = GNN[idx]; k1[idx] = XN1[idx]; });
+    __syncthreads();
+    gemm_store(W, false, r1, false, y1);                              // Y = W r
+    double gN = 2.0 * trace_prod(n, k1, y1, sm.red).x;
+    // right lead term 2 Re Tr[W r_{N-1} S'_R X]
+    gemm_store(y1, false, dSR, false, tA);
+    gN += 2.0 * trace_prod(n, tA, XN1, sm.red).x + leadR;
+    if (threadIdx.x == 0) tk.dTdV[nx - 1] = gN;
+    double ds = 0.0;
+    for (int sg = nseg - 1; sg >= 0; sg--) {
+      const int l0 = sg * S, l1 = (l0 + S < nl) ? l0 + S : nl;
+      if (nseg > 1) {  // recompute the segment from its checkpoint
+        for_each_elem(n, [&](int, int, int idx) { sgg(0)[idx] = ckg(sg)[idx]; sgc(0)[idx] = ckc(sg)[idx]; });
+        __syncthreads();
+        for (int l = l0 + 1; l < l1; l++) fwd_step(l, sgg(l - 1 - l0), sgc(l - 1 - l0), sgg(l - l0), sgc(l - l0));
+      }
+      for (int l = l1 - 1; l >= l0; l--) {
+        const double2* g = sgg(l - l0);
+        const double2* c = sgc(l - l0);
+        const double2* Hn = blk(H1i, l + 1);                          // H_{l+1,l}
+        gemm_store(r1, false, Hn, false, tA);
+        gemm_store(tA, false, g, false, r0);                          // r_l = r_{l+1} H_{l+1,l} g_l
+        gemm_store(g, false, Hn, true, tA);
+        gemm(tA, false, k1, false, [&](int i, int j, double2 v) {     // k_l = c_l + g_l H^H k_{l+1}
+          const int idx = i + j * nn;
+          k0[idx] = cadd(c[idx], v);
+        });
+        gemm_store(W, false, r0, false, y0);                          // Y_l = W r_l
+        double gl_ = 2.0 * trace_prod(n, k0, y0, sm.red).x;
+        if (l == 0) {  // left lead: 2 Re Tr[W X S'_L k_0] + Tr[Gamma_R X dGamma_L X^H]
+          gemm_store(W, false, XN1, false, tA);
+          gemm_store(tA, false, dSL, false, tB);
+          gl_ += 2.0 * trace_prod(n, tB, k0, sm.red).x + leadL;
+        }
+        if (threadIdx.x == 0) tk.dTdV[l] = gl_;
+        const int m = l + 1;                                          // coupling H_{m,m-1}
+        if (m >= 1 && m <= nx - 2) {
+          gemm_store(y1, false, Hn, false, tA);                       // Y_m H_{m,m-1}
+          double t1 = trace_prod(n, tA, k0, sm.red).x;
+          gemm_store(y0, false, Hn, true, tB);                        // Y_{m-1} H^H
+          t1 += trace_prod(n, tB, k1, sm.red).x;
+          ds += 2.0 * t1;
+        }
+        double2* t;
+        t = r1; r1 = r0; r0 = t;
+        t = k1; k1 = k0; k0 = t;
+        t = y1; y1 = y0; y0 = t;
+      }
+    }
+    if (threadIdx.x == 0) {
+      if (tk.T) *tk.T = T;
+      if (tk.dTds) *tk.dTds = ds;
+    }
+    if (info && threadIdx.x == 0) {
+      info->status = status;
+      info->sancho_iters_left = itL;
+      info->sancho_iters_right = itR;
+      info->n_gemm = n_gemm;
+      info->n_inv = n_inv;
+    }
+    __syncthreads();
+  }
+
   __device__ double* blk2(double* base, int l) const { return base + (size_t)l * n2; }
 };
 
@@ -480,9 +740,24 @@ __global__ void __launch_bounds__(kThreads, 2) rgf_fp64_kernel(KParams p) {
     __syncthreads();
     if (q >= p.n_tasks) break;
     const int64_t t = p.order ? p.order[q] : q;
+    DInfo* info = p.info ? p.info + t : nullptr;
+    if (p.adj) {
+      const DAdj ak = p.adj[t];
+      const DDev dva = p.devs[ak.dev];
+      if ((int)dva.nm != p.nb || dva.nx < 2 || dva.nx > p.nx_max) {
+        if (info && threadIdx.x == 0) info->status = RGF_ST_BAD_TASK;
+        continue;
+      }
+      const int na = (int)dva.nm;
+      const size_t na2 = (size_t)na * na;
+      double2* temps_a = slot + 2 * p.nx_max * na2;
+      Ops opsa(sm.inv, dyn_smem, temps_a + (size_t)T_INV * na2, temps_a + (size_t)T_RT * na2, na);
+      Solver<Ops> sa(p.o, p.nx_max, sm, opsa, slot, na, (int)dva.nx);
+      sa.run_adjoint(ak, dva, info);
+      continue;
+    }
     const DTask tk = p.tasks[t];
     const DDev dv = p.devs[tk.dev];
-    DInfo* info = p.info ? p.info + t : nullptr;
     if ((int)dv.nm != p.nb || dv.nx < 2 || dv.nx > p.nx_max) {
       if (info && threadIdx.x == 0) info->status = RGF_ST_BAD_TASK;
       continue;

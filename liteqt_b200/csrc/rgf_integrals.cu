@@ -58,6 +58,39 @@ __global__ void n_electron_kernel(const double2* Gl, const double2* Gg, int64_t 
   }
 }
 
+// calc_block_current (src/green_rgf.f90:4602-4640): one thread per output
+// element (io, jo, l); energies summed in the reference's order.  The last
+// sub-block of a block repeats the previous one (ib = ns - 1), as the
+// reference's stale matrix does; ns = 1 gives zeros.
+__global__ void block_current_kernel(const double2* H, const double2* G, int64_t nen, const double* en,
+                                     double scale, int64_t nb, int64_t ns, int64_t nm, int64_t nx,
+                                     double* tot_cur, double* tot_ecur, double* jdens) {
+  const int64_t b2 = nb * nb, nl = nx * ns;
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= b2 * nl) return;
+  const int64_t kk = q % b2, l = q / b2;
+  const int64_t io = kk % nb, jo = kk / nb;
+  const int64_t ix = l / ns, ibm = l % ns;             // 0-based sub-block index
+  const int64_t ib = (ibm == ns - 1) ? ns - 2 : ibm;   // last sub-block repeats the previous one
+  const size_t n2 = (size_t)nm * nm;
+  double tc = 0.0, te = 0.0;
+  for (int64_t ie = 0; ie < nen; ie++) {
+    double v = 0.0;
+    if (ib >= 0) {
+      const size_t i = io + ib * nb, j = jo + (ib + 1) * nb;
+      const double2* Hx = H + ix * n2;
+      const double2* Gx = G + ix * n2 + (size_t)ie * nx * n2;
+      const double2 b = rgf::csub(rgf::cmul(Hx[i + j * nm], Gx[j + i * nm]), rgf::cmul(Hx[j + i * nm], Gx[i + j * nm]));
+      v = b.x * scale;
+    }
+    if (jdens) jdens[q + (size_t)ie * nl * b2] = v;
+    te += en[ie] * v;
+    tc += v;
+  }
+  tot_cur[q] = tc;
+  if (tot_ecur) tot_ecur[q] = te;
+}
+
 bool is_dev(const void* p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -97,6 +130,33 @@ extern "C" int rgf_terminal_current(rgf_ctx* ctx, const double* tr, int64_t nen,
   if (e != cudaSuccess) return RGF_E_CUDA;
   *current = s * dE * kE0 / kTpi / kHbar * kE0 * spindeg / (double)nk;
   return RGF_OK;
+}
+
+extern "C" int rgf_calc_block_current(rgf_ctx* ctx, const rgf_c16* H, const rgf_c16* G_lesser,
+                                      int64_t nen, const double* E, double spindeg, int64_t nb,
+                                      int64_t ns, int64_t nm, int64_t nx, double* tot_cur,
+                                      double* tot_ecur, double* jdens) {
+  if (!ctx || !H || !G_lesser || !E || !tot_cur) return RGF_E_ARG;
+  if (nen < 2 || nb < 1 || ns < 1 || nm != nb * ns || nx < 1) return RGF_E_ARG;
+  const size_t n2 = (size_t)nm * nm;
+  In h(H, sizeof(rgf_c16) * n2 * nx), g(G_lesser, sizeof(rgf_c16) * n2 * nx * nen), e(E, sizeof(double) * nen);
+  if (h.err || g.err || e.err) return RGF_E_CUDA;
+  const size_t nout = (size_t)nb * nb * nx * ns;
+  double* d_out = nullptr;
+  const size_t jbytes = jdens ? sizeof(double) * nout * nen : 0;
+  if (cudaMalloc(&d_out, sizeof(double) * 2 * nout + jbytes) != cudaSuccess) return RGF_E_NOMEM;
+  const double kTpiLocal = 6.28318530718;  // calc_block_current's own tpi (green_rgf.f90:4614)
+  const double scale = (E[1] - E[0]) * kE0 / kTpiLocal / kHbar * kE0 * spindeg;
+  const int thr = 256;
+  const unsigned blocks = (unsigned)((nout + thr - 1) / thr);
+  block_current_kernel<<<blocks, thr>>>((const double2*)h.d, (const double2*)g.d, nen, (const double*)e.d,
+                                        scale, nb, ns, nm, nx, d_out, d_out + nout,
+                                        jdens ? d_out + 2 * nout : nullptr);
+  cudaError_t err = cudaMemcpy(tot_cur, d_out, sizeof(double) * nout, cudaMemcpyDeviceToHost);
+  if (err == cudaSuccess && tot_ecur) err = cudaMemcpy(tot_ecur, d_out + nout, sizeof(double) * nout, cudaMemcpyDeviceToHost);
+  if (err == cudaSuccess && jdens) err = cudaMemcpy(jdens, d_out + 2 * nout, jbytes, cudaMemcpyDeviceToHost);
+  cudaFree(d_out);
+  return err == cudaSuccess ? RGF_OK : RGF_E_CUDA;
 }
 
 extern "C" int rgf_calc_n_electron(rgf_ctx* ctx, const rgf_c16* G_lesser, const rgf_c16* G_greater,

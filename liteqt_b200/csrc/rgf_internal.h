@@ -61,6 +61,17 @@ struct DInfo {
 };
 static_assert(sizeof(DInfo) == sizeof(rgf_task_info), "DInfo layout");
 
+// One adjoint task (ballistic): T(E), dT/dV_l for every block, dT/ds for the
+// interior coupling scale.
+struct DAdj {
+  int32_t dev;
+  int32_t pad;
+  double E;
+  double* T;       // scalar
+  double* dTdV;    // nx values
+  double* dTds;    // scalar
+};
+
 struct KParams {
   KOpts o;
   const DDev* devs;
@@ -74,6 +85,7 @@ struct KParams {
   int32_t nb;              // block size of every task in this launch
   int32_t pad;
   DInfo* info;             // per task
+  const DAdj* adj;         // non-null: run the adjoint instead of the drop-in solve
 };
 
 // Number of named scratch blocks in a slot besides Gl[nx_max], Gln[nx_max].

@@ -45,7 +45,8 @@ EXPORTS = (
     "rgf_opts_default", "rgf_ctx_create", "rgf_ctx_destroy", "rgf_ctx_set_opts",
     "rgf_solve_batch", "rgf_green_rgf_rs", "rgf_rgf_g", "rgf_solve_energies",
     "rgf_terminal_current", "rgf_calc_n_electron", "rgf_last_error", "rgf_version",
-    "rgf_ctx_get_stats",
+    "rgf_ctx_get_stats", "rgf_adjoint_energies", "rgf_solve_energies_noalloc",
+    "rgf_noalloc_last_error", "rgf_calc_block_current",
 )
 
 
@@ -123,11 +124,16 @@ def load(path: str = LIB_PATH):
     L.rgf_calc_n_electron.argtypes = [P, P, P, ctypes.c_int64, P, ctypes.c_int64, ctypes.c_int64,
                                       ctypes.c_int64, P, P, P]
     L.rgf_ctx_get_stats.argtypes = [P, ctypes.POINTER(c_stats)]
+    L.rgf_calc_block_current.argtypes = [P, P, P, ctypes.c_int64, P, ctypes.c_double, ctypes.c_int64,
+                                         ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, P, P, P]
+    L.rgf_calc_block_current.restype = ctypes.c_int
+    L.rgf_adjoint_energies.argtypes = [P, ctypes.POINTER(c_device), ctypes.c_int64, P, P, P, P,
+                                       ctypes.c_double, P, P, P, P]
     L.rgf_last_error.restype = ctypes.c_char_p
     L.rgf_version.restype = ctypes.c_char_p
     for name in ("rgf_ctx_create", "rgf_ctx_destroy", "rgf_ctx_set_opts", "rgf_solve_batch",
                  "rgf_green_rgf_rs", "rgf_rgf_g", "rgf_solve_energies", "rgf_terminal_current",
-                 "rgf_calc_n_electron", "rgf_ctx_get_stats"):
+                 "rgf_calc_n_electron", "rgf_ctx_get_stats", "rgf_adjoint_energies"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -249,6 +255,25 @@ class Context:
             _ptr(info), stream)
         return _check(rc, allow_status)
 
+    def adjoint_energies(self, Hii, H1i, E, mu, temp, *, T=None, dTdV=None, dTds=None,
+                         spindeg=1.0, want_current=True, info=None, stream=None, allow_status=True):
+        """rgf_adjoint_energies: T(E), dT/dV_l, dT/ds per energy and the current's
+        derivatives.  Returns (dIdV, dIds) (NumPy) when want_current."""
+        nx, nm = int(Hii.shape[0]), int(Hii.shape[1])
+        d = c_device()
+        d.nm, d.nx = nm, nx
+        d.Hii, d.H1i = _ptr(Hii), _ptr(H1i)
+        d.mu[0], d.mu[1] = float(mu[0]), float(mu[1])
+        d.temp[0], d.temp[1] = float(temp[0]), float(temp[1])
+        E = np.ascontiguousarray(E, np.float64)
+        dIdV = np.zeros(nx) if want_current else None
+        dIds = np.zeros(1) if want_current else None
+        rc = load().rgf_adjoint_energies(self.h, ctypes.byref(d), int(E.shape[0]), _ptr(E), _ptr(T),
+                                         _ptr(dTdV), _ptr(dTds), float(spindeg), _ptr(dIdV),
+                                         _ptr(dIds), _ptr(info), stream)
+        _check(rc, allow_status)
+        return (dIdV, float(dIds[0])) if want_current else None
+
     def solve_batch(self, devices, tasks, info=None, stream=None, allow_status=True):
         """rgf_solve_batch with ctypes c_device / c_task arrays."""
         nd, nt = len(devices), len(tasks)
@@ -262,6 +287,20 @@ class Context:
         _check(load().rgf_terminal_current(self.h, _ptr(tr), int(tr.shape[0]), float(dE),
                                            float(spindeg), int(nk), ctypes.addressof(out)))
         return out.value
+
+    def calc_block_current(self, H, G_lesser, E, spindeg, nb, ns, jdens=False):
+        """calc_block_current (green_rgf.f90:4602-4640).  H (nx, nm, nm), G_lesser
+        (nen, nx, nm, nm) Fortran block layouts.  Returns tot_cur, tot_ecur
+        (nx*ns, nb, nb) and jdens (nen, nx*ns, nb, nb) or None."""
+        nx, nm = int(H.shape[0]), int(H.shape[1])
+        nen = int(G_lesser.shape[0])
+        E = np.ascontiguousarray(E, np.float64)
+        tc = np.zeros((nx * ns, nb, nb))
+        te = np.zeros((nx * ns, nb, nb))
+        jd = np.zeros((nen, nx * ns, nb, nb)) if jdens else None
+        _check(load().rgf_calc_block_current(self.h, _ptr(H), _ptr(G_lesser), nen, _ptr(E), float(spindeg),
+                                             int(nb), int(ns), nm, nx, _ptr(tc), _ptr(te), _ptr(jd)))
+        return tc, te, jd
 
     def calc_n_electron(self, G_lesser, G_greater, E, midgap):
         """G arrays (nk, nen, nx, nm, nm): the Fortran (nm,nm,nx,nen,nk) layout."""

@@ -138,6 +138,10 @@ def lib():
         L.oracle_calc_n_electron.argtypes = [P, P, ctypes.c_int64, P, ctypes.c_int64,
                                              ctypes.c_int64, ctypes.c_int64, P, P, P]
         L.oracle_calc_n_electron.restype = None
+        L.oracle_calc_block_current.argtypes = [P, P, ctypes.c_int64, P, ctypes.c_double,
+                                                ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                                ctypes.c_int64, P, P, P]
+        L.oracle_calc_block_current.restype = None
         _lib = L
     return _lib
 
@@ -209,6 +213,23 @@ def calc_n_electron(G_lesser, G_greater, E, midgap):
     pe = np.zeros(nx)
     lib().oracle_calc_n_electron(_p(gl), _p(gg), nen, _p(E), nm, nk, nx, _p(ne), _p(pe), _p(midgap))
     return ne, pe
+
+
+def calc_block_current(H, G_lesser, E, spindeg, nb, ns, jdens=False):
+    """calc_block_current (green_rgf.f90:4602-4640).  H: (nx, nm, nm) and
+    G_lesser: (nen, nx, nm, nm), Fortran block layouts.  Returns tot_cur,
+    tot_ecur (nx*ns, nb, nb) and jdens (nen, nx*ns, nb, nb) or None."""
+    nx, nm, _ = H.shape
+    nen = G_lesser.shape[0]
+    Hc = np.ascontiguousarray(H, np.complex128)
+    Gc = np.ascontiguousarray(G_lesser, np.complex128)
+    E = np.ascontiguousarray(E, np.float64)
+    tc = np.zeros((nx * ns, nb, nb))
+    te = np.zeros((nx * ns, nb, nb))
+    jd = np.zeros((nen, nx * ns, nb, nb)) if jdens else None
+    lib().oracle_calc_block_current(_p(Hc), _p(Gc), nen, _p(E), float(spindeg), nb, ns, nm, nx,
+                                    _p(tc), _p(te), _p(jd))
+    return tc, te, jd
 
 
 def terminal_current(tr, dE, spindeg=1.0, nk=1):
@@ -387,3 +408,92 @@ def dense_green(Hb, H1b, E, sigmal, sigmar, eta_dev=0.0, sigr=None):
     M[:nm, :nm] += sigmal
     M[-nm:, -nm:] += sigmar
     return np.linalg.inv(complex(E, eta_dev) * np.eye(N) - M)
+
+
+# ---------------------------------------------------------------------------
+# Adjoint of T(E) (checker for rgf_adjoint_energies).  No counterpart in the
+# reference; T is the Caroli transmission of src/green.f90:2571-2580 and the
+# parameters are the per-block potential V_l (Hii(:,:,l) += V_l I, the end
+# blocks also shifting their leads, which the reference builds from
+# Hii(:,:,1) / Hii(:,:,nx)) and the interior coupling scale s
+# (H1i(:,:,m) *= s for m = 2..nx-1, 1-based).
+def _dgs_dE(g, H10, tol=1e-17, cap=400):
+    """dg/dE of g = (z - H00 - H10^H g H10)^-1 by doubling of the Stein
+    equation X = -g g + (g H10^H) X (H10 g)."""
+    P = g @ H10.conj().T
+    R = H10 @ g
+    X = -g @ g
+    for _ in range(cap):
+        D = P @ X @ R
+        X = X + D
+        if not np.sum(np.abs(D)) > tol * np.sum(np.abs(X)):
+            break
+        P = P @ P
+        R = R @ R
+    return X
+
+
+def adjoint_numpy(Hb, H1b, E, opts: Opts):
+    """Returns T, dT/dV (nx), dT/ds on mathematical blocks (ballistic)."""
+    H = lambda X: X.conj().T
+    nx, nm, _ = Hb.shape
+    I = np.eye(nm)
+    z = complex(E, opts.eta_dev)
+    gL, _, _, _ = sancho_numpy(E, Hb[0], H(H1b[0]), opts)
+    gR, _, _, _ = sancho_numpy(E, Hb[-1], H1b[-1], opts)
+    SL = H1b[0] @ gL @ H(H1b[0])
+    SR = H(H1b[-1]) @ gR @ H1b[-1]
+    SpL = -(H1b[0] @ _dgs_dE(gL, H(H1b[0])) @ H(H1b[0]))
+    SpR = -(H(H1b[-1]) @ _dgs_dE(gR, H1b[-1]) @ H1b[-1])
+    g = [None] * nx
+    c = [None] * nx
+    g[0] = np.linalg.inv(z * I - Hb[0] - SL)
+    c[0] = g[0]
+    for l in range(1, nx - 1):
+        g[l] = np.linalg.inv(z * I - Hb[l] - H1b[l] @ g[l - 1] @ H(H1b[l]))
+        c[l] = g[l] @ H1b[l] @ c[l - 1]
+    GNN = np.linalg.inv(z * I - Hb[-1] - SR - H1b[-1] @ g[nx - 2] @ H(H1b[-1]))
+    X = GNN @ H1b[-1] @ c[nx - 2]
+    GamL = 1j * (SL - H(SL))
+    GamR = 1j * (SR - H(SR))
+    T = float(np.real(np.trace(GamR @ X @ GamL @ H(X))))
+    W = GamL @ H(X) @ GamR
+    r = [None] * nx
+    k = [None] * nx
+    r[-1] = GNN
+    k[-1] = X
+    for l in range(nx - 2, -1, -1):
+        r[l] = r[l + 1] @ H1b[l + 1] @ g[l]
+        k[l] = c[l] + g[l] @ H(H1b[l + 1]) @ k[l + 1]
+    dV = np.array([2 * np.real(np.trace(k[l] @ W @ r[l])) for l in range(nx)])
+    dV[0] += 2 * np.real(np.trace(W @ X @ SpL @ k[0])) + np.real(np.trace(GamR @ X @ (1j * (SpL - H(SpL))) @ H(X)))
+    dV[-1] += 2 * np.real(np.trace(W @ r[-1] @ SpR @ X)) + np.real(np.trace((1j * (SpR - H(SpR))) @ X @ GamL @ H(X)))
+    ds = 0.0
+    for m in range(1, nx - 1):
+        ds += 2 * np.real(np.trace(W @ r[m] @ H1b[m] @ k[m - 1]) + np.trace(W @ r[m - 1] @ H(H1b[m]) @ k[m]))
+    return T, dV, float(ds)
+
+
+def fd_gradient(Hii, H1i, E, mu, temp, opts: Opts, h=1e-6):
+    """Central finite differences of the C++ oracle's T(E) (the reference
+    algorithm in FP64) w.r.t. V_l and s.  Arrays in the Fortran block layout."""
+    nx, nm, _ = Hii.shape
+    E = np.atleast_1d(np.asarray(E, float))
+    o = Opts(**{**opts.__dict__, "want_T": True})
+    eye = np.eye(nm, dtype=complex)
+    dV = np.zeros((len(E), nx))
+    for l in range(nx):
+        Hp = Hii.copy()
+        Hm = Hii.copy()
+        Hp[l] += h * eye
+        Hm[l] -= h * eye
+        Tp = rgf_batch(Hp, H1i, E, mu, temp, o, outputs=())["T"]
+        Tm = rgf_batch(Hm, H1i, E, mu, temp, o, outputs=())["T"]
+        dV[:, l] = (Tp - Tm) / (2 * h)
+    Sp = H1i.copy()
+    Sm = H1i.copy()
+    Sp[1:nx - 1] *= (1 + h)
+    Sm[1:nx - 1] *= (1 - h)
+    ds = (rgf_batch(Hii, Sp, E, mu, temp, o, outputs=())["T"]
+          - rgf_batch(Hii, Sm, E, mu, temp, o, outputs=())["T"]) / (2 * h)
+    return dV, ds

@@ -616,3 +616,43 @@ extern "C" void oracle_calc_n_electron(const cd* G_lesser, const cd* G_greater, 
             pelec[ix] = pelec[ix] - G_greater[off].imag() * dE * dK;
         }
 }
+
+// calc_block_current (green_rgf.f90:4602-4640): bond current between the
+// sub-blocks ib, ib+1 (nb orbitals each, ns per block) of every block, per
+// energy (jdens) and summed over energies (tot_cur, tot_ecur).  The last
+// sub-block of each block repeats the previous sub-block's values, as the
+// reference does; for ns = 1 the reference uses an unset matrix there, taken
+// as zero here.  H (nm,nm,nx), G_lesser (nm,nm,nx,nen); outputs (nb,nb,nx*ns[,nen]).
+extern "C" void oracle_calc_block_current(const cd* H, const cd* G_lesser, int64_t nen,
+                                          const double* en, double spindeg, int64_t nb,
+                                          int64_t ns, int64_t nm, int64_t nx, double* tot_cur,
+                                          double* tot_ecur, double* jdens) {
+  const double e0 = 1.6022e-19, hbar = 1.0546e-34, tpi = 6.28318530718;
+  const size_t n2 = (size_t)nm * nm, b2 = (size_t)nb * nb, nl = (size_t)nx * ns;
+  for (size_t k = 0; k < b2 * nl; k++) { tot_cur[k] = 0.0; if (tot_ecur) tot_ecur[k] = 0.0; }
+  std::vector<cd> B(b2, cd(0.0, 0.0));
+  const double scale = (en[1] - en[0]) * e0 / tpi / hbar * e0 * spindeg;
+  for (int64_t ie = 0; ie < nen; ie++)
+    for (int64_t ix = 0; ix < nx; ix++) {
+      const cd* Hx = H + ix * n2;
+      const cd* Gx = G_lesser + ix * n2 + (size_t)ie * nx * n2;
+      if (ns == 1) std::fill(B.begin(), B.end(), cd(0.0, 0.0));
+      for (int64_t ib = 1; ib <= ns; ib++) {
+        if (ib < ns) {
+          for (int64_t io = 0; io < nb; io++)
+            for (int64_t jo = 0; jo < nb; jo++) {
+              const size_t i = io + (ib - 1) * nb, j = jo + ib * nb;
+              const cd b = Hx[i + j * nm] * Gx[j + i * nm] - Hx[j + i * nm] * Gx[i + j * nm];
+              B[io + jo * nb] = b * scale;
+            }
+        }
+        const size_t l = (size_t)ix * ns + (ib - 1);
+        for (size_t k = 0; k < b2; k++) {
+          const double v = B[k].real();
+          if (jdens) jdens[k + l * b2 + (size_t)ie * nl * b2] = v;
+          if (tot_ecur) tot_ecur[k + l * b2] += en[ie] * v;
+          tot_cur[k + l * b2] += v;
+        }
+      }
+    }
+}

@@ -32,6 +32,21 @@ def random_sigma(nm, nx, nen, seed, scale=0.02):
     return sl, sr
 
 
+def perturbed_inputs(Hii, H1i, seed, eps=2.0 ** -52):
+    """Hii, H1i with every element scaled by (1 + eps*u), u uniform in
+    [-1, 1]: one rounding of the input.  Each diagonal block stays Hermitian
+    (the perturbed upper triangle is mirrored, the diagonal kept real)."""
+    rng = np.random.default_rng(10_000 + seed)
+    P = np.array(Hii, np.complex128) * (1 + eps * rng.uniform(-1, 1, np.shape(Hii)))
+    up = np.triu(P, 1)
+    P = up + np.conj(np.swapaxes(up, -1, -2))
+    n = P.shape[-1]
+    P[..., range(n), range(n)] = (np.asarray(Hii)[..., range(n), range(n)].real
+                                  * (1 + eps * rng.uniform(-1, 1, P.shape[:-2] + (n,))))
+    Q = np.array(H1i, np.complex128) * (1 + eps * rng.uniform(-1, 1, np.shape(H1i)))
+    return P, Q
+
+
 def rel_err(a, b, scale=None):
     a = np.asarray(a)
     b = np.asarray(b)

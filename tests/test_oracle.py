@@ -218,3 +218,58 @@ def test_oracle_reproduces_golden(oracle_mod, path):
     assert rel_err(r["pdens"], z["pdens"], scale=np.max(np.abs(z["ldos"]))) < 1e-12
     assert rel_err(r["T"], z["T"]) < 1e-12
     assert rel_err(r["tr"], z["tr"]) < 1e-10
+
+
+def test_adjoint_restatement_matches_finite_differences(oracle_mod):
+    """The analytic adjoint of T(E) (checker of rgf_adjoint_energies) against
+    central differences of the C++ FP64 oracle, including the lead shift of
+    the end blocks and the interior coupling scale."""
+    O = oracle_mod
+    nm, nx = 6, 5
+    d = S.make_device(nm, nx, seed=7)
+    Hb, H1b = O.to_blocks(d.Hii), O.to_blocks(d.H1i)
+    opts = O.Opts(eta_dev=0.0, eta_lead=1e-3)
+    E = np.array([-1.3, 0.4])
+    fdV, fds = O.fd_gradient(d.Hii, d.H1i, E, MU, _temp(), opts, h=1e-5)
+    for ie, e in enumerate(E):
+        T, dV, ds = O.adjoint_numpy(Hb, H1b, e, opts)
+        scale = np.max(np.abs(dV))
+        assert np.max(np.abs(dV - fdV[ie])) < 1e-6 * scale
+        assert abs(ds - fds[ie]) < 1e-6 * max(abs(ds), 1.0)
+
+
+def test_calc_block_current_loops(oracle_mod):
+    """calc_block_current against a direct transcription of its loops."""
+    O = oracle_mod
+    rng = np.random.default_rng(0)
+    nb, ns, nx, nen = 3, 3, 2, 4
+    nm = nb * ns
+    H = rng.normal(size=(nx, nm, nm)) + 1j * rng.normal(size=(nx, nm, nm))
+    G = rng.normal(size=(nen, nx, nm, nm)) + 1j * rng.normal(size=(nen, nx, nm, nm))
+    E = np.linspace(-1, 1, nen)
+    tc, te, jd = O.calc_block_current(H, G, E, 2.0, nb, ns, jdens=True)
+    Hm, Gm = O.to_blocks(H), O.to_blocks(G)
+    scale = (E[1] - E[0]) * O.E0 / 6.28318530718 / O.HBAR * O.E0 * 2.0
+    ref = np.zeros((nx * ns, nb, nb))
+    for ie in range(nen):
+        for ix in range(nx):
+            B = np.zeros((nb, nb))
+            for ib in range(ns - 1):
+                for io in range(nb):
+                    for jo in range(nb):
+                        i, j = io + ib * nb, jo + (ib + 1) * nb
+                        B[io, jo] = ((Hm[ix][i, j] * Gm[ie, ix][j, i] - Hm[ix][j, i] * Gm[ie, ix][i, j]) * scale).real
+                ref[ix * ns + ib] += B
+            ref[ix * ns + ns - 1] += B
+    assert np.allclose(O.to_blocks(tc), ref, rtol=1e-13, atol=1e-25)
+
+
+def test_perturbed_inputs_stay_hermitian_and_close():
+    from conftest import perturbed_inputs
+    d = S.make_device(8, 3, seed=2)
+    P, Q = perturbed_inputs(d.Hii, d.H1i, 0)
+    for l in range(3):
+        assert np.array_equal(P[l], P[l].conj().T)
+    assert np.max(np.abs(P - d.Hii) / np.maximum(np.abs(d.Hii), 1e-300)) <= 2.0 ** -51
+    assert np.max(np.abs(Q - d.H1i) / np.maximum(np.abs(d.H1i), 1e-300)) <= 2.0 ** -51
+    assert not np.array_equal(P, d.Hii)
