@@ -55,6 +55,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-threads", type=int, default=0)
+    p.add_argument("--adjoint", action="store_true",
+                   help="time the adjoint (dT/dV_l, dT/ds, dI/dV_l) against forward solves on the "
+                        "adjoint workload (nb=64, Nx=200, per-block potential U[-0.2,0.2] eV)")
     p.add_argument("--single", action="store_true",
                    help="one device-resident solve and exit (for profiler captures; prints no JSON)")
     return p.parse_args()
@@ -398,9 +401,84 @@ def run_single(args):
           f"{st['last_flops'] / st['last_kernel_ms'] / 1e9:.2f} TFLOP/s executed")
 
 
+def run_adjoint(args):
+    """Adjoint workload: nb = 64, Nx = 200, on-site potential V_l ~ U[-0.2, 0.2] eV
+    per block (seed 2), --nen energies (default 1024) on [-3, 3] eV, eta = 1e-5.
+    One step = one rgf_adjoint_energies call (T, dT/dV_l, dT/ds and the
+    current's derivatives); it is timed next to forward solves of the same
+    energies (T only, and G^R_ll + G^<_ll + T) with CUDA events on the
+    library's stream, inputs and outputs resident in HBM."""
+    import torch
+    from liteqt_b200 import rgf
+    from liteqt_b200 import synthetic as S
+    nb, nx, nen = 64, 200, (args.nen if args.nen != 296 else 1024)
+    pot = np.random.default_rng(2).uniform(-0.2, 0.2, nx)
+    d = S.make_device(nb, nx, seed=1, potential=pot)
+    E = S.energy_grid(nen, -3.0, 3.0)
+    temp = (S.temperature_for_kT(KT),) * 2
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    Hii = torch.from_numpy(d.Hii).to(dev)
+    H1i = torch.from_numpy(d.H1i).to(dev)
+    T = torch.empty(nen, dtype=torch.float64, device=dev)
+    dTdV = torch.empty((nen, nx), dtype=torch.float64, device=dev)
+    dTds = torch.empty(nen, dtype=torch.float64, device=dev)
+    ldos = torch.empty((nen, nx, nb, nb), dtype=torch.complex128, device=dev)
+    ndens = torch.empty_like(ldos)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sh = stream.cuda_stream
+    ctx = rgf.Context(rgf.Options(eta_dev=ETA, eta_lead=ETA))
+    runs = {
+        "adjoint": lambda: ctx.adjoint_energies(Hii, H1i, E, MU, temp, T=T, dTdV=dTdV, dTds=dTds,
+                                                spindeg=2.0, stream=sh),
+        "forward_T": lambda: ctx.solve_energies(Hii, H1i, E, MU, temp, T=T, stream=sh),
+        "forward_GR_GL_T": lambda: ctx.solve_energies(Hii, H1i, E, MU, temp, ldos=ldos, ndens=ndens,
+                                                      T=T, stream=sh),
+    }
+    ms = {}
+    clocks = ClockSampler(0)
+    with torch.cuda.stream(stream):
+        for name, fn in runs.items():
+            for _ in range(args.warmup):
+                fn()
+            torch.cuda.synchronize(dev)
+            if name == "adjoint":
+                clocks.start()
+            t = []
+            for _ in range(args.steps):
+                flush.fill_(1.0)
+                s = torch.cuda.Event(enable_timing=True)
+                e = torch.cuda.Event(enable_timing=True)
+                s.record(stream)
+                fn()
+                e.record(stream)
+                e.synchronize()
+                t.append(s.elapsed_time(e))
+            if name == "adjoint":
+                clk = clocks.stop()
+            ms[name] = float(np.mean(t))
+    launches = ctx.stats()["launches"]
+    ctx.close()
+    line = {"metric": "adjoint RGF energy-pts/s (dT/dV_l, dT/ds, dI/dV_l)", "value": nen / (ms["adjoint"] * 1e-3),
+            "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms["adjoint"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"adjoint_nb{nb}_nx{nx}", "nb": nb, "nx": nx, "energies": nen,
+                       "eta_eV": ETA, "potential": "U[-0.2,0.2] eV per block, seed 2",
+                       "l2": "flushed between timed steps (256 MiB write)"},
+            "forward_ms": {"T_only": ms["forward_T"], "GR_GL_T": ms["forward_GR_GL_T"]},
+            "cost_vs_forward": {"T_only": ms["adjoint"] / ms["forward_T"],
+                                "GR_GL_T": ms["adjoint"] / ms["forward_GR_GL_T"]},
+            "gpu_launches_total": int(launches), "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
-    if args.single:
+    if args.adjoint:
+        run_adjoint(args)
+    elif args.single:
         run_single(args)
     elif args.impl == "reference":
         run_reference(args)
