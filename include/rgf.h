@@ -153,6 +153,49 @@ RGF_API int rgf_ctx_get_stats(const rgf_ctx* ctx, rgf_stats* stats);
 RGF_API int rgf_solve_batch(rgf_ctx* ctx, const rgf_device* devices, int32_t n_devices,
                     const rgf_task* tasks, int64_t n_tasks, rgf_task_info* info, void* stream);
 
+/* Reusable batched solve captured in a CUDA graph.  No counterpart in the
+ * reference: for drivers that solve the same task list again and again (the
+ * self-consistent GW and Poisson loops re-solve every energy with new
+ * self-energies or potentials written in place).  rgf_plan_create checks the
+ * task list, builds the device task table and workspace once and captures the
+ * launch (queue reset + one persistent launch over all tasks, any mix of
+ * block sizes) in a CUDA graph; rgf_plan_execute replays it on `stream`.
+ * Every array the devices and tasks reference must be device memory and stay
+ * valid while the plan exists; their contents may change between executions
+ * (they are read when the graph runs), the energies and addresses may not.
+ * The plan keeps the context's options and kernel choices of creation time. */
+typedef struct rgf_plan rgf_plan;
+RGF_API int rgf_plan_create(rgf_ctx* ctx, const rgf_device* devices, int32_t n_devices,
+                            const rgf_task* tasks, int64_t n_tasks, rgf_plan** plan);
+/* Replay.  info == NULL: returns once the graph is launched (stream-ordered).
+ * info != NULL (host, n_tasks entries): waits for the solve, copies the
+ * per-task diagnostics, updates the context's stats and returns
+ * RGF_E_STATUS if any status word is non-zero. */
+RGF_API int rgf_plan_execute(rgf_plan* plan, rgf_task_info* info, void* stream);
+RGF_API int rgf_plan_destroy(rgf_plan* plan);
+
+/* Autotuner.  No counterpart in the reference.  For the block size of
+ * `device`, times every kernel variant that supports it (staged GEMM with
+ * blocked inverse for nb = 32, 64, 128, 256; register-direct GEMMs with 8x8,
+ * 8x16 and 16x16 warp tiles for any multiple of 8 / 16) at 1 and at the
+ * largest number of resident CTAs per SM, each on a probe batch of the
+ * device's first min(nx, 12) blocks with one energy per resident CTA
+ * (outputs G^R_ll, G^<_ll, T; energies spread over [-3, 3] eV), and keeps the
+ * fastest per energy in the context for later solves of that block size.
+ * Inputs may be host or device memory.  result may be NULL. */
+typedef struct rgf_tune_result {
+  int32_t nb;
+  int32_t variant;              /* chosen kernel variant (rgf_variant_name) */
+  int32_t ctas_per_sm;          /* chosen resident CTAs per SM */
+  int32_t n_candidates;
+  int32_t cand_variant[16];
+  int32_t cand_ctas_per_sm[16];
+  double cand_us_per_energy[16];
+} rgf_tune_result;
+RGF_API int rgf_autotune(rgf_ctx* ctx, const rgf_device* device, rgf_tune_result* result);
+/* Name of a kernel variant id ("staged128", "generic2x2", ...). */
+RGF_API const char* rgf_variant_name(int32_t variant);
+
 /* Drop-in for green_RGF_RS (src/green_rgf.f90:3950): same arguments in the
  * same order, scalars by reference.  sigma_greater_ph is accepted and unused,
  * as in the reference.  GRi1 / GLi1 / GGi1 may be NULL (absent optional). */

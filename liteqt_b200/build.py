@@ -1,9 +1,15 @@
 """Build the sm_100a CUDA library liteqt_b200/librgf_b200.so in-tree with nvcc.
 
-    python -m liteqt_b200.build [--force]
+    python -m liteqt_b200.build [--force] [--ptxas]
+
+Every .cu file is compiled separately (in parallel) as relocatable device
+code: each kernel variant's task function lives in its own translation unit
+(rgf_task_*.cu) and the persistent kernel (rgf_fp64.cu) calls them across
+units, resolved by the device link of the final shared library.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import glob
 import os
 import shutil
@@ -17,7 +23,10 @@ BUILD_DIR = os.path.join(HERE, "_build")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-O3", "-lineinfo", "-std=c++17",
+    "-O3", "-lineinfo", "-std=c++17", "-rdc=true",
+    # the persistent kernel runs 2 CTAs of 256 threads per SM: every task
+    # function it calls must fit the same 128-register budget
+    "-maxrregcount=128",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
     "--expt-relaxed-constexpr",
 ]
@@ -49,6 +58,7 @@ def _stale(target, deps):
 def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(BUILD_DIR, exist_ok=True)
     objs = []
+    jobs = []
     hdrs = headers()
     for src in sources():
         obj = os.path.join(BUILD_DIR, os.path.basename(src) + ".o")
@@ -57,12 +67,28 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             cmd = [nvcc(), *NVCC_FLAGS, "-c", src, "-o", obj]
             if ptxas_info:
                 cmd.insert(1, "-Xptxas=-v")
-            if verbose:
-                print(" ".join(cmd), flush=True)
-            subprocess.check_call(cmd)
+            jobs.append(cmd)
+    if jobs:
+        workers = max(1, min(len(jobs), os.cpu_count() or 1))
+        with concurrent.futures.ThreadPoolExecutor(workers) as pool:
+            futs = []
+            for cmd in jobs:
+                if verbose:
+                    print(" ".join(cmd), flush=True)
+                futs.append(pool.submit(subprocess.run, cmd, capture_output=True, text=True))
+            failed = None
+            for cmd, f in zip(jobs, futs):
+                r = f.result()
+                if r.stdout or r.stderr:
+                    sys.stdout.write(r.stdout + r.stderr)
+                if r.returncode != 0 and failed is None:
+                    failed = subprocess.CalledProcessError(r.returncode, cmd)
+            if failed is not None:
+                raise failed
     if force or _stale(LIB, objs):
-        # exported symbols: the extern "C" rgf_* entry points (visibility default via the map)
-        cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB, *objs,
+        # device link of the relocatable objects + host link; exported symbols:
+        # the extern "C" rgf_* entry points (visibility default via the map)
+        cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-rdc=true", "-shared", "-o", LIB, *objs,
                "-Xlinker", "--version-script=" + os.path.join(CSRC, "exports.map")]
         if verbose:
             print(" ".join(cmd), flush=True)

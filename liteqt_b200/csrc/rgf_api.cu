@@ -85,6 +85,8 @@ struct rgf_ctx {
   DevBuf work, tasks, devs, info, queue, stage;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   rgf_stats stats;
+  int8_t variant[kVariantSlots];  // kernel variant per block size (defaults; rgf_autotune may override)
+  int8_t ctas[kVariantSlots];     // resident CTAs per SM per block size, 0 = as many as fit
 };
 
 extern "C" void rgf_opts_default(rgf_opts* o) {
@@ -132,6 +134,10 @@ extern "C" int rgf_ctx_create(const rgf_opts* opts, rgf_ctx** out) {
   c->device = opts->device;
   RGF_CUDA(cudaSetDevice(c->device));
   RGF_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device));
+  for (int i = 0; i < kVariantSlots; i++) {
+    c->variant[i] = (int8_t)default_variant(i * 8);
+    c->ctas[i] = 0;
+  }
   RGF_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   RGF_CUDA(cudaEventCreate(&c->ev0));
   RGF_CUDA(cudaEventCreate(&c->ev1));
@@ -239,6 +245,74 @@ struct Stage {
 
 }  // namespace
 
+// Kernel parameters common to every launch of a context.
+static void fill_params(const rgf_ctx* c, KParams& p) {
+  std::memset(&p, 0, sizeof(p));
+  p.o.eta_dev = c->opts.eta_dev;
+  p.o.eta_lead = c->opts.eta_lead;
+  p.o.boltz = c->opts.boltz;
+  p.o.sancho_tol = c->opts.sancho_tol;
+  p.o.sancho_nmax = c->opts.sancho_nmax;
+  p.o.consistent = c->opts.consistent;
+  p.o.want_T = c->opts.want_T;
+  std::memcpy(p.variant, c->variant, sizeof(p.variant));
+}
+
+// Resident CTAs per SM of a launch with this much dynamic shared memory over
+// tasks of the block sizes in nb_mask (bit nb/8): the occupancy limit, or the
+// smallest count the autotuner chose for one of those block sizes.
+static int launch_ctas_per_sm(const rgf_ctx* c, size_t smem, uint64_t nb_mask) {
+  int k = solver_blocks_per_sm(smem);
+  for (int i = 0; i < kVariantSlots; i++)
+    if (((nb_mask >> i) & 1) && c->ctas[i] > 0 && c->ctas[i] < k) k = c->ctas[i];
+  return k;
+}
+
+// Checks a task list; RGF_OK or the error.
+static int validate_batch(const rgf_device* devices, int32_t n_devices, const rgf_task* tasks,
+                          int64_t n_tasks) {
+  for (int32_t d = 0; d < n_devices; d++) {
+    const rgf_device& v = devices[d];
+    if (v.nm < 8 || v.nm > kMaxNb || v.nm % 8 != 0)
+      return fail(RGF_E_UNSUPPORTED, "device %d: nm=%lld unsupported (multiple of 8 in [8,%d])", d,
+                  (long long)v.nm, kMaxNb);
+    if (v.nx < 2) return fail(RGF_E_ARG, "device %d: nx=%lld < 2", d, (long long)v.nx);
+    if (!v.Hii || !v.H1i) return fail(RGF_E_ARG, "device %d: Hii/H1i is NULL", d);
+    if (!(v.temp[0] > 0.0) || !(v.temp[1] > 0.0))
+      return fail(RGF_E_ARG, "device %d: temperature must be > 0", d);
+  }
+  for (int64_t t = 0; t < n_tasks; t++)
+    if (tasks[t].device < 0 || tasks[t].device >= n_devices)
+      return fail(RGF_E_ARG, "task %lld: device index %d out of range", (long long)t, tasks[t].device);
+  return RGF_OK;
+}
+
+// Launch geometry of a task list: queue order (descending estimated cost:
+// nb^3 x (block operations of the chain + both leads)), slot size, dynamic
+// shared memory and the block sizes present.
+struct LaunchShape {
+  std::vector<int32_t> order;
+  int64_t slot = 0;
+  size_t smem = 0;
+  uint64_t nb_mask = 0;
+};
+static LaunchShape launch_shape(const rgf_ctx* c, const rgf_device* devices, const rgf_task* tasks,
+                                int64_t n_tasks) {
+  LaunchShape L;
+  L.order.resize(n_tasks);
+  std::vector<double> cost(n_tasks);
+  for (int64_t t = 0; t < n_tasks; t++) {
+    const rgf_device& v = devices[tasks[t].device];
+    L.order[t] = (int32_t)t;
+    cost[t] = (double)v.nm * v.nm * v.nm * (30.0 * (double)v.nx + 400.0);
+    L.slot = std::max<int64_t>(L.slot, slot_elems_for(v.nm, v.nx));
+    L.smem = std::max(L.smem, variant_smem(c->variant[v.nm / 8], (int)v.nm));
+    L.nb_mask |= 1ull << (v.nm / 8);
+  }
+  std::stable_sort(L.order.begin(), L.order.end(), [&](int32_t a, int32_t b) { return cost[a] > cost[b]; });
+  return L;
+}
+
 extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_devices,
                                const rgf_task* tasks, int64_t n_tasks, rgf_task_info* info,
                                void* stream_) {
@@ -254,19 +328,8 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
   const bool want_T = c->opts.want_T != 0;
 
   // ---- validate
-  for (int32_t d = 0; d < n_devices; d++) {
-    const rgf_device& v = devices[d];
-    if (v.nm < 8 || v.nm > kMaxNb || v.nm % 8 != 0)
-      return fail(RGF_E_UNSUPPORTED, "device %d: nm=%lld unsupported (multiple of 8 in [8,%d])", d,
-                  (long long)v.nm, kMaxNb);
-    if (v.nx < 2) return fail(RGF_E_ARG, "device %d: nx=%lld < 2", d, (long long)v.nx);
-    if (!v.Hii || !v.H1i) return fail(RGF_E_ARG, "device %d: Hii/H1i is NULL", d);
-    if (!(v.temp[0] > 0.0) || !(v.temp[1] > 0.0))
-      return fail(RGF_E_ARG, "device %d: temperature must be > 0", d);
-  }
-  for (int64_t t = 0; t < n_tasks; t++)
-    if (tasks[t].device < 0 || tasks[t].device >= n_devices)
-      return fail(RGF_E_ARG, "task %lld: device index %d out of range", (long long)t, tasks[t].device);
+  int rc = validate_batch(devices, n_devices, tasks, n_tasks);
+  if (rc) return rc;
 
   // ---- staging of host arrays
   Stage sg;
@@ -294,7 +357,7 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
     if (want_T) sg.add(k.T, sizeof(double), false, true);
   }
   sg.layout();
-  int rc = c->stage.reserve(std::max<size_t>(sg.total, 256));
+  rc = c->stage.reserve(std::max<size_t>(sg.total, 256));
   if (rc) return rc;
   char* sbase = (char*)c->stage.p;
   for (const auto& s : sg.segs)
@@ -333,33 +396,15 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
     o.T = want_T ? (double*)sg.resolve(k.T, sbase) : nullptr;
   }
 
-  // ---- launch plan: one persistent launch per block size, longest devices first
-  std::map<int64_t, std::vector<int32_t>> groups;
-  for (int64_t t = 0; t < n_tasks; t++) groups[devices[tasks[t].device].nm].push_back((int32_t)t);
-  if (groups.size() > 64) return fail(RGF_E_ARG, "too many distinct block sizes in one batch");
-  struct Launch { int nb; int grid; int64_t nx_max, slot; size_t order_off, count; };
-  std::vector<Launch> plan;
-  std::vector<int32_t> order;
-  order.reserve(n_tasks);
-  size_t work_elems = 0;
-  for (auto& kv : groups) {
-    std::vector<int32_t> ids = kv.second;
-    std::stable_sort(ids.begin(), ids.end(), [&](int32_t a, int32_t b) {
-      return devices[tasks[a].device].nx > devices[tasks[b].device].nx;
-    });
-    Launch L;
-    L.nb = (int)kv.first;
-    L.nx_max = devices[tasks[ids.front()].device].nx;
-    L.slot = slot_elems_for(L.nb, L.nx_max);
-    L.grid = std::max(1, c->sm_count * fp64_blocks_per_sm(L.nb));
-    if ((int64_t)L.grid > (int64_t)ids.size()) L.grid = (int)ids.size();
-    L.order_off = order.size();
-    L.count = ids.size();
-    order.insert(order.end(), ids.begin(), ids.end());
-    work_elems = std::max(work_elems, (size_t)L.slot * L.grid);
-    plan.push_back(L);
-  }
-  if ((rc = c->work.reserve(sizeof(double2) * work_elems))) return rc;
+  // ---- launch plan: one persistent launch for every block size, longest
+  // tasks first, so the launch ends on its shortest tasks
+  const LaunchShape shape = launch_shape(c, devices, tasks, n_tasks);
+  const std::vector<int32_t>& order = shape.order;
+  const int64_t slot = shape.slot;
+  const size_t smem = shape.smem;
+  int grid = c->sm_count * launch_ctas_per_sm(c, smem, shape.nb_mask);
+  if ((int64_t)grid > n_tasks) grid = (int)n_tasks;
+  if ((rc = c->work.reserve(sizeof(double2) * (size_t)slot * grid))) return rc;
   if ((rc = c->devs.reserve(sizeof(DDev) * n_devices))) return rc;
   if ((rc = c->tasks.reserve(sizeof(DTask) * n_tasks + sizeof(int32_t) * n_tasks))) return rc;
   if ((rc = c->info.reserve(sizeof(DInfo) * n_tasks))) return rc;
@@ -369,33 +414,21 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
   RGF_CUDA(cudaMemcpyAsync(c->tasks.p, dtask.data(), sizeof(DTask) * n_tasks, cudaMemcpyHostToDevice, st));
   RGF_CUDA(cudaMemcpyAsync(order_d, order.data(), sizeof(int32_t) * n_tasks, cudaMemcpyHostToDevice, st));
   RGF_CUDA(cudaMemsetAsync(c->info.p, 0, sizeof(DInfo) * n_tasks, st));
-  RGF_CUDA(cudaMemsetAsync(c->queue.p, 0, sizeof(int32_t) * 64, st));
+  RGF_CUDA(cudaMemsetAsync(c->queue.p, 0, sizeof(int32_t), st));
+  KParams p;
+  fill_params(c, p);
+  p.devs = (const DDev*)c->devs.p;
+  p.tasks = (const DTask*)c->tasks.p;
+  p.n_tasks = n_tasks;
+  p.order = order_d;
+  p.queue = (int32_t*)c->queue.p;
+  p.work = (double2*)c->work.p;
+  p.slot_elems = slot;
+  p.info = (DInfo*)c->info.p;
   RGF_CUDA(cudaEventRecord(c->ev0, st));
-  for (size_t g = 0; g < plan.size(); g++) {
-    const Launch& L = plan[g];
-    KParams p;
-    std::memset(&p, 0, sizeof(p));
-    p.o.eta_dev = c->opts.eta_dev;
-    p.o.eta_lead = c->opts.eta_lead;
-    p.o.boltz = c->opts.boltz;
-    p.o.sancho_tol = c->opts.sancho_tol;
-    p.o.sancho_nmax = c->opts.sancho_nmax;
-    p.o.consistent = c->opts.consistent;
-    p.o.want_T = c->opts.want_T;
-    p.devs = (const DDev*)c->devs.p;
-    p.tasks = (const DTask*)c->tasks.p;
-    p.n_tasks = (int64_t)L.count;
-    p.order = order_d + L.order_off;
-    p.queue = (int32_t*)c->queue.p + g;
-    p.work = (double2*)c->work.p;
-    p.slot_elems = L.slot;
-    p.nx_max = L.nx_max;
-    p.nb = L.nb;
-    p.info = (DInfo*)c->info.p;
-    cudaError_t e = launch_fp64(p, L.grid, st);  // launches on one stream run in order
-    if (e != cudaSuccess) return fail(RGF_E_CUDA, "solver launch failed: %s", cudaGetErrorString(e));
-    c->stats.launches++;
-  }
+  cudaError_t e = launch_solver(p, grid, smem, st);
+  if (e != cudaSuccess) return fail(RGF_E_CUDA, "solver launch failed: %s", cudaGetErrorString(e));
+  c->stats.launches++;
   RGF_CUDA(cudaEventRecord(c->ev1, st));
 
   // ---- outputs back
@@ -490,31 +523,23 @@ extern "C" int rgf_adjoint_energies(rgf_ctx* c, const rgf_device* v, int64_t nen
   RGF_CUDA(cudaMemcpyAsync(tb, tasks.data(), sizeof(DAdj) * nen, cudaMemcpyHostToDevice, st));
   RGF_CUDA(cudaMemsetAsync(c->info.p, 0, sizeof(DInfo) * nen, st));
   RGF_CUDA(cudaMemsetAsync(c->queue.p, 0, sizeof(int32_t), st));
-  const int nb = (int)nm;
-  int grid = std::max(1, c->sm_count * fp64_blocks_per_sm(nb));
+  const size_t smem = variant_smem(c->variant[nm / 8], (int)nm);
+  int grid = c->sm_count * launch_ctas_per_sm(c, smem, 1ull << (nm / 8));
   if ((int64_t)grid > nen) grid = (int)nen;
   const int64_t slot = slot_elems_for(nm, nx);
   if ((rc = c->work.reserve(sizeof(double2) * (size_t)slot * grid))) return rc;
   KParams p;
-  std::memset(&p, 0, sizeof(p));
-  p.o.eta_dev = c->opts.eta_dev;
-  p.o.eta_lead = c->opts.eta_lead;
-  p.o.boltz = c->opts.boltz;
-  p.o.sancho_tol = c->opts.sancho_tol;
-  p.o.sancho_nmax = c->opts.sancho_nmax;
-  p.o.consistent = c->opts.consistent;
+  fill_params(c, p);
   p.o.want_T = 1;
   p.devs = (const DDev*)c->devs.p;
   p.n_tasks = nen;
   p.queue = (int32_t*)c->queue.p;
   p.work = (double2*)c->work.p;
   p.slot_elems = slot;
-  p.nx_max = nx;
-  p.nb = nb;
   p.info = (DInfo*)c->info.p;
   p.adj = (const DAdj*)tb;
   RGF_CUDA(cudaEventRecord(c->ev0, st));
-  cudaError_t e = launch_fp64(p, grid, st);
+  cudaError_t e = launch_solver(p, grid, smem, st);
   if (e != cudaSuccess) return fail(RGF_E_CUDA, "adjoint launch failed: %s", cudaGetErrorString(e));
   c->stats.launches++;
   RGF_CUDA(cudaEventRecord(c->ev1, st));
@@ -692,4 +717,253 @@ extern "C" int rgf_solve_energies(rgf_ctx* ctx, const rgf_device* device, int64_
     t.T = T ? T + e : nullptr;
   }
   return rgf_solve_batch(ctx, device, 1, tasks.data(), nen, info, stream);
+}
+
+// ------------------------------------------------------------------ plans
+struct rgf_plan {
+  rgf_ctx* ctx = nullptr;
+  int64_t n_tasks = 0;
+  std::vector<int> task_nb;
+  DevBuf work, tasks, devs, info, queue;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  ~rgf_plan() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    work.release();
+    tasks.release();
+    devs.release();
+    info.release();
+    queue.release();
+  }
+};
+
+extern "C" int rgf_plan_create(rgf_ctx* c, const rgf_device* devices, int32_t n_devices,
+                               const rgf_task* tasks, int64_t n_tasks, rgf_plan** out) {
+  if (!c || !out) return fail(RGF_E_ARG, "NULL argument");
+  *out = nullptr;
+  if (n_tasks < 1 || !tasks || !devices || n_devices < 1) return fail(RGF_E_ARG, "invalid task list");
+  if (n_tasks > (int64_t)INT32_MAX) return fail(RGF_E_ARG, "too many tasks in one plan");
+  if (c->opts.precision != RGF_PREC_FP64)
+    return fail(RGF_E_UNSUPPORTED, "precision mode %d is not available in this build", c->opts.precision);
+  int rc = validate_batch(devices, n_devices, tasks, n_tasks);
+  if (rc) return rc;
+  RGF_CUDA(cudaSetDevice(c->device));
+  auto dev_ok = [](const void* p) { return !p || is_device_ptr(p); };
+  for (int32_t d = 0; d < n_devices; d++)
+    if (!dev_ok(devices[d].Hii) || !dev_ok(devices[d].H1i))
+      return fail(RGF_E_ARG, "device %d: plan arrays must be device memory", d);
+  const bool want_T = c->opts.want_T != 0;
+  std::vector<DDev> ddev(n_devices);
+  for (int32_t d = 0; d < n_devices; d++) {
+    ddev[d].nm = devices[d].nm;
+    ddev[d].nx = devices[d].nx;
+    ddev[d].Hii = (const double2*)devices[d].Hii;
+    ddev[d].H1i = (const double2*)devices[d].H1i;
+    for (int i = 0; i < 2; i++) {
+      ddev[d].mu[i] = devices[d].mu[i];
+      ddev[d].temp[i] = devices[d].temp[i];
+    }
+  }
+  std::unique_ptr<rgf_plan> pl(new rgf_plan());
+  pl->ctx = c;
+  pl->n_tasks = n_tasks;
+  pl->task_nb.resize(n_tasks);
+  std::vector<DTask> dtask(n_tasks);
+  for (int64_t t = 0; t < n_tasks; t++) {
+    const rgf_task& k = tasks[t];
+    const void* ptrs[] = {k.sigma_lesser, k.sigma_r, k.ldos, k.ndens, k.pdens, k.GRi1, k.GLi1,
+                          k.GGi1, k.cur, k.tr, k.tre, want_T ? k.T : nullptr};
+    for (const void* q : ptrs)
+      if (!dev_ok(q)) return fail(RGF_E_ARG, "task %lld: plan arrays must be device memory", (long long)t);
+    DTask& o = dtask[t];
+    std::memset(&o, 0, sizeof(o));
+    o.dev = k.device;
+    o.E = k.E;
+    o.sig_lesser = (const double2*)k.sigma_lesser;
+    o.sig_r = (const double2*)k.sigma_r;
+    o.ldos = (double2*)k.ldos;
+    o.ndens = (double2*)k.ndens;
+    o.pdens = (double2*)k.pdens;
+    o.GRi1 = (double2*)k.GRi1;
+    o.GLi1 = (double2*)k.GLi1;
+    o.GGi1 = (double2*)k.GGi1;
+    o.cur = k.cur;
+    o.tr = k.tr;
+    o.tre = k.tre;
+    o.T = want_T ? k.T : nullptr;
+    pl->task_nb[t] = (int)devices[k.device].nm;
+  }
+  const LaunchShape shape = launch_shape(c, devices, tasks, n_tasks);
+  int grid = c->sm_count * launch_ctas_per_sm(c, shape.smem, shape.nb_mask);
+  if ((int64_t)grid > n_tasks) grid = (int)n_tasks;
+  if ((rc = pl->work.reserve(sizeof(double2) * (size_t)shape.slot * grid))) return rc;
+  if ((rc = pl->devs.reserve(sizeof(DDev) * n_devices))) return rc;
+  if ((rc = pl->tasks.reserve(sizeof(DTask) * n_tasks + sizeof(int32_t) * n_tasks))) return rc;
+  if ((rc = pl->info.reserve(sizeof(DInfo) * n_tasks))) return rc;
+  if ((rc = pl->queue.reserve(256))) return rc;
+  int32_t* order_d = (int32_t*)((char*)pl->tasks.p + sizeof(DTask) * n_tasks);
+  RGF_CUDA(cudaMemcpy(pl->devs.p, ddev.data(), sizeof(DDev) * n_devices, cudaMemcpyHostToDevice));
+  RGF_CUDA(cudaMemcpy(pl->tasks.p, dtask.data(), sizeof(DTask) * n_tasks, cudaMemcpyHostToDevice));
+  RGF_CUDA(cudaMemcpy(order_d, shape.order.data(), sizeof(int32_t) * n_tasks, cudaMemcpyHostToDevice));
+  KParams p;
+  fill_params(c, p);
+  p.devs = (const DDev*)pl->devs.p;
+  p.tasks = (const DTask*)pl->tasks.p;
+  p.n_tasks = n_tasks;
+  p.order = order_d;
+  p.queue = (int32_t*)pl->queue.p;
+  p.work = (double2*)pl->work.p;
+  p.slot_elems = shape.slot;
+  p.info = (DInfo*)pl->info.p;
+  solver_blocks_per_sm(shape.smem);  // raises the kernel's shared-memory limit before the capture
+  cudaStream_t cs = nullptr;
+  RGF_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    cudaError_t e1 = cudaMemsetAsync(pl->queue.p, 0, sizeof(int32_t), cs);
+    cudaError_t e2 = cudaMemsetAsync(pl->info.p, 0, sizeof(DInfo) * n_tasks, cs);
+    cudaError_t e3 = launch_solver(p, grid, shape.smem, cs, false);
+    e = cudaStreamEndCapture(cs, &pl->graph);
+    if (e == cudaSuccess) e = e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&pl->exec, pl->graph, 0);
+  cudaStreamDestroy(cs);
+  if (e != cudaSuccess) return fail(RGF_E_CUDA, "plan capture failed: %s", cudaGetErrorString(e));
+  *out = pl.release();
+  return RGF_OK;
+}
+
+extern "C" int rgf_plan_execute(rgf_plan* pl, rgf_task_info* info, void* stream_) {
+  if (!pl || !pl->ctx) return fail(RGF_E_ARG, "plan is NULL");
+  rgf_ctx* c = pl->ctx;
+  RGF_CUDA(cudaSetDevice(c->device));
+  cudaStream_t st = stream_ ? (cudaStream_t)stream_ : c->stream;
+  RGF_CUDA(cudaEventRecord(c->ev0, st));
+  RGF_CUDA(cudaGraphLaunch(pl->exec, st));
+  RGF_CUDA(cudaEventRecord(c->ev1, st));
+  c->stats.launches++;
+  if (!info) return RGF_OK;
+  std::vector<DInfo> h(pl->n_tasks);
+  RGF_CUDA(cudaMemcpyAsync(h.data(), pl->info.p, sizeof(DInfo) * pl->n_tasks, cudaMemcpyDeviceToHost, st));
+  RGF_CUDA(cudaStreamSynchronize(st));
+  int worst = 0;
+  double flops = 0.0;
+  for (int64_t t = 0; t < pl->n_tasks; t++) {
+    worst |= h[t].status;
+    const double nb = (double)pl->task_nb[t];
+    flops += 8.0 * nb * nb * nb * (double)(h[t].n_gemm + h[t].n_inv);
+  }
+  float kms = 0.0f;
+  RGF_CUDA(cudaEventElapsedTime(&kms, c->ev0, c->ev1));
+  c->stats.last_kernel_ms = kms;
+  c->stats.last_flops = flops;
+  c->stats.last_tasks = pl->n_tasks;
+  std::memcpy(info, h.data(), sizeof(DInfo) * pl->n_tasks);
+  if (worst & RGF_ST_BAD_TASK) return fail(RGF_E_ARG, "a task was rejected on the device");
+  return worst ? RGF_E_STATUS : RGF_OK;
+}
+
+extern "C" int rgf_plan_destroy(rgf_plan* pl) {
+  if (!pl) return RGF_OK;
+  if (pl->ctx) cudaSetDevice(pl->ctx->device);
+  cudaDeviceSynchronize();
+  delete pl;
+  return RGF_OK;
+}
+
+// --------------------------------------------------------------- autotuner
+extern "C" const char* rgf_variant_name(int32_t v) { return variant_name(v); }
+
+extern "C" int rgf_autotune(rgf_ctx* c, const rgf_device* v, rgf_tune_result* res) {
+  if (!c || !v) return fail(RGF_E_ARG, "NULL argument");
+  rgf_task dummy;
+  std::memset(&dummy, 0, sizeof(dummy));
+  int rc = validate_batch(v, 1, &dummy, 1);
+  if (rc) return rc;
+  RGF_CUDA(cudaSetDevice(c->device));
+  const int nb = (int)v->nm;
+  const int64_t nxp = std::min<int64_t>(v->nx, 12);
+  const size_t blk = (size_t)nb * nb;
+  // probe device: the first nxp blocks, on the device
+  rgf_device pd = *v;
+  pd.nx = nxp;
+  void* hbuf = nullptr;
+  if (!is_device_ptr(v->Hii) || !is_device_ptr(v->H1i)) {
+    RGF_CUDA(cudaMalloc(&hbuf, 2 * sizeof(rgf_c16) * blk * nxp));
+    RGF_CUDA(cudaMemcpy(hbuf, v->Hii, sizeof(rgf_c16) * blk * nxp,
+                        is_device_ptr(v->Hii) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice));
+    RGF_CUDA(cudaMemcpy((rgf_c16*)hbuf + blk * nxp, v->H1i, sizeof(rgf_c16) * blk * nxp,
+                        is_device_ptr(v->H1i) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice));
+    pd.Hii = (const rgf_c16*)hbuf;
+    pd.H1i = (const rgf_c16*)hbuf + blk * nxp;
+  }
+  struct Cand { int v, k; double us; };
+  std::vector<Cand> cands;
+  int kmax_all = 1;
+  for (int vv = 0; vv < KV_COUNT; vv++) {
+    if (!variant_ok(vv, nb)) continue;
+    const int occ = solver_blocks_per_sm(variant_smem(vv, nb));
+    kmax_all = std::max(kmax_all, occ);
+    cands.push_back({vv, 1, 0.0});
+    if (occ > 1) cands.push_back({vv, occ, 0.0});
+  }
+  if (cands.size() > 16) cands.resize(16);
+  const int64_t nen_max = (int64_t)c->sm_count * kmax_all;
+  void* obuf = nullptr;
+  const size_t gbytes = sizeof(rgf_c16) * blk * nxp * nen_max;
+  cudaError_t ae = cudaMalloc(&obuf, 2 * gbytes + sizeof(double) * nen_max);
+  if (ae != cudaSuccess) {
+    cudaGetLastError();
+    if (hbuf) cudaFree(hbuf);
+    return fail(RGF_E_NOMEM, "autotune: cudaMalloc of the probe outputs failed");
+  }
+  rgf_c16* ldos = (rgf_c16*)obuf;
+  rgf_c16* ndens = (rgf_c16*)((char*)obuf + gbytes);
+  double* T = (double*)((char*)obuf + 2 * gbytes);
+  const int8_t keep_v = c->variant[nb / 8], keep_k = c->ctas[nb / 8];
+  const int32_t keep_T = c->opts.want_T;
+  c->opts.want_T = 1;
+  rc = RGF_OK;
+  for (Cand& cd : cands) {
+    c->variant[nb / 8] = (int8_t)cd.v;
+    c->ctas[nb / 8] = (int8_t)cd.k;
+    const int64_t nen = (int64_t)c->sm_count * cd.k;
+    std::vector<double> E(nen);
+    for (int64_t i = 0; i < nen; i++) E[i] = -3.0 + 6.0 * ((double)i + 0.5) / (double)nen;
+    double best = 1e300;
+    for (int rep = 0; rep < 3 && rc == RGF_OK; rep++) {  // first run warms up
+      int r = rgf_solve_energies(c, &pd, nen, E.data(), nullptr, nullptr, ldos, ndens, nullptr, nullptr,
+                                 nullptr, nullptr, nullptr, T, nullptr, nullptr);
+      if (r != RGF_OK && r != RGF_E_STATUS) rc = r;
+      if (rep > 0) best = std::min(best, c->stats.last_kernel_ms);
+    }
+    cd.us = best * 1e3 / (double)nen;
+  }
+  c->opts.want_T = keep_T;
+  cudaFree(obuf);
+  if (hbuf) cudaFree(hbuf);
+  if (rc != RGF_OK) {
+    c->variant[nb / 8] = keep_v;
+    c->ctas[nb / 8] = keep_k;
+    return rc;
+  }
+  size_t bi = 0;
+  for (size_t i = 1; i < cands.size(); i++)
+    if (cands[i].us < cands[bi].us) bi = i;
+  c->variant[nb / 8] = (int8_t)cands[bi].v;
+  c->ctas[nb / 8] = (int8_t)cands[bi].k;
+  if (res) {
+    std::memset(res, 0, sizeof(*res));
+    res->nb = nb;
+    res->variant = cands[bi].v;
+    res->ctas_per_sm = cands[bi].k;
+    res->n_candidates = (int32_t)cands.size();
+    for (size_t i = 0; i < cands.size(); i++) {
+      res->cand_variant[i] = cands[i].v;
+      res->cand_ctas_per_sm[i] = cands[i].k;
+      res->cand_us_per_energy[i] = cands[i].us;
+    }
+  }
+  return RGF_OK;
 }

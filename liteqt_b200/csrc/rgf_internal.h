@@ -72,6 +72,17 @@ struct DAdj {
   double* dTds;    // scalar
 };
 
+// Block-operation policies ("kernel variants") a task can run with:
+// staged = shared-memory-staged GEMM + blocked inverse for one block size;
+// generic = register-direct GEMM with TM x TN warp tiles for any multiple of 8.
+enum KVariant : int {
+  KV_NONE = -1,
+  KV_STAGED32 = 0, KV_STAGED64, KV_STAGED128, KV_STAGED256,
+  KV_GENERIC11, KV_GENERIC12, KV_GENERIC22,
+  KV_COUNT
+};
+constexpr int kVariantSlots = kMaxNb / 8 + 1;  // indexed by nb / 8
+
 struct KParams {
   KOpts o;
   const DDev* devs;
@@ -80,27 +91,33 @@ struct KParams {
   const int32_t* order;    // task order of the queue (longest first), or NULL
   int32_t* queue;          // work-queue counter (zeroed before launch)
   double2* work;           // workspace: one slot per resident CTA
-  int64_t slot_elems;      // complex elements per slot
-  int64_t nx_max;          // Gl / Gln capacity per slot
-  int32_t nb;              // block size of every task in this launch
-  int32_t pad;
+  int64_t slot_elems;      // complex elements per slot (>= slot_elems_for(nb, nx) of every task)
   DInfo* info;             // per task
   const DAdj* adj;         // non-null: run the adjoint instead of the drop-in solve
+  int8_t variant[kVariantSlots];  // kernel variant per block size (nb / 8), KV_NONE = unsupported
 };
 
-// Number of named scratch blocks in a slot besides Gl[nx_max], Gln[nx_max].
+// Number of named scratch blocks in a slot besides Gl[nx], Gln[nx].
 constexpr int kNumTemps = 32;
 
-inline int64_t slot_elems_for(int64_t nb, int64_t nx_max) {
-  return (2 * nx_max + kNumTemps) * nb * nb;
+__host__ __device__ inline int64_t slot_elems_for(int64_t nb, int64_t nx) {
+  return (2 * nx + kNumTemps) * nb * nb;
 }
 
-// Launch the FP64 solver over all tasks (all tasks have block size p.nb).
-// Returns the CUDA error of the launch.
-cudaError_t launch_fp64(const KParams& p, int grid, cudaStream_t stream);
-int fp64_threads();
-// Max resident CTAs per SM for block size nb (occupancy query).
-int fp64_blocks_per_sm(int nb);
-size_t fp64_smem_bytes(int nb);
+// Variant selection (rgf_fp64.cu).
+int default_variant(int nb);                 // KV_NONE if nb is unsupported
+bool variant_ok(int variant, int nb);
+const char* variant_name(int variant);
+size_t variant_smem(int variant, int nb);    // dynamic shared memory of a CTA
+void set_default_variants(KParams& p);
+// Max resident CTAs per SM of the solver kernel with this much dynamic
+// shared memory (occupancy query).
+int solver_blocks_per_sm(size_t smem);
+// Launch the persistent solver over all tasks of p (any mix of block sizes).
+// set_attr = false skips raising the kernel's dynamic shared-memory limit
+// (inside a stream capture, after solver_blocks_per_sm(smem) has done it).
+cudaError_t launch_solver(const KParams& p, int grid, size_t smem, cudaStream_t stream,
+                          bool set_attr = true);
+int solver_threads();
 
 }  // namespace rgf

@@ -147,11 +147,13 @@ extern "C" int rgf_solve_energies_noalloc(const rgf_opts* opts, const rgf_device
 
   int sms = 0;
   NA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  int64_t grid = (int64_t)sms * fp64_blocks_per_sm((int)nm);
+  const size_t smem = variant_smem(default_variant((int)nm), (int)nm);
+  int64_t grid = (int64_t)sms * solver_blocks_per_sm(smem);
   grid = std::min<int64_t>(grid, nen);
   grid = std::min<int64_t>(grid, (int64_t)((kScratchBytes - off_slots) / slot_bytes));
   KParams p;
   std::memset(&p, 0, sizeof(p));
+  set_default_variants(p);
   p.o.eta_dev = opts->eta_dev;
   p.o.eta_lead = opts->eta_lead;
   p.o.boltz = opts->boltz;
@@ -166,10 +168,8 @@ extern "C" int rgf_solve_energies_noalloc(const rgf_opts* opts, const rgf_device
   p.queue = (int32_t*)base;
   p.work = (double2*)(base + off_slots);
   p.slot_elems = slot_elems_for(nm, nx);
-  p.nx_max = nx;
-  p.nb = (int)nm;
   p.info = (DInfo*)(base + off_info);
-  NA_CUDA(launch_fp64(p, (int)grid, st));
+  NA_CUDA(launch_solver(p, (int)grid, smem, st));
   std::vector<DInfo> hinfo((size_t)nen);
   NA_CUDA(cudaMemcpyAsync(hinfo.data(), base + off_info, sizeof(DInfo) * (size_t)nen, cudaMemcpyDeviceToHost, st));
   NA_CUDA(cudaStreamSynchronize(st));

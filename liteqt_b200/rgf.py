@@ -46,8 +46,12 @@ EXPORTS = (
     "rgf_solve_batch", "rgf_green_rgf_rs", "rgf_rgf_g", "rgf_solve_energies",
     "rgf_terminal_current", "rgf_calc_n_electron", "rgf_last_error", "rgf_version",
     "rgf_ctx_get_stats", "rgf_adjoint_energies", "rgf_solve_energies_noalloc",
-    "rgf_noalloc_last_error", "rgf_calc_block_current",
+    "rgf_noalloc_last_error", "rgf_calc_block_current", "rgf_plan_create", "rgf_plan_execute",
+    "rgf_plan_destroy", "rgf_autotune", "rgf_variant_name",
 )
+
+# kernel variant ids (rgf_variant_name)
+VARIANTS = ("staged32", "staged64", "staged128", "staged256", "generic1x1", "generic1x2", "generic2x2")
 
 
 class RgfError(RuntimeError):
@@ -96,6 +100,14 @@ INFO_DTYPE = np.dtype([("status", "<i4"), ("sancho_iters_left", "<i4"),
                        ("sancho_iters_right", "<i4"), ("n_gemm", "<i4"), ("n_inv", "<i4"),
                        ("reserved", "<i4")])
 
+
+
+class c_tune_result(ctypes.Structure):
+    _fields_ = [("nb", ctypes.c_int32), ("variant", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32),
+                ("n_candidates", ctypes.c_int32), ("cand_variant", ctypes.c_int32 * 16),
+                ("cand_ctas_per_sm", ctypes.c_int32 * 16), ("cand_us_per_energy", ctypes.c_double * 16)]
+
+
 _lib = None
 
 
@@ -129,6 +141,15 @@ def load(path: str = LIB_PATH):
     L.rgf_calc_block_current.restype = ctypes.c_int
     L.rgf_adjoint_energies.argtypes = [P, ctypes.POINTER(c_device), ctypes.c_int64, P, P, P, P,
                                        ctypes.c_double, P, P, P, P]
+    L.rgf_plan_create.argtypes = [P, ctypes.POINTER(c_device), ctypes.c_int32, ctypes.POINTER(c_task),
+                                  ctypes.c_int64, ctypes.POINTER(ctypes.c_void_p)]
+    L.rgf_plan_execute.argtypes = [P, P, P]
+    L.rgf_plan_destroy.argtypes = [P]
+    L.rgf_autotune.argtypes = [P, ctypes.POINTER(c_device), ctypes.POINTER(c_tune_result)]
+    L.rgf_variant_name.argtypes = [ctypes.c_int32]
+    L.rgf_variant_name.restype = ctypes.c_char_p
+    for name in ("rgf_plan_create", "rgf_plan_execute", "rgf_plan_destroy", "rgf_autotune"):
+        getattr(L, name).restype = ctypes.c_int
     L.rgf_last_error.restype = ctypes.c_char_p
     L.rgf_version.restype = ctypes.c_char_p
     for name in ("rgf_ctx_create", "rgf_ctx_destroy", "rgf_ctx_set_opts", "rgf_solve_batch",
@@ -192,6 +213,28 @@ def _ptr(a):
             raise ValueError("tensors must be contiguous")
         return a.data_ptr()
     raise TypeError(f"unsupported array type {type(a)}")
+
+
+class Plan:
+    """An rgf_plan: replay with execute(); release with close()."""
+
+    def __init__(self, h, n_tasks):
+        self.h = h
+        self.n_tasks = n_tasks
+
+    def execute(self, info=None, stream=None, allow_status=True):
+        return _check(load().rgf_plan_execute(self.h, _ptr(info), stream), allow_status)
+
+    def close(self):
+        if self.h:
+            load().rgf_plan_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 class Context:
@@ -273,6 +316,32 @@ class Context:
                                          _ptr(dIds), _ptr(info), stream)
         _check(rc, allow_status)
         return (dIdV, float(dIds[0])) if want_current else None
+
+    def plan(self, devices, tasks):
+        """rgf_plan_create: a CUDA-graph-captured batched solve over ctypes
+        c_device / c_task arrays whose pointers are all device memory."""
+        nd, nt = len(devices), len(tasks)
+        DA = (c_device * nd)(*devices)
+        TA = (c_task * nt)(*tasks)
+        h = ctypes.c_void_p()
+        _check(load().rgf_plan_create(self.h, DA, nd, TA, nt, ctypes.byref(h)))
+        return Plan(h, nt)
+
+    def autotune(self, Hii, H1i, mu, temp) -> dict:
+        """rgf_autotune for the block size of this device; returns the choice
+        and every candidate's time per energy."""
+        nx, nm = int(Hii.shape[0]), int(Hii.shape[1])
+        d = c_device()
+        d.nm, d.nx = nm, nx
+        d.Hii, d.H1i = _ptr(Hii), _ptr(H1i)
+        d.mu[0], d.mu[1] = float(mu[0]), float(mu[1])
+        d.temp[0], d.temp[1] = float(temp[0]), float(temp[1])
+        r = c_tune_result()
+        _check(load().rgf_autotune(self.h, ctypes.byref(d), ctypes.byref(r)))
+        cands = [(VARIANTS[r.cand_variant[i]], r.cand_ctas_per_sm[i], r.cand_us_per_energy[i])
+                 for i in range(r.n_candidates)]
+        return {"nb": r.nb, "variant": VARIANTS[r.variant], "ctas_per_sm": r.ctas_per_sm,
+                "candidates": cands}
 
     def solve_batch(self, devices, tasks, info=None, stream=None, allow_status=True):
         """rgf_solve_batch with ctypes c_device / c_task arrays."""

@@ -128,12 +128,10 @@ def lib():
             raise RuntimeError(f"oracle_init failed ({rc})")
         P = ctypes.c_void_p
         L.oracle_rgf_energy.argtypes = [ctypes.POINTER(OracleOpts), ctypes.c_int64, ctypes.c_int64,
-                                        ctypes.c_double, P, P, P, P, P, P, P, P, P, P, P, P, P, P,
-                                        P, P, ctypes.POINTER(OracleStat)]
+                                        ctypes.c_double] + [P] * 17 + [ctypes.POINTER(OracleStat)]
         L.oracle_rgf_energy.restype = ctypes.c_int
         L.oracle_rgf_batch.argtypes = [ctypes.POINTER(OracleOpts), ctypes.c_int64, ctypes.c_int64,
-                                       ctypes.c_int64, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P,
-                                       P, ctypes.c_int, ctypes.c_int]
+                                       ctypes.c_int64] + [P] * 19 + [ctypes.c_int, ctypes.c_int]
         L.oracle_rgf_batch.restype = ctypes.c_int
         L.oracle_calc_n_electron.argtypes = [P, P, ctypes.c_int64, P, ctypes.c_int64,
                                              ctypes.c_int64, ctypes.c_int64, P, P, P]
@@ -160,8 +158,12 @@ def _fortran3(a, nm, nx, dtype=np.complex128):
 
 def rgf_batch(Hii, H1i, E, mu, temp, opts: Opts | None = None, sig_lesser=None, sig_r=None,
               outputs=("ldos", "ndens", "pdens", "cur", "GRi1"), threads: int | None = None,
-              extended: bool = False):
+              extended: bool = False, Sii=None):
     """Run the C++ oracle over a batch of energies.
+
+    Sii=None: green_RGF_RS (S = I).  Sii given (same layout as Hii):
+    green_RGF_CMS (green_rgf.f90:4167-4383).  outputs may also name "GLi1"
+    and "GGi1".
 
     extended=False: FP64 with OpenBLAS, the reference's arithmetic.
     extended=True: the same algorithm in x87 80-bit long double with plain
@@ -182,8 +184,9 @@ def rgf_batch(Hii, H1i, E, mu, temp, opts: Opts | None = None, sig_lesser=None, 
     H1i = _fortran3(H1i, nm, nx)
     sl = None if sig_lesser is None else np.ascontiguousarray(sig_lesser, dtype=np.complex128)
     sr = None if sig_r is None else np.ascontiguousarray(sig_r, dtype=np.complex128)
+    Sii = None if Sii is None else _fortran3(Sii, nm, nx)
     out = {}
-    for name in ("ldos", "ndens", "pdens", "GRi1"):
+    for name in ("ldos", "ndens", "pdens", "GRi1", "GLi1", "GGi1"):
         out[name] = np.zeros((nE, nx, nm, nm), np.complex128) if name in outputs else None
     out["cur"] = np.zeros((nE, nx, nm, nm), np.float64) if "cur" in outputs else None
     tr = np.zeros(nE)
@@ -193,10 +196,11 @@ def rgf_batch(Hii, H1i, E, mu, temp, opts: Opts | None = None, sig_lesser=None, 
     if threads is None:
         threads = os.cpu_count() or 1
     o = opts.c()
-    rc = lib().oracle_rgf_batch(ctypes.byref(o), nm, nx, nE, _p(E), _p(mu), _p(temp), _p(Hii),
-                                _p(H1i), _p(sl), _p(sr), _p(out["ndens"]), _p(out["pdens"]),
+    rc = lib().oracle_rgf_batch(ctypes.byref(o), nm, nx, nE, _p(E), _p(mu), _p(temp), _p(Sii),
+                                _p(Hii), _p(H1i), _p(sl), _p(sr), _p(out["ndens"]), _p(out["pdens"]),
                                 _p(out["ldos"]), _p(tr), _p(tre), _p(out["cur"]), _p(out["GRi1"]),
-                                _p(T), _p(stats), int(threads), int(extended))
+                                _p(out["GLi1"]), _p(out["GGi1"]), _p(T), _p(stats), int(threads),
+                                int(extended))
     out.update(tr=tr, tre=tre, T=T, stats=stats, status=rc)
     return out
 

@@ -189,10 +189,11 @@ inline R ferm(R a) { return R(1) / (R(1) + std::exp(a)); }  // green_rgf.f90:444
 
 inline size_t nn(int nm) { return (size_t)nm * nm; }
 
-// sancho: green_rgf.f90:4451-4537 (S00 = identity at every call site).
+// sancho: green_rgf.f90:4451-4537.  S00 = nullptr is the identity (the
+// green_RGF_RS call sites); green_RGF_CMS passes Sii(:,:,1) / Sii(:,:,nx).
 // Returns the iteration count taken (nmax+1 encodes "not converged").
 template <typename R>
-int sancho(Work<R>& w, const OracleOpts& o, R E, const std::complex<R>* H00,
+int sancho(Work<R>& w, const OracleOpts& o, R E, const std::complex<R>* S00, const std::complex<R>* H00,
            const std::complex<R>* H10, std::complex<R>* G00, std::complex<R>* GBB) {
   typedef std::complex<R> cd;
   const int nm = w.nm;
@@ -203,10 +204,14 @@ int sancho(Work<R>& w, const OracleOpts& o, R E, const std::complex<R>* H00,
   for (int j = 0; j < nm; j++)
     for (int i = 0; i < nm; i++) H_01[i + (size_t)j * nm] = std::conj(H_10[j + (size_t)i * nm]);
   int taken = 0;
+  auto zS_minus = [&](const std::vector<cd>& H, cd* out) {  // out = z*S00 - H
+    for (size_t k = 0; k < n2; k++) out[k] = (S00 ? z * S00[k] : cd(0, 0)) - H[k];
+    if (!S00)
+      for (int i = 0; i < nm; i++) out[i + (size_t)i * nm] += z;
+  };
   for (int it = 1; it <= o.sancho_nmax; it++) {
     taken = it;
-    for (size_t k = 0; k < n2; k++) A[k] = -H_BB[k];
-    for (int i = 0; i < nm; i++) A[i + (size_t)i * nm] += z;
+    zS_minus(H_BB, A.data());
     w.invert(A.data());
     w.gemm('n', 'n', A.data(), H_10.data(), B.data());
     w.gemm('n', 'n', H_01.data(), B.data(), C.data());
@@ -229,11 +234,9 @@ int sancho(Work<R>& w, const OracleOpts& o, R E, const std::complex<R>* H00,
       taken = o.sancho_nmax + 1;
     }
   }
-  for (size_t k = 0; k < n2; k++) G00[k] = -H_SS[k];
-  for (int i = 0; i < nm; i++) G00[i + (size_t)i * nm] += z;
+  zS_minus(H_SS, G00);
   w.invert(G00);
-  for (size_t k = 0; k < n2; k++) GBB[k] = -H_BB[k];
-  for (int i = 0; i < nm; i++) GBB[i + (size_t)i * nm] += z;
+  zS_minus(H_BB, GBB);
   w.invert(GBB);
   return taken;
 }
@@ -249,8 +252,9 @@ namespace {
 
 template <typename R>
 int rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E_in, const double* mu,
-               const double* temp, const cd* Hii_in, const cd* H1i_in, const cd* sig_lesser_in,
-               const cd* sig_r_in, cd* ndens_out, cd* pdens_out, cd* ldos_out, double* tr,
+               const double* temp, const cd* Sii_in, const cd* Hii_in, const cd* H1i_in,
+               const cd* sig_lesser_in, const cd* sig_r_in, cd* ndens_out, cd* pdens_out,
+               cd* ldos_out, double* tr,
                double* tre, double* cur_out, cd* GRi1_out, cd* GLi1_out, cd* GGi1_out,
                double* T_out, OracleStat* st) {
   typedef std::complex<R> cd;
@@ -266,7 +270,11 @@ int rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E_in, 
   Work<R> w(nm, st);
   // inputs and outputs in the working precision
   const size_t nall = n2 * (size_t)nx;
-  std::vector<cd> Hii_v(Hii_in, Hii_in + nall), H1i_v(H1i_in, H1i_in + nall);
+  std::vector<cd> Hii_v(Hii_in, Hii_in + nall), H1i_v(H1i_in, H1i_in + nall), Sii_v;
+  if (Sii_in) Sii_v.assign(Sii_in, Sii_in + nall);
+  // green_RGF_CMS (green_rgf.f90:4167-4383) when an overlap is given
+  const bool cms = Sii_in != nullptr;
+  const cd* Sii = cms ? Sii_v.data() : nullptr;
   std::vector<cd> sl_v, sr_v, nd_v, pd_v, ld_v, gr_v, gl_v, gg_v;
   std::vector<R> cur_v;
   if (sig_lesser_in) sl_v.assign(sig_lesser_in, sig_lesser_in + nall);
@@ -296,12 +304,32 @@ int rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E_in, 
   };
   auto sigR = [&](int l, size_t k) { return sig_r ? blk(sig_r, l)[k] : cd(0.0, 0.0); };
   auto sigL = [&](int l, size_t k) { return sig_lesser ? blk(sig_lesser, l)[k] : cd(0.0, 0.0); };
+  // CMS multiplies the scattering self-energies by the overlap block:
+  // sigma_r_ph(l) S00 (:4204, :4226) and sigma_lesser_ph(l) S00 (:4211, :4240);
+  // RS adds them as they are.  SR[l-1] / SL[l-1] hold the per-block terms.
+  std::vector<std::vector<cd>> SRt, SLt;
+  if (cms) {
+    SRt.assign(nx, std::vector<cd>(n2, cd(0, 0)));
+    SLt.assign(nx, std::vector<cd>(n2, cd(0, 0)));
+    for (int l = 1; l <= nx; l++) {
+      if (sig_r) w.gemm('n', 'n', blk(sig_r, l), blk(Sii, l), SRt[l - 1].data());
+      if (sig_lesser) w.gemm('n', 'n', blk(sig_lesser, l), blk(Sii, l), SLt[l - 1].data());
+    }
+  }
+  auto sR = [&](int l, size_t k) { return cms ? SRt[l - 1][k] : sigR(l, k); };
+  auto sL = [&](int l, size_t k) { return cms ? SLt[l - 1][k] : sigL(l, k); };
   // The backward sweep's coupling block: reference uses H1i(:,:,l) (trap T3);
   // the consistent variant uses H_{l+1,l} = H1i(:,:,l+1).
   auto H1b = [&](int l) { return o.consistent ? blk(H1i, l + 1) : blk(H1i, l); };
 
   const R mul = mu[0], mur = mu[1], templ = temp[0], tempr = temp[1];
   const cd z(E, (R)o.eta_dev);
+  // A = z*S_ll - X (RS: S = I)
+  auto zS = [&](int l, const cd* X, cd* Aout) {
+    for (size_t k = 0; k < n2; k++) Aout[k] = (cms ? z * blk(Sii, l)[k] : cd(0, 0)) - X[k];
+    if (!cms)
+      for (int i = 0; i < nm; i++) Aout[i + (size_t)i * nm] += z;
+  };
   std::vector<cd> Gl(n2 * nx), Gln(n2 * nx);
   std::vector<cd> H00(n2), H10(n2), A(n2), B(n2), C(n2), D(n2), G00(n2), GBB(n2), GN0(n2),
       Gn(n2), Gp(n2), sig(n2), sigmal(n2), sigmar(n2), tmp(n2), GN1(n2), GN1b(n2);
@@ -312,10 +340,11 @@ int rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E_in, 
   if (cur) std::fill(cur, cur + n2 * nx, R(0));
 
   // ---- left contact (green_rgf.f90:3992-4012)
-  for (size_t k = 0; k < n2; k++) H00[k] = blk(Hii, 1)[k] + sigR(1, k);
+  for (size_t k = 0; k < n2; k++) H00[k] = blk(Hii, 1)[k] + sR(1, k);
   std::copy(blk(H1i, 1), blk(H1i, 1) + n2, H10.begin());
   adj(H10.data(), tmp.data());
-  st->sancho_iters_left = sancho(w, o, E, H00.data(), tmp.data(), G00.data(), GBB.data());
+  st->sancho_iters_left = sancho(w, o, E, cms ? blk(Sii, 1) : nullptr, H00.data(), tmp.data(),
+                                 G00.data(), GBB.data());
   w.gemm('n', 'n', H10.data(), G00.data(), A.data());
   w.gemm('n', 'c', A.data(), H10.data(), sigmal.data());
   {
@@ -323,11 +352,11 @@ int rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E_in, 
     for (int j = 0; j < nm; j++)
       for (int i = 0; i < nm; i++) {
         const size_t k = i + (size_t)j * nm;
-        sig[k] = -(sigmal[k] - std::conj(sigmal[j + (size_t)i * nm])) * f + sigL(1, k);
+        sig[k] = -(sigmal[k] - std::conj(sigmal[j + (size_t)i * nm])) * f + sL(1, k);
       }
   }
-  for (size_t k = 0; k < n2; k++) A[k] = -H00[k] - sigmal[k];
-  for (int i = 0; i < nm; i++) A[i + (size_t)i * nm] += z;
+  for (size_t k = 0; k < n2; k++) C[k] = H00[k] + sigmal[k];
+  zS(1, C.data(), A.data());
   w.invert(A.data());
   std::copy(A.begin(), A.end(), blkw(Gl.data(), 1));
   w.gemm('n', 'n', A.data(), sig.data(), B.data());
@@ -338,18 +367,18 @@ int rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E_in, 
 
   // ---- forward sweep (green_rgf.f90:4013-4030)
   for (int l = 2; l <= nx - 1; l++) {
-    for (size_t k = 0; k < n2; k++) H00[k] = blk(Hii, l)[k] + sigR(l, k);
+    for (size_t k = 0; k < n2; k++) H00[k] = blk(Hii, l)[k] + sR(l, k);
     std::copy(blk(H1i, l), blk(H1i, l) + n2, H10.begin());
     w.gemm('n', 'n', H10.data(), blkw(Gl.data(), l - 1), B.data());
     w.gemm('n', 'c', B.data(), H10.data(), C.data());
-    for (size_t k = 0; k < n2; k++) A[k] = -H00[k] - C[k];
-    for (int i = 0; i < nm; i++) A[i + (size_t)i * nm] += z;
+    for (size_t k = 0; k < n2; k++) C[k] += H00[k];
+    zS(l, C.data(), A.data());
     w.invert(A.data());
     std::copy(A.begin(), A.end(), blkw(Gl.data(), l));
     std::copy(blkw(Gln.data(), l - 1), blkw(Gln.data(), l - 1) + n2, sig.begin());
     w.gemm('n', 'n', H10.data(), sig.data(), B.data());
     w.gemm('n', 'c', B.data(), H10.data(), C.data());
-    for (size_t k = 0; k < n2; k++) C[k] += sigL(l, k);
+    for (size_t k = 0; k < n2; k++) C[k] += sL(l, k);
     w.gemm('n', 'n', A.data(), C.data(), B.data());
     w.gemm('n', 'c', B.data(), A.data(), Gn.data());
     std::copy(Gn.begin(), Gn.end(), blkw(Gln.data(), l));
@@ -360,15 +389,16 @@ int rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E_in, 
   }
 
   // ---- right contact and G_NN (green_rgf.f90:4031-4066)
-  for (size_t k = 0; k < n2; k++) H00[k] = blk(Hii, nx)[k] + sigR(nx, k);
+  for (size_t k = 0; k < n2; k++) H00[k] = blk(Hii, nx)[k] + sR(nx, k);
   std::copy(blk(H1i, nx), blk(H1i, nx) + n2, H10.begin());
-  st->sancho_iters_right = sancho(w, o, E, H00.data(), H10.data(), G00.data(), GBB.data());
+  st->sancho_iters_right = sancho(w, o, E, cms ? blk(Sii, nx) : nullptr, H00.data(), H10.data(),
+                                  G00.data(), GBB.data());
   w.gemm('c', 'n', H10.data(), G00.data(), A.data());
   w.gemm('n', 'n', A.data(), H10.data(), sigmar.data());
   w.gemm('n', 'n', H10.data(), blkw(Gl.data(), nx - 1), B.data());
   w.gemm('n', 'c', B.data(), H10.data(), C.data());
-  for (size_t k = 0; k < n2; k++) G00[k] = -H00[k] - sigmar[k] - C[k];
-  for (int i = 0; i < nm; i++) G00[i + (size_t)i * nm] += z;
+  for (size_t k = 0; k < n2; k++) C[k] += H00[k] + sigmar[k];
+  zS(nx, C.data(), G00.data());
   w.invert(G00.data());
   if (ldos) std::copy(G00.begin(), G00.end(), ldos + (size_t)(nx - 1) * n2);
   std::copy(blkw(Gln.data(), nx - 1), blkw(Gln.data(), nx - 1) + n2, sig.begin());
@@ -378,7 +408,7 @@ int rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E_in, 
   for (int j = 0; j < nm; j++)
     for (int i = 0; i < nm; i++) {
       const size_t k = i + (size_t)j * nm;
-      sig[k] = -(sigmar[k] - std::conj(sigmar[j + (size_t)i * nm])) * fR + C[k] + sigL(nx, k);
+      sig[k] = -(sigmar[k] - std::conj(sigmar[j + (size_t)i * nm])) * fR + C[k] + sL(nx, k);
     }
   w.gemm('n', 'n', G00.data(), sig.data(), B.data());
   w.gemm('n', 'c', B.data(), G00.data(), Gn.data());
@@ -453,8 +483,9 @@ int rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E_in, 
     if (cur)
       for (size_t k = 0; k < n2; k++) cur[(size_t)(l - 1) * n2 + k] -= A[k].real();
     if (GGi1) {
-      // Reproduces the reference: Glp is never filled (zero) and Gp keeps its
-      // value from the right closure (green_rgf.f90:4094-4103, trap T4).
+      // Reproduces the reference: Glp is never filled (zero); in RS Gp keeps
+      // its value from the right closure (green_rgf.f90:4094-4103, trap T4),
+      // in CMS it is the running G^> of block l+1 (:4313-4322).
       A = Gp;
       w.gemm('c', 'c', Gll, H10.data(), B.data());
       w.gemm('n', 'n', B.data(), A.data(), C.data());
@@ -486,7 +517,17 @@ int rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E_in, 
     w.gemm('n', 'c', B.data(), GN0.data(), C.data());
     for (size_t k = 0; k < n2; k++) Gn[k] += C[k];  // G<_{l,l}
     if (ndens) std::copy(Gn.begin(), Gn.end(), ndens + (size_t)(l - 1) * n2);
-    if (pdens)
+    if (cms) {
+      // CMS recurses G^> like G^< with the never-filled Glp (zero):
+      // Gp = Glp + g H10^H Gp H10 g^H + GN0 H10 Glp + Glp H10^H GN0^H  (:4353-4369)
+      A = Gp;
+      w.gemm('n', 'c', D.data(), H10.data(), B.data());
+      w.gemm('n', 'n', B.data(), A.data(), C.data());
+      w.gemm('n', 'n', C.data(), H10.data(), A.data());
+      w.gemm('n', 'c', A.data(), D.data(), C.data());
+      Gp = C;
+      if (pdens) std::copy(Gp.begin(), Gp.end(), pdens + (size_t)(l - 1) * n2);
+    } else if (pdens)
       for (int j = 0; j < nm; j++)
         for (int i = 0; i < nm; i++) {
           const size_t k = i + (size_t)j * nm;
@@ -536,24 +577,24 @@ int rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E_in, 
 }  // namespace
 
 extern "C" int oracle_rgf_energy(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E,
-                                 const double* mu, const double* temp, const cd* Hii,
+                                 const double* mu, const double* temp, const cd* Sii, const cd* Hii,
                                  const cd* H1i, const cd* sig_lesser, const cd* sig_r,
                                  cd* ndens, cd* pdens, cd* ldos, double* tr, double* tre,
                                  double* cur, cd* GRi1, cd* GLi1, cd* GGi1, double* T_out,
                                  OracleStat* st) {
-  return rgf_energy<double>(opts, nm64, nx64, E, mu, temp, Hii, H1i, sig_lesser, sig_r, ndens,
+  return rgf_energy<double>(opts, nm64, nx64, E, mu, temp, Sii, Hii, H1i, sig_lesser, sig_r, ndens,
                             pdens, ldos, tr, tre, cur, GRi1, GLi1, GGi1, T_out, st);
 }
 
 // The same computation in x87 extended precision (64-bit mantissa) with
 // plain loops: the ground truth that FP64 results are measured against.
 extern "C" int oracle_rgf_energy_ld(const OracleOpts* opts, int64_t nm64, int64_t nx64, double E,
-                                    const double* mu, const double* temp, const cd* Hii,
+                                    const double* mu, const double* temp, const cd* Sii, const cd* Hii,
                                     const cd* H1i, const cd* sig_lesser, const cd* sig_r,
                                     cd* ndens, cd* pdens, cd* ldos, double* tr, double* tre,
                                     double* cur, cd* GRi1, cd* GLi1, cd* GGi1, double* T_out,
                                     OracleStat* st) {
-  return rgf_energy<long double>(opts, nm64, nx64, E, mu, temp, Hii, H1i, sig_lesser, sig_r,
+  return rgf_energy<long double>(opts, nm64, nx64, E, mu, temp, Sii, Hii, H1i, sig_lesser, sig_r,
                                  ndens, pdens, ldos, tr, tre, cur, GRi1, GLi1, GGi1, T_out, st);
 }
 
@@ -561,13 +602,14 @@ extern "C" int oracle_rgf_energy_ld(const OracleOpts* opts, int64_t nm64, int64_
 // call, mirroring `!$omp parallel do ie` around green_RGF_RS
 // (green_rgf.f90:2916-2925) with single-threaded BLAS.  Hii/H1i are shared by
 // all points; per-point arrays are strided by nm*nm*nx elements (cur by the
-// same count of doubles).  Null arrays are skipped.
+// same count of doubles).  Null arrays are skipped.  Sii non-null runs
+// green_RGF_CMS instead of green_RGF_RS.
 extern "C" int oracle_rgf_batch(const OracleOpts* opts, int64_t nm, int64_t nx, int64_t nE,
                                 const double* E, const double* mu, const double* temp,
-                                const cd* Hii, const cd* H1i, const cd* sig_lesser,
+                                const cd* Sii, const cd* Hii, const cd* H1i, const cd* sig_lesser,
                                 const cd* sig_r, cd* ndens, cd* pdens, cd* ldos, double* tr,
-                                double* tre, double* cur, cd* GRi1, double* T_out,
-                                OracleStat* stats, int n_threads, int extended) {
+                                double* tre, double* cur, cd* GRi1, cd* GLi1, cd* GGi1,
+                                double* T_out, OracleStat* stats, int n_threads, int extended) {
   const size_t per = (size_t)nm * nm * nx;
   std::atomic<int64_t> next(0);
   std::atomic<int> worst(0);
@@ -577,11 +619,12 @@ extern "C" int oracle_rgf_batch(const OracleOpts* opts, int64_t nm, int64_t nx, 
       if (e >= nE) break;
       OracleStat st{};
       const int s = (extended ? oracle_rgf_energy_ld : oracle_rgf_energy)(
-          opts, nm, nx, E[e], mu, temp, Hii, H1i, sig_lesser ? sig_lesser + e * per : nullptr,
+          opts, nm, nx, E[e], mu, temp, Sii, Hii, H1i, sig_lesser ? sig_lesser + e * per : nullptr,
           sig_r ? sig_r + e * per : nullptr, ndens ? ndens + e * per : nullptr,
           pdens ? pdens + e * per : nullptr, ldos ? ldos + e * per : nullptr,
           tr ? tr + e : nullptr, tre ? tre + e : nullptr, cur ? cur + e * per : nullptr,
-          GRi1 ? GRi1 + e * per : nullptr, nullptr, nullptr, T_out ? T_out + e : nullptr, &st);
+          GRi1 ? GRi1 + e * per : nullptr, GLi1 ? GLi1 + e * per : nullptr,
+          GGi1 ? GGi1 + e * per : nullptr, T_out ? T_out + e : nullptr, &st);
       if (stats) stats[e] = st;
       int cur_w = worst.load();
       while ((s | cur_w) != cur_w && !worst.compare_exchange_weak(cur_w, s | cur_w)) {}

@@ -26,7 +26,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import perturbed_inputs, random_sigma, rel_err
+from conftest import compare, errors, perturbed_inputs, random_sigma, rel_err
 from liteqt_b200 import synthetic as S
 
 pytestmark = pytest.mark.gpu
@@ -66,42 +66,6 @@ def gpu_solve(R, Hii, H1i, E, opts, sl=None, sr=None, mu=MU, temp=None, outputs=
                                 T=out["T"], info=out["info"])
     out["rc"] = rc
     return out
-
-
-def errors(g, r, nm, H1i, skip_last_gri1=True):
-    errs = {}
-    errs["ldos"] = rel_err(g["ldos"], r["ldos"])
-    errs["ndens"] = rel_err(g["ndens"], r["ndens"])
-    errs["pdens"] = rel_err(g["pdens"], r["pdens"], scale=max(np.max(np.abs(r["ldos"])),
-                                                                np.max(np.abs(r["ndens"]))))
-    sl = slice(0, -1) if skip_last_gri1 else slice(None)
-    errs["GRi1"] = rel_err(g["GRi1"][:, sl], r["GRi1"][:, sl])
-    cur_scale = nm * np.max(np.abs(H1i)) * np.max(np.abs(r["ndens"]))
-    errs["cur"] = rel_err(g["cur"], r["cur"], scale=cur_scale)
-    trs = max(np.max(np.abs(r["tr"])), np.max(np.abs(r["tre"])), np.max(np.abs(r["T"])), 1e-300)
-    errs["tr"] = float(np.max(np.abs(g["tr"] - r["tr"])) / trs)
-    errs["tre"] = float(np.max(np.abs(g["tre"] - r["tre"])) / trs)
-    errs["T"] = float(np.max(np.abs(g["T"] - r["T"]) / np.maximum(1.0, np.abs(r["T"]))))
-    return errs
-
-
-def compare(g, r, nm, H1i, tol=TOL, truth=None, skip_last_gri1=True, floor=()):
-    """g: GPU outputs, r: FP64 oracle outputs, truth: 80-bit oracle outputs,
-    floor: FP64 oracle outputs on perturbed inputs (noise floor)."""
-    e_go = errors(g, r, nm, H1i, skip_last_gri1)
-    if truth is None:
-        bad = {k: v for k, v in e_go.items() if not v <= tol}
-        assert not bad, f"errors above {tol}: {bad} (all: {e_go})"
-        return e_go
-    e_gt = errors(g, truth, nm, H1i, skip_last_gri1)
-    e_rt = errors(r, truth, nm, H1i, skip_last_gri1)
-    for f in floor:
-        e_ft = errors(f, truth, nm, H1i, skip_last_gri1)
-        e_rt = {k: max(e_rt[k], e_ft[k]) for k in e_rt}
-    bad = {k: (e_go[k], e_gt[k], e_rt[k]) for k in e_go
-           if not (e_go[k] <= tol or e_gt[k] <= 8.0 * e_rt[k] + 1e-12) or not e_gt[k] < 1e-6}
-    assert not bad, f"(gpu-oracle, gpu-exact, oracle-exact) failing: {bad}"
-    return e_go
 
 
 def oracle_solve(Hii, H1i, E, oopts, sl=None, sr=None, extended=False):
