@@ -4,6 +4,7 @@
 ! Drop-in for the liteQT RGF routines:
 !   green_RGF_RS  (src/green_rgf.f90:3950, module green_rgf)
 !   RGF_G         (src/rgf_mod.f90:26,     module rgf_mod)
+!   green_RGF_CMS (src/green_rgf.f90:4167, module green_rgf; overlap Sii)
 ! The wrappers below keep the reference's argument lists, so the call sites
 ! (green_rgf.f90:2918-2923, :3174-3178, :735-739, :970-974, gw_sparse.f90:285-292)
 ! compile unchanged once `use rgf_cuda` replaces the module-local routine.
@@ -17,12 +18,13 @@ module rgf_cuda
   use, intrinsic :: iso_c_binding
   implicit none
   private
-  public :: green_RGF_RS, RGF_G, rgf_solve_energies_f, rgf_device_t, rgf_task_info_t
+  public :: green_RGF_RS, RGF_G, green_RGF_CMS, rgf_solve_energies_f, rgf_device_t, rgf_task_info_t
 
   type, bind(C) :: rgf_device_t
     integer(c_int64_t) :: nm, nx
     type(c_ptr) :: Hii, H1i
     real(c_double) :: mu(2), temp(2)
+    type(c_ptr) :: Sii
   end type rgf_device_t
 
   type, bind(C) :: rgf_task_info_t
@@ -49,6 +51,16 @@ module rgf_cuda
       type(c_ptr), value :: Hii, H1i, sl, sg, sr, ndens, pdens, ldos, cur, GRi1, GLi1, GGi1
       real(c_double), intent(inout) :: tr, tre
     end function c_rgf_rgf_g
+
+    integer(c_int) function c_rgf_green_rgf_cms(ctx, temp, nm, nx, E, mu, Sii, Hii, H1i, sl, sg, sr, &
+        ndens, pdens, ldos, tr, tre, cur, GRi1, GLi1, GGi1) bind(C, name="rgf_green_rgf_cms")
+      import :: c_int, c_ptr, c_double, c_int64_t
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: temp(2), E, mu(2)
+      integer(c_int64_t), intent(in) :: nm, nx
+      type(c_ptr), value :: Sii, Hii, H1i, sl, sg, sr, ndens, pdens, ldos, cur, GRi1, GLi1, GGi1
+      real(c_double), intent(inout) :: tr, tre
+    end function c_rgf_green_rgf_cms
 
     integer(c_int) function c_rgf_solve_energies(ctx, device, nen, E, sl, sr, ldos, ndens, pdens, &
         GRi1, cur, tr, tre, T, info, stream) bind(C, name="rgf_solve_energies")
@@ -133,6 +145,27 @@ contains
     call check(rc, 'RGF_G')
   end subroutine RGF_G
 
+  ! green_RGF_CMS with the reference's argument list (src/green_rgf.f90:4167).
+  subroutine green_RGF_CMS(TEMP, nm, nx, E, mu, Sii, Hii, H1i, sigma_lesser_ph, sigma_greater_ph, &
+      sigma_r_ph, ndens, pdens, ldos, tr, tre, cur, GRi1, GLi1, GGi1)
+    integer, intent(in) :: nm, nx
+    real(8), intent(in) :: E, mu(2), temp(2)
+    complex(8), intent(in), target, dimension(nm,nm,nx) :: sigma_lesser_ph, sigma_greater_ph, sigma_r_ph
+    complex(8), intent(in), target, dimension(nm,nm,nx) :: Sii, Hii, H1i
+    complex(8), intent(inout), target, dimension(nm,nm,nx) :: ldos, ndens, pdens
+    real(8), intent(inout), target, dimension(nm,nm,nx) :: cur
+    complex(8), intent(inout), target, dimension(nm,nm,nx), optional :: GRi1, GLi1, GGi1
+    real(8), intent(inout) :: tr, tre
+    integer(c_int64_t) :: nm8, nx8
+    integer(c_int) :: rc
+    nm8 = nm
+    nx8 = nx
+    rc = c_rgf_green_rgf_cms(c_null_ptr, temp, nm8, nx8, E, mu, c_loc(Sii), c_loc(Hii), c_loc(H1i), &
+        c_loc(sigma_lesser_ph), c_loc(sigma_greater_ph), c_loc(sigma_r_ph), c_loc(ndens), &
+        c_loc(pdens), c_loc(ldos), tr, tre, c_loc(cur), opt_ptr(GRi1), opt_ptr(GLi1), opt_ptr(GGi1))
+    call check(rc, 'green_RGF_CMS')
+  end subroutine green_RGF_CMS
+
   ! All energies of one k-point in one launch: replaces
   !   !$omp do; do ie=1,nen; call green_RGF_RS(...); enddo
   ! (green_rgf.f90:2916-2925) for arrays g(nm,nm,nx,nen).
@@ -154,6 +187,7 @@ contains
     dev%H1i = c_loc(H1i)
     dev%mu = mu
     dev%temp = temp
+    dev%Sii = c_null_ptr
     rc = c_rgf_solve_energies(ctx, dev, int(nen, c_int64_t), c_loc(En), c_loc(sigma_lesser), &
         c_loc(sigma_r), c_loc(g_r), c_loc(g_lesser), c_loc(g_greater), c_loc(g_r_i1), c_loc(cur), &
         c_loc(tr), c_loc(tre), c_null_ptr, c_null_ptr, c_null_ptr)

@@ -87,13 +87,21 @@ typedef struct rgf_ctx rgf_ctx;
 /* One device (Hamiltonian) shared by many energy points.  Hii and H1i are
  * (nm,nm,nx); H1i(:,:,l) couples block l-1 to block l (forward-sweep meaning),
  * H1i(:,:,1) and Hii(:,:,1) / Hii(:,:,nx), H1i(:,:,nx) also define the two
- * semi-infinite leads, exactly as in green_RGF_RS. */
+ * semi-infinite leads, exactly as in green_RGF_RS.
+ * Sii: NULL for an orthogonal basis (green_RGF_RS / RGF_G); otherwise the
+ * (nm,nm,nx) overlap blocks of a non-orthogonal basis, which selects
+ * green_RGF_CMS (src/green_rgf.f90:4167-4383): z*Sii(:,:,l) in place of z*I,
+ * sigma_r_ph(:,:,l)*Sii(:,:,l) and sigma_lesser_ph(:,:,l)*Sii(:,:,l) in place
+ * of the self-energies, Sancho-Rubio leads with the end blocks' overlap, and
+ * G^>_ll (pdens, l < nx) and GGi1 from that routine's own recursion through
+ * the never-filled Glp (zero) instead of G^> = G^< + G^R - G^A. */
 typedef struct rgf_device {
   int64_t nm, nx;
   const rgf_c16* Hii;
   const rgf_c16* H1i;
   double mu[2];            /* (muL, muR) eV */
   double temp[2];          /* (TL, TR) K */
+  const rgf_c16* Sii;      /* overlap blocks, or NULL = identity */
 } rgf_device;
 
 /* One (device, k, E) task: one call of green_RGF_RS.  Inputs and outputs are
@@ -215,6 +223,15 @@ RGF_API int rgf_rgf_g(rgf_ctx* ctx, const double* temperature, const int64_t* nm
               rgf_c16* pdens, rgf_c16* ldos, double* cur, rgf_c16* GRi1, rgf_c16* GLi1,
               rgf_c16* GGi1);
 
+/* Drop-in for green_RGF_CMS (src/green_rgf.f90:4167): green_RGF_RS's
+ * arguments with the overlap blocks Sii before Hii, as in the reference. */
+RGF_API int rgf_green_rgf_cms(rgf_ctx* ctx, const double* temp, const int64_t* nm, const int64_t* nx,
+                      const double* E, const double* mu, const rgf_c16* Sii, const rgf_c16* Hii,
+                      const rgf_c16* H1i, const rgf_c16* sigma_lesser_ph,
+                      const rgf_c16* sigma_greater_ph, const rgf_c16* sigma_r_ph, rgf_c16* ndens,
+                      rgf_c16* pdens, rgf_c16* ldos, double* tr, double* tre, double* cur,
+                      rgf_c16* GRi1, rgf_c16* GLi1, rgf_c16* GGi1);
+
 /* Strided batch over the energies of one device, in the layout the reference
  * drivers allocate: g(nm,nm,nx,nen) (green_rgf.f90:2880-2890, one ik slice).
  * Any array may be NULL.  Equivalent to nen calls of green_RGF_RS. */
@@ -236,7 +253,8 @@ RGF_API int rgf_solve_energies(rgf_ctx* ctx, const rgf_device* device, int64_t n
  * receive the derivatives of the Landauer current
  *   I = spindeg * e0^2/(2 pi hbar) * dE * sum_e T(E_e) (f_L(E_e) - f_R(E_e)),
  * with dE = E[1] - E[0] and the constants of green_rgf.f90:18-24.  T, dTdV and
- * dTds may be host or device memory; E, dIdV and dIds are host memory. */
+ * dTds may be host or device memory; E, dIdV and dIds are host memory.
+ * Orthogonal basis only (device->Sii must be NULL). */
 RGF_API int rgf_adjoint_energies(rgf_ctx* ctx, const rgf_device* device, int64_t nen,
                                  const double* E, double* T, double* dTdV, double* dTds,
                                  double spindeg, double* dIdV, double* dIds,

@@ -337,6 +337,7 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
     const size_t bytes = (size_t)devices[d].nm * devices[d].nm * devices[d].nx * sizeof(rgf_c16);
     sg.add(devices[d].Hii, bytes, true, false);
     sg.add(devices[d].H1i, bytes, true, false);
+    sg.add(devices[d].Sii, bytes, true, false);
   }
   for (int64_t t = 0; t < n_tasks; t++) {
     const rgf_task& k = tasks[t];
@@ -370,6 +371,7 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
     ddev[d].nx = devices[d].nx;
     ddev[d].Hii = (const double2*)sg.resolve(devices[d].Hii, sbase);
     ddev[d].H1i = (const double2*)sg.resolve(devices[d].H1i, sbase);
+    ddev[d].Sii = (const double2*)sg.resolve(devices[d].Sii, sbase);
     for (int i = 0; i < 2; i++) {
       ddev[d].mu[i] = devices[d].mu[i];
       ddev[d].temp[i] = devices[d].temp[i];
@@ -472,6 +474,7 @@ extern "C" int rgf_adjoint_energies(rgf_ctx* c, const rgf_device* v, int64_t nen
     return fail(RGF_E_UNSUPPORTED, "nm=%lld unsupported (multiple of 8 in [8,%d])", (long long)v->nm, kMaxNb);
   if (v->nx < 2) return fail(RGF_E_ARG, "nx < 2");
   if (!v->Hii || !v->H1i) return fail(RGF_E_ARG, "Hii/H1i is NULL");
+  if (v->Sii) return fail(RGF_E_UNSUPPORTED, "the adjoint is for an orthogonal basis (Sii must be NULL)");
   if (!(v->temp[0] > 0.0) || !(v->temp[1] > 0.0)) return fail(RGF_E_ARG, "temperature must be > 0");
   if ((dIdV || dIds) && nen < 2) return fail(RGF_E_ARG, "the current needs at least two energies");
   RGF_CUDA(cudaSetDevice(c->device));
@@ -495,6 +498,7 @@ extern "C" int rgf_adjoint_energies(rgf_ctx* c, const rgf_device* v, int64_t nen
   const size_t grad_bytes = sizeof(double) * (size_t)nen * (nx + 2);
   double* dT_d = dTdV ? (double*)sg.resolve(dTdV, sbase) : nullptr;
   DDev dd;
+  std::memset(&dd, 0, sizeof(dd));
   dd.nm = nm;
   dd.nx = nx;
   dd.Hii = (const double2*)sg.resolve(v->Hii, sbase);
@@ -621,7 +625,7 @@ rgf_ctx* default_ctx(double boltz, int* rc) {
 }
 
 int solve_one(rgf_ctx* ctx, double boltz, const double* temp, const int64_t* nm, const int64_t* nx,
-              const double* E, const double* mu, const rgf_c16* Hii, const rgf_c16* H1i,
+              const double* E, const double* mu, const rgf_c16* Sii, const rgf_c16* Hii, const rgf_c16* H1i,
               const rgf_c16* sl, const rgf_c16* sr, rgf_c16* ndens, rgf_c16* pdens, rgf_c16* ldos,
               double* tr, double* tre, double* cur, rgf_c16* GRi1, rgf_c16* GLi1, rgf_c16* GGi1) {
   if (!temp || !nm || !nx || !E || !mu) return fail(RGF_E_ARG, "NULL scalar argument");
@@ -635,8 +639,10 @@ int solve_one(rgf_ctx* ctx, double boltz, const double* temp, const int64_t* nm,
     ctx->opts.boltz = boltz;
   }
   rgf_device d;
+  std::memset(&d, 0, sizeof(d));
   d.nm = *nm;
   d.nx = *nx;
+  d.Sii = Sii;
   d.Hii = Hii;
   d.H1i = H1i;
   d.mu[0] = mu[0];
@@ -677,7 +683,20 @@ extern "C" int rgf_green_rgf_rs(rgf_ctx* ctx, const double* temp, const int64_t*
                                 double* tre, double* cur, rgf_c16* GRi1, rgf_c16* GLi1,
                                 rgf_c16* GGi1) {
   (void)sigma_greater_ph;  // unused by the reference as well
-  return solve_one(ctx, 8.61734e-05, temp, nm, nx, E, mu, Hii, H1i, sigma_lesser_ph, sigma_r_ph,
+  return solve_one(ctx, 8.61734e-05, temp, nm, nx, E, mu, nullptr, Hii, H1i, sigma_lesser_ph, sigma_r_ph,
+                   ndens, pdens, ldos, tr, tre, cur, GRi1, GLi1, GGi1);
+}
+
+extern "C" int rgf_green_rgf_cms(rgf_ctx* ctx, const double* temp, const int64_t* nm, const int64_t* nx,
+                                 const double* E, const double* mu, const rgf_c16* Sii,
+                                 const rgf_c16* Hii, const rgf_c16* H1i,
+                                 const rgf_c16* sigma_lesser_ph, const rgf_c16* sigma_greater_ph,
+                                 const rgf_c16* sigma_r_ph, rgf_c16* ndens, rgf_c16* pdens,
+                                 rgf_c16* ldos, double* tr, double* tre, double* cur, rgf_c16* GRi1,
+                                 rgf_c16* GLi1, rgf_c16* GGi1) {
+  (void)sigma_greater_ph;  // unused by the reference as well
+  if (!Sii) return fail(RGF_E_ARG, "green_RGF_CMS needs the overlap blocks Sii");
+  return solve_one(ctx, 8.61734e-05, temp, nm, nx, E, mu, Sii, Hii, H1i, sigma_lesser_ph, sigma_r_ph,
                    ndens, pdens, ldos, tr, tre, cur, GRi1, GLi1, GGi1);
 }
 
@@ -688,7 +707,7 @@ extern "C" int rgf_rgf_g(rgf_ctx* ctx, const double* temperature, const int64_t*
                          double* tre, rgf_c16* ndens, rgf_c16* pdens, rgf_c16* ldos, double* cur,
                          rgf_c16* GRi1, rgf_c16* GLi1, rgf_c16* GGi1) {
   (void)sigma_greater_ph;
-  return solve_one(ctx, 8.617333262e-05, temperature, nm, nx, E, mu, Hii, H1i, sigma_lesser_ph,
+  return solve_one(ctx, 8.617333262e-05, temperature, nm, nx, E, mu, nullptr, Hii, H1i, sigma_lesser_ph,
                    sigma_r_ph, ndens, pdens, ldos, tr, tre, cur, GRi1, GLi1, GGi1);
 }
 
@@ -751,7 +770,7 @@ extern "C" int rgf_plan_create(rgf_ctx* c, const rgf_device* devices, int32_t n_
   RGF_CUDA(cudaSetDevice(c->device));
   auto dev_ok = [](const void* p) { return !p || is_device_ptr(p); };
   for (int32_t d = 0; d < n_devices; d++)
-    if (!dev_ok(devices[d].Hii) || !dev_ok(devices[d].H1i))
+    if (!dev_ok(devices[d].Hii) || !dev_ok(devices[d].H1i) || !dev_ok(devices[d].Sii))
       return fail(RGF_E_ARG, "device %d: plan arrays must be device memory", d);
   const bool want_T = c->opts.want_T != 0;
   std::vector<DDev> ddev(n_devices);
@@ -760,6 +779,7 @@ extern "C" int rgf_plan_create(rgf_ctx* c, const rgf_device* devices, int32_t n_
     ddev[d].nx = devices[d].nx;
     ddev[d].Hii = (const double2*)devices[d].Hii;
     ddev[d].H1i = (const double2*)devices[d].H1i;
+    ddev[d].Sii = (const double2*)devices[d].Sii;
     for (int i = 0; i < 2; i++) {
       ddev[d].mu[i] = devices[d].mu[i];
       ddev[d].temp[i] = devices[d].temp[i];

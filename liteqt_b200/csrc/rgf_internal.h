@@ -29,6 +29,7 @@ struct DDev {
   const double2* H1i;
   double mu[2];
   double temp[2];
+  const double2* Sii;      // overlap blocks (green_RGF_CMS), or NULL = identity
 };
 
 // One task, device pointers only (NULL = absent).

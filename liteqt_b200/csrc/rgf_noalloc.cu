@@ -69,8 +69,8 @@ extern "C" int rgf_solve_energies_noalloc(const rgf_opts* opts, const rgf_device
   if (nm < 8 || nm > kMaxNb || nm % 8 != 0) return err(RGF_E_UNSUPPORTED, "nm must be a multiple of 8 in [8, 256]");
   if (nx < 2) return err(RGF_E_ARG, "nx < 2");
   if (!(device->temp[0] > 0.0) || !(device->temp[1] > 0.0)) return err(RGF_E_ARG, "temperature must be > 0");
-  const void* arrays[] = {device->Hii, device->H1i, sigma_lesser, sigma_r, ldos, ndens, pdens,
-                          GRi1, cur, tr, tre, T};
+  const void* arrays[] = {device->Hii, device->H1i, device->Sii, sigma_lesser, sigma_r, ldos, ndens,
+                          pdens, GRi1, cur, tr, tre, T};
   if (!device->Hii || !device->H1i) return err(RGF_E_ARG, "Hii / H1i is NULL");
   for (const void* a : arrays)
     if (a && !on_device(a))
@@ -108,10 +108,12 @@ extern "C" int rgf_solve_energies_noalloc(const rgf_opts* opts, const rgf_device
   cudaStream_t st = (cudaStream_t)stream;
 
   DDev dd;
+  std::memset(&dd, 0, sizeof(dd));
   dd.nm = nm;
   dd.nx = nx;
   dd.Hii = (const double2*)device->Hii;
   dd.H1i = (const double2*)device->H1i;
+  dd.Sii = (const double2*)device->Sii;
   for (int i = 0; i < 2; i++) { dd.mu[i] = device->mu[i]; dd.temp[i] = device->temp[i]; }
   const size_t per = (size_t)nm * nm * nx;
   std::vector<DTask> tasks((size_t)nen);

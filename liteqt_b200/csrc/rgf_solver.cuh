@@ -44,6 +44,7 @@ enum TmpBlock {
   T_H00 = 0, T_SA, T_SB, T_HBB, T_HSS, T_H10A, T_H10B, T_H01A, T_H01B, T_GS,
   T_SIGL, T_SIGR, T_SIG, T_F1, T_F2, T_F3, T_F4, T_GN1A, T_GN1B, T_G00A,
   T_G00B, T_GNA, T_GNB, T_Q1, T_Q2, T_Q3, T_Q4, T_R5, T_INV, T_RT,
+  T_SRS, T_SLS,  // green_RGF_CMS: sigma_r_ph S_ll, sigma_lesser_ph S_ll of the current block
   T_COUNT,
   // aliases (lifetimes do not overlap)
   T_R7 = T_F4, T_P1 = T_F1, T_P2 = T_F2, T_P3 = T_F3, T_P4 = T_SIG,
@@ -143,10 +144,19 @@ struct Solver {
     if (ops.invert(n, dst, dst2)) status |= RGF_ST_SINGULAR;
   }
 
-  // sancho (green_rgf.f90:4451-4537) with S00 = I.  H00 is a slot block; the
-  // coupling argument is H10arg = conj_src ? src^H : src.  Result -> GS.
+  // z*S - h for element (i, j): S = I (S == nullptr) or the overlap block S.
+  __device__ __forceinline__ static double2 zs_minus(double2 z, const double2* S, int i, int j,
+                                                     int idx, double2 h) {
+    if (S) return csub(cmul(z, S[idx]), h);
+    return (i == j) ? make_double2(z.x - h.x, z.y - h.y) : make_double2(-h.x, -h.y);
+  }
+
+  // sancho (green_rgf.f90:4451-4537); S00 = nullptr is the identity (the
+  // green_RGF_RS call sites), green_RGF_CMS passes its end blocks' overlap.
+  // H00 is a slot block; the coupling argument is H10arg = conj_src ? src^H :
+  // src.  Result -> GS.
   __device__ int sancho(double E, const double2* H00, const double2* src, bool conj_src,
-                        double2* GS) {
+                        double2* GS, const double2* S00 = nullptr) {
     const int nn = n;
     const double2 z = make_double2(E, o.eta_lead);
     double2 *H10 = tmp(T_H10A), *H10n = tmp(T_H10B), *H01 = tmp(T_H01A), *H01n = tmp(T_H01B);
@@ -163,10 +173,7 @@ struct Solver {
     for (int it = 1; it <= o.sancho_nmax; it++) {
       taken = it;
       // A = inv(z*S00 - H_BB)
-      for_each_elem(n, [&](int i, int j, int idx) {
-        const double2 h = HBB[idx];
-        X[idx] = (i == j) ? make_double2(z.x - h.x, z.y - h.y) : make_double2(-h.x, -h.y);
-      });
+      for_each_elem(n, [&](int i, int j, int idx) { X[idx] = zs_minus(z, S00, i, j, idx, HBB[idx]); });
       __syncthreads();
       invert_X(SA);
       gemm_store(SA, false, H10, false, SB);                         // B = A H_10
@@ -198,10 +205,7 @@ struct Solver {
       }
     }
     // G00 = inv(z*S00 - H_SS); the reference's GBB inverse is unused and skipped
-    for_each_elem(n, [&](int i, int j, int idx) {
-      const double2 h = HSS[idx];
-      X[idx] = (i == j) ? make_double2(z.x - h.x, z.y - h.y) : make_double2(-h.x, -h.y);
-    });
+    for_each_elem(n, [&](int i, int j, int idx) { X[idx] = zs_minus(z, S00, i, j, idx, HSS[idx]); });
     __syncthreads();
     invert_X(GS);
     return taken;
@@ -219,29 +223,44 @@ struct Solver {
     auto blk = [&](const double2* base, int l) { return base + (size_t)l * n2; };
     auto wblk = [&](double2* base, int l) { return base + (size_t)l * n2; };
     const bool want_T = o.want_T && tk.T;
+    // green_RGF_CMS (overlap given): z*S_ll, and the scattering self-energies
+    // enter as sigma_r_ph(l) S_ll and sigma_lesser_ph(l) S_ll (:4203-4211,
+    // :4225-4240, :4258-4265); green_RGF_RS adds them as they are.
+    const double2* Sii = dv.Sii;
+    const bool cms = Sii != nullptr;
+    auto S_l = [&](int l) -> const double2* { return cms ? blk(Sii, l) : nullptr; };
+    auto scat = [&](const double2* sg, int l, int slot) -> const double2* {
+      if (!sg) return nullptr;
+      if (!cms) return blk(sg, l);
+      gemm_store(blk(sg, l), false, blk(Sii, l), false, tmp(slot));
+      return tmp(slot);
+    };
 
     // ------------------------------------------------ left contact
     double2* H00 = tmp(T_H00);
-    for_each_elem(n, [&](int, int, int idx) {
-      H00[idx] = sr ? cadd(Hii[idx], sr[idx]) : Hii[idx];
-    });
-    __syncthreads();
+    {
+      const double2* sr0 = scat(sr, 0, T_SRS);
+      for_each_elem(n, [&](int, int, int idx) {
+        H00[idx] = sr0 ? cadd(Hii[idx], sr0[idx]) : Hii[idx];
+      });
+      __syncthreads();
+    }
     const double2* H10 = blk(H1i, 0);
-    const int itL = sancho(E, H00, H10, true, tmp(T_GS));
+    const int itL = sancho(E, H00, H10, true, tmp(T_GS), S_l(0));
     double2* sigmal = tmp(T_SIGL);
     gemm_store(H10, false, tmp(T_GS), false, tmp(T_F1));            // A = H10 G00
     gemm_store(tmp(T_F1), false, H10, true, sigmal);                // sigmal = A H10^H
     {
       const double fl = fermi((E - mul) / (o.boltz * templ));
       double2* sig = tmp(T_SIG);
+      const double2* sl0 = scat(sl, 0, T_SLS);
+      const double2* S0 = S_l(0);
       for_each_elem(n, [&](int i, int j, int idx) {
         const double2 s = sigmal[idx], st = cconj(sigmal[j + i * nn]);
         double2 v = cscale(csub(s, st), -fl);
-        if (sl) v = cadd(v, sl[idx]);
+        if (sl0) v = cadd(v, sl0[idx]);
         sig[idx] = v;
-        const double2 h = H00[idx];
-        double2 a = (i == j) ? make_double2(z.x - h.x, z.y - h.y) : make_double2(-h.x, -h.y);
-        X[idx] = csub(a, s);                                         // A = z S00 - H00 - sigmal
+        X[idx] = csub(zs_minus(z, S0, i, j, idx, H00[idx]), s);      // A = z S00 - H00 - sigmal
       });
       __syncthreads();
     }
@@ -256,14 +275,14 @@ struct Solver {
     for (int l = 1; l <= nx - 2; l++) {
       const double2* H = blk(H1i, l);
       const double2* Hl = blk(Hii, l);
-      const double2* srl = sr ? blk(sr, l) : nullptr;
-      const double2* sll = sl ? blk(sl, l) : nullptr;
+      const double2* srl = scat(sr, l, T_SRS);
+      const double2* sll = scat(sl, l, T_SLS);
+      const double2* Sl = S_l(l);
       gemm_store(H, false, Gl(l - 1), false, tmp(T_F1));            // B = H10 Gl(l-1)
-      gemm(tmp(T_F1), false, H, true, [&](int i, int j, double2 v) { // A = z - H00 - B H10^H
+      gemm(tmp(T_F1), false, H, true, [&](int i, int j, double2 v) { // A = z S - H00 - B H10^H
         const int idx = i + j * nn;
         const double2 h = srl ? cadd(Hl[idx], srl[idx]) : Hl[idx];
-        const double2 a = (i == j) ? make_double2(z.x - h.x, z.y - h.y) : make_double2(-h.x, -h.y);
-        X[idx] = csub(a, v);
+        X[idx] = csub(zs_minus(z, Sl, i, j, idx, h), v);
       });
       invert_X(Gl(l));
       gemm_store(H, false, Gln(l - 1), false, tmp(T_F2));           // B = H10 Gln(l-1)
@@ -285,26 +304,25 @@ struct Solver {
     {
       const int l = nx - 1;
       const double2* Hl = blk(Hii, l);
-      const double2* srl = sr ? blk(sr, l) : nullptr;
-      const double2* sll = sl ? blk(sl, l) : nullptr;
+      const double2* srl = scat(sr, l, T_SRS);
       for_each_elem(n, [&](int, int, int idx) {
         H00[idx] = srl ? cadd(Hl[idx], srl[idx]) : Hl[idx];
       });
       __syncthreads();
     }
     const double2* H = blk(H1i, nx - 1);
-    const int itR = sancho(E, H00, H, false, tmp(T_GS));
+    const int itR = sancho(E, H00, H, false, tmp(T_GS), S_l(nx - 1));
     double2* sigmar = tmp(T_SIGR);
     gemm_store(H, true, tmp(T_GS), false, tmp(T_F1));               // A = H10^H G00
     gemm_store(tmp(T_F1), false, H, false, sigmar);                 // sigmar = A H10
     gemm_store(H, false, Gl(nx - 2), false, tmp(T_F2));             // B = H10 Gl(nx-1)
-    gemm(tmp(T_F2), false, H, true, [&](int i, int j, double2 v) {   // G00 = z - H00 - sigmar - B H10^H
-      const int idx = i + j * nn;
-      const double2 h = H00[idx];
-      double2 a = (i == j) ? make_double2(z.x - h.x, z.y - h.y) : make_double2(-h.x, -h.y);
-      a = csub(a, sigmar[idx]);
-      X[idx] = csub(a, v);
-    });
+    {
+      const double2* SN = S_l(nx - 1);
+      gemm(tmp(T_F2), false, H, true, [&](int i, int j, double2 v) { // G00 = z S - H00 - sigmar - B H10^H
+        const int idx = i + j * nn;
+        X[idx] = csub(csub(zs_minus(z, SN, i, j, idx, H00[idx]), sigmar[idx]), v);
+      });
+    }
     double2* G00 = tmp(T_G00A);
     double2* G00n = tmp(T_G00B);
     double2* Gn = tmp(T_GNA);
@@ -313,7 +331,7 @@ struct Solver {
     const double fR = fermi((E - mur) / (o.boltz * templ));      // TEMPl: as the reference (:4051)
     gemm_store(H, false, Gln(nx - 2), false, tmp(T_F3));            // B = H10 Gln(nx-1)
     {
-      const double2* sll = sl ? blk(sl, nx - 1) : nullptr;
+      const double2* sll = scat(sl, nx - 1, T_SLS);
       gemm(tmp(T_F3), false, H, true, [&](int i, int j, double2 v) { // sig = -(sR - sR^H) fR + C + sig<
         const int idx = i + j * nn;
         const double2 s = sigmar[idx], st = cconj(sigmar[j + i * nn]);
@@ -326,7 +344,8 @@ struct Solver {
     {
       double2* nd = tk.ndens ? wblk(tk.ndens, nx - 1) : nullptr;
       double2* pd = tk.pdens ? wblk(tk.pdens, nx - 1) : nullptr;
-      double2* gpn = tk.GGi1 ? tmp(T_GPN) : nullptr;
+      // the running G^> of green_RGF_CMS's recursion starts from this block's
+      double2* gpn = (tk.GGi1 || (cms && tk.pdens)) ? tmp(T_GPN) : nullptr;
       gemm(tmp(T_F4), false, G00, true, [&](int i, int j, double2 v) {  // Gn = B G00^H
         const int idx = i + j * nn;
         Gn[idx] = v;
@@ -412,7 +431,8 @@ struct Solver {
             curl[idx] = curl[idx] - v.x;
           });
       }
-      if (tk.GGi1) {  // the reference's GGi1: Gl^H H10^H Gp(nx) (+ Glp terms, which are zero)
+      if (tk.GGi1) {  // the reference's GGi1: Gl^H H10^H Gp (+ Glp terms, which are zero); Gp
+                      // is G^>_NN in green_RGF_RS, the running G^>_{l+1} in green_RGF_CMS
         gemm_store(gl, true, Hb, true, tmp(T_R1));
         gemm_store(tmp(T_R1), false, tmp(T_GPN), false, wblk(tk.GGi1, l));
       }
@@ -439,13 +459,24 @@ struct Solver {
       });
       {
         double2* nd = tk.ndens ? wblk(tk.ndens, l) : nullptr;
-        double2* pd = tk.pdens ? wblk(tk.pdens, l) : nullptr;
+        double2* pd = (tk.pdens && !cms) ? wblk(tk.pdens, l) : nullptr;
         gemm(tmp(T_Q3), false, GN0, true, [&](int i, int j, double2 v) {
           const int idx = i + j * nn;
           const double2 w = cadd(Gnn[idx], v);                      // Gn += Gl< H10^H GN0^H
           Gnn[idx] = w;
           if (nd) nd[idx] = w;
           if (pd) pd[idx] = cadd(w, csub(G00n[idx], cconj(G00n[j + i * nn])));
+        });
+      }
+      if (cms && (tk.pdens || tk.GGi1)) {
+        // green_RGF_CMS's G^> (:4353-4369) with its never-filled Glp (zero):
+        // Gp = Gl H10^H Gp H10 Gl^H
+        double2* pd = tk.pdens ? wblk(tk.pdens, l) : nullptr;
+        gemm_store(tmp(T_Q1), false, tmp(T_GPN), false, tmp(T_R1));
+        gemm(tmp(T_R1), false, tmp(T_Q1), true, [&](int i, int j, double2 v) {
+          const int idx = i + j * nn;
+          tmp(T_GPN)[idx] = v;
+          if (pd) pd[idx] = v;
         });
       }
       double2* t1 = G00; G00 = G00n; G00n = t1;

@@ -47,7 +47,7 @@ EXPORTS = (
     "rgf_terminal_current", "rgf_calc_n_electron", "rgf_last_error", "rgf_version",
     "rgf_ctx_get_stats", "rgf_adjoint_energies", "rgf_solve_energies_noalloc",
     "rgf_noalloc_last_error", "rgf_calc_block_current", "rgf_plan_create", "rgf_plan_execute",
-    "rgf_plan_destroy", "rgf_autotune", "rgf_variant_name",
+    "rgf_plan_destroy", "rgf_autotune", "rgf_variant_name", "rgf_green_rgf_cms",
 )
 
 # kernel variant ids (rgf_variant_name)
@@ -76,6 +76,7 @@ class c_device(ctypes.Structure):
         ("nm", ctypes.c_int64), ("nx", ctypes.c_int64),
         ("Hii", ctypes.c_void_p), ("H1i", ctypes.c_void_p),
         ("mu", ctypes.c_double * 2), ("temp", ctypes.c_double * 2),
+        ("Sii", ctypes.c_void_p),
     ]
 
 
@@ -130,6 +131,8 @@ def load(path: str = LIB_PATH):
                                   ctypes.POINTER(c_task), ctypes.c_int64, P, P]
     L.rgf_green_rgf_rs.argtypes = [P] * 20
     L.rgf_rgf_g.argtypes = [P] * 20
+    L.rgf_green_rgf_cms.argtypes = [P] * 21
+    L.rgf_green_rgf_cms.restype = ctypes.c_int
     L.rgf_solve_energies.argtypes = [P, ctypes.POINTER(c_device), ctypes.c_int64] + [P] * 13
     L.rgf_terminal_current.argtypes = [P, P, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_int64, P]
@@ -279,16 +282,18 @@ class Context:
     # ------------------------------------------------------------------ batch
     def solve_energies(self, Hii, H1i, E, mu, temp, *, sigma_lesser=None, sigma_r=None,
                        ldos=None, ndens=None, pdens=None, GRi1=None, cur=None, tr=None, tre=None,
-                       T=None, info=None, stream=None, allow_status=True):
+                       T=None, info=None, stream=None, allow_status=True, Sii=None):
         """Solve all energies of one device (rgf_solve_energies).
 
-        Hii, H1i: (nx, nm, nm) complex128.  Per-energy arrays: (nen, nx, nm, nm);
-        tr, tre, T: (nen,) float64.  Outputs are written in place.  Returns the
-        rc (RGF_OK or RGF_E_STATUS)."""
+        Hii, H1i (and the overlap Sii of green_RGF_CMS, or None): (nx, nm, nm)
+        complex128.  Per-energy arrays: (nen, nx, nm, nm); tr, tre, T: (nen,)
+        float64.  Outputs are written in place.  Returns the rc (RGF_OK or
+        RGF_E_STATUS)."""
         nx, nm = int(Hii.shape[0]), int(Hii.shape[1])
         d = c_device()
         d.nm, d.nx = nm, nx
         d.Hii, d.H1i = _ptr(Hii), _ptr(H1i)
+        d.Sii = _ptr(Sii)
         d.mu[0], d.mu[1] = float(mu[0]), float(mu[1])
         d.temp[0], d.temp[1] = float(temp[0]), float(temp[1])
         nen = int(E.shape[0])
@@ -407,8 +412,17 @@ def RGF_G(temperature, nm, nx, E, mu, Hii, H1i, sigma_lesser_ph, sigma_greater_p
                     cur, GRi1, GLi1, GGi1, ctx)
 
 
+def green_RGF_CMS(TEMP, nm, nx, E, mu, Sii, Hii, H1i, sigma_lesser_ph, sigma_greater_ph, sigma_r_ph,
+                  ndens, pdens, ldos, tr, tre, cur, GRi1=None, GLi1=None, GGi1=None, ctx=None):
+    """Drop-in for green_RGF_CMS (src/green_rgf.f90:4167): green_RGF_RS's
+    arguments with the overlap blocks Sii before Hii."""
+    return _drop_in(load().rgf_green_rgf_cms, False, TEMP, nm, nx, E, mu, Hii, H1i,
+                    sigma_lesser_ph, sigma_greater_ph, sigma_r_ph, ndens, pdens, ldos, tr, tre,
+                    cur, GRi1, GLi1, GGi1, ctx, Sii=Sii)
+
+
 def _drop_in(fn, rgf_g_order, TEMP, nm, nx, E, mu, Hii, H1i, sl, sg, sr, ndens, pdens, ldos, tr,
-             tre, cur, GRi1, GLi1, GGi1, ctx):
+             tre, cur, GRi1, GLi1, GGi1, ctx, Sii=None):
     temp = np.ascontiguousarray(TEMP, np.float64)
     muv = np.ascontiguousarray(mu, np.float64)
     nm_ = ctypes.c_int64(int(nm))
@@ -418,8 +432,10 @@ def _drop_in(fn, rgf_g_order, TEMP, nm, nx, E, mu, Hii, H1i, sl, sg, sr, ndens, 
     tres = _scalar_slot(tre)
     P = _ptr
     h = ctx.h if ctx is not None else None
-    base = [h, P(temp), ctypes.addressof(nm_), ctypes.addressof(nx_), ctypes.addressof(E_),
-            P(muv), P(Hii), P(H1i), P(sl), P(sg), P(sr)]
+    base = [h, P(temp), ctypes.addressof(nm_), ctypes.addressof(nx_), ctypes.addressof(E_), P(muv)]
+    if Sii is not None:
+        base.append(P(Sii))
+    base += [P(Hii), P(H1i), P(sl), P(sg), P(sr)]
     if rgf_g_order:
         args = base + [P(trs), P(tres), P(ndens), P(pdens), P(ldos), P(cur), P(GRi1), P(GLi1),
                        P(GGi1)]

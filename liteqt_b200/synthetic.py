@@ -64,6 +64,25 @@ def make_device(nm: int, nx: int, seed: int = 1234, onsite=(-0.5, 0.5), offdiag_
     return Device(nm, nx, _to_fortran_blocks(Hb), _to_fortran_blocks(H1b), seed)
 
 
+def make_overlap(nm: int, nx: int, seed: int = 4321, sigma: float = 0.05) -> np.ndarray:
+    """Overlap blocks S_ll of a non-orthogonal basis (green_RGF_CMS's Sii):
+    I + a Hermitian perturbation with complex N(0, sigma/sqrt(nm))
+    off-diagonal and real N(0, sigma) diagonal entries.  The 1/sqrt(nm)
+    keeps the perturbation's spectral radius near 2*sqrt(2)*sigma whatever
+    the block size, so S stays positive definite (a physical overlap).
+    Fortran block layout (nx, nm, nm) like Hii."""
+    rng = np.random.default_rng(seed)
+    Sb = np.empty((nx, nm, nm), np.complex128)
+    so = sigma / np.sqrt(nm)
+    for l in range(nx):
+        X = rng.normal(0.0, so, (nm, nm)) + 1j * rng.normal(0.0, so, (nm, nm))
+        U = np.triu(X, 1)
+        M = U + U.conj().T
+        M[np.diag_indices(nm)] = 1.0 + rng.normal(0.0, sigma, nm)
+        Sb[l] = M
+    return _to_fortran_blocks(Sb)
+
+
 def uniform_chain(nm: int, nx: int, t: float = -1.0, eps: float = 0.0) -> Device:
     """nm decoupled identical 1D chains: H_ll = eps*I, H_{l,l-1} = t*I.
     Its exact transmission is nm inside the band |E - eps| < 2|t|."""

@@ -265,11 +265,12 @@ def _inv(A):
         return np.zeros_like(A), ST_SINGULAR
 
 
-def sancho_numpy(E, H00, H10, opts: Opts):
-    """sancho (green_rgf.f90:4451-4537) on mathematical blocks; S00 = I."""
+def sancho_numpy(E, H00, H10, opts: Opts, S00=None):
+    """sancho (green_rgf.f90:4451-4537) on mathematical blocks; S00 = I
+    unless given (green_RGF_CMS)."""
     nm = H00.shape[0]
     z = complex(E, opts.eta_lead)
-    I = np.eye(nm)
+    I = np.eye(nm) if S00 is None else S00
     H_BB = H00.copy()
     H_SS = H00.copy()
     H_10 = H10.copy()
@@ -304,16 +305,25 @@ def sancho_numpy(E, H00, H10, opts: Opts):
     return G00, GBB, taken, status | s1 | s2
 
 
-def rgf_numpy(Hb, H1b, E, mu, temp, opts: Opts | None = None, sigl=None, sigr=None):
+def rgf_numpy(Hb, H1b, E, mu, temp, opts: Opts | None = None, sigl=None, sigr=None, Sb=None):
     """One energy of green_RGF_RS on mathematical blocks Hb[l], H1b[l]
-    (l = 0..nx-1; H1b[l] is H1i(:,:,l+1)).  Returns dict of block lists."""
+    (l = 0..nx-1; H1b[l] is H1i(:,:,l+1)).  Returns dict of block lists.
+    Sb (overlap blocks) given: green_RGF_CMS (green_rgf.f90:4167-4383) --
+    z S_ll in place of z I, Sigma^R_ph S and Sigma^<_ph S, Sancho with the end
+    blocks' S, and G^> recursed through the never-filled Glp."""
     opts = opts or Opts()
     nx, nm, _ = Hb.shape
+    cms = Sb is not None
+    Sl = (lambda l: Sb[l]) if cms else (lambda l: np.eye(nm))
     I = np.eye(nm)
     z = complex(E, opts.eta_dev)
     zero = np.zeros((nm, nm), complex)
-    sl = (lambda l: sigl[l]) if sigl is not None else (lambda l: zero)
-    sr = (lambda l: sigr[l]) if sigr is not None else (lambda l: zero)
+    if cms:
+        sl = (lambda l: sigl[l] @ Sb[l]) if sigl is not None else (lambda l: zero)
+        sr = (lambda l: sigr[l] @ Sb[l]) if sigr is not None else (lambda l: zero)
+    else:
+        sl = (lambda l: sigl[l]) if sigl is not None else (lambda l: zero)
+        sr = (lambda l: sigr[l]) if sigr is not None else (lambda l: zero)
     mul, mur = mu
     templ, tempr = temp
     H = lambda X: X.conj().T
@@ -328,12 +338,12 @@ def rgf_numpy(Hb, H1b, E, mu, temp, opts: Opts | None = None, sigl=None, sigr=No
     # left contact
     H00 = Hb[0] + sr(0)
     H10 = H1b[0]
-    G00, _, itL, s = sancho_numpy(E, H00, H(H10), opts)
+    G00, _, itL, s = sancho_numpy(E, H00, H(H10), opts, Sb[0] if cms else None)
     status |= s
     sigmal = H10 @ G00 @ H(H10)
     fl = ferm((E - mul) / (opts.boltz * templ))
     sig = -(sigmal - H(sigmal)) * fl + sl(0)
-    A, s = _inv(z * I - H00 - sigmal)
+    A, s = _inv(z * Sl(0) - H00 - sigmal)
     status |= s
     Gl[0] = A
     Gln[0] = A @ sig @ H(A)
@@ -341,7 +351,7 @@ def rgf_numpy(Hb, H1b, E, mu, temp, opts: Opts | None = None, sigl=None, sigr=No
     for l in range(1, nx - 1):
         H00 = Hb[l] + sr(l)
         H10 = H1b[l]
-        A, s = _inv(z * I - H00 - H10 @ Gl[l - 1] @ H(H10))
+        A, s = _inv(z * Sl(l) - H00 - H10 @ Gl[l - 1] @ H(H10))
         status |= s
         Gl[l] = A
         Gln[l] = A @ (H10 @ Gln[l - 1] @ H(H10) + sl(l)) @ H(A)
@@ -349,10 +359,10 @@ def rgf_numpy(Hb, H1b, E, mu, temp, opts: Opts | None = None, sigl=None, sigr=No
     # right contact
     H00 = Hb[nx - 1] + sr(nx - 1)
     H10 = H1b[nx - 1]
-    G00s, _, itR, s = sancho_numpy(E, H00, H10, opts)
+    G00s, _, itR, s = sancho_numpy(E, H00, H10, opts, Sb[nx - 1] if cms else None)
     status |= s
     sigmar = H(H10) @ G00s @ H10
-    G00, s = _inv(z * I - H00 - sigmar - H10 @ Gl[nx - 2] @ H(H10))
+    G00, s = _inv(z * Sl(nx - 1) - H00 - sigmar - H10 @ Gl[nx - 2] @ H(H10))
     status |= s
     ldos[nx - 1] = G00
     fr = ferm((E - mur) / (opts.boltz * templ))
@@ -384,7 +394,11 @@ def rgf_numpy(Hb, H1b, E, mu, temp, opts: Opts | None = None, sigl=None, sigr=No
         ldos[l] = G00
         Gn = gn + g @ H(H10) @ Gn @ H10 @ H(g) + GN0 @ H10 @ gn + gn @ H(H10) @ H(GN0)
         ndens[l] = Gn
-        pdens[l] = Gn + (G00 - H(G00))
+        if cms:   # Gp = Glp + g H^H Gp H g^H + (terms with Glp = 0)
+            Gp = g @ H(H10) @ Gp @ H10 @ H(g)
+            pdens[l] = Gp
+        else:
+            pdens[l] = Gn + (G00 - H(G00))
     cur[nx - 1] = np.zeros((nm, nm))
     Gp = Gn + (G00 - H(G00))
     fl2 = ferm((E - mul) / (opts.boltz * tempr))
@@ -396,22 +410,28 @@ def rgf_numpy(Hb, H1b, E, mu, temp, opts: Opts | None = None, sigl=None, sigr=No
                 iters=(itL, itR), status=status, sigmal=sigmal, sigmar=sigmar)
 
 
-def dense_green(Hb, H1b, E, sigmal, sigmar, eta_dev=0.0, sigr=None):
-    """Known answer: invert the whole device (E - H - Sigma)^-1 with the
-    consistent coupling H_{l,l-1} = H1b[l].  Returns the full G^R matrix."""
+def dense_green(Hb, H1b, E, sigmal, sigmar, eta_dev=0.0, sigr=None, Sb=None):
+    """Known answer: invert the whole device (E S - H - Sigma)^-1 with the
+    consistent coupling H_{l,l-1} = H1b[l] and block-diagonal overlap Sb
+    (None = I; with Sb the scattering term is sigr[l] Sb[l], as in
+    green_RGF_CMS).  Returns the full G^R matrix."""
     nx, nm, _ = Hb.shape
     N = nx * nm
     M = np.zeros((N, N), complex)
+    Sfull = np.eye(N, dtype=complex)
     for l in range(nx):
         s = slice(l * nm, (l + 1) * nm)
-        M[s, s] = Hb[l] + (sigr[l] if sigr is not None else 0)
+        sr_l = 0 if sigr is None else (sigr[l] if Sb is None else sigr[l] @ Sb[l])
+        M[s, s] = Hb[l] + sr_l
+        if Sb is not None:
+            Sfull[s, s] = Sb[l]
         if l > 0:
             p = slice((l - 1) * nm, l * nm)
             M[s, p] = H1b[l]
             M[p, s] = H1b[l].conj().T
     M[:nm, :nm] += sigmal
     M[-nm:, -nm:] += sigmar
-    return np.linalg.inv(complex(E, eta_dev) * np.eye(N) - M)
+    return np.linalg.inv(complex(E, eta_dev) * Sfull - M)
 
 
 # ---------------------------------------------------------------------------

@@ -28,8 +28,8 @@ int main(int argc, char** argv) {
            offsetof(rgf_opts, sancho_tol), offsetof(rgf_opts, sancho_nmax),
            offsetof(rgf_opts, consistent), offsetof(rgf_opts, precision),
            offsetof(rgf_opts, want_T), offsetof(rgf_opts, verbose), offsetof(rgf_opts, reserved));
-    printf("device %zu %zu %zu %zu\n", sizeof(rgf_device), offsetof(rgf_device, Hii),
-           offsetof(rgf_device, mu), offsetof(rgf_device, temp));
+    printf("device %zu %zu %zu %zu %zu\n", sizeof(rgf_device), offsetof(rgf_device, Hii),
+           offsetof(rgf_device, mu), offsetof(rgf_device, temp), offsetof(rgf_device, Sii));
     printf("task %zu %zu %zu %zu %zu\n", sizeof(rgf_task), offsetof(rgf_task, E),
            offsetof(rgf_task, sigma_lesser), offsetof(rgf_task, cur), offsetof(rgf_task, T));
     printf("info %zu\n", sizeof(rgf_task_info));

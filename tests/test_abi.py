@@ -65,7 +65,7 @@ def test_struct_layouts_match_python_mirror(harness):
                      rgf.c_opts.want_T.offset, rgf.c_opts.verbose.offset, rgf.c_opts.reserved.offset]
     d = vals["device"]
     assert d == [ctypes.sizeof(rgf.c_device), rgf.c_device.Hii.offset, rgf.c_device.mu.offset,
-                 rgf.c_device.temp.offset]
+                 rgf.c_device.temp.offset, rgf.c_device.Sii.offset]
     t = vals["task"]
     assert t == [ctypes.sizeof(rgf.c_task), rgf.c_task.E.offset, rgf.c_task.sigma_lesser.offset,
                  rgf.c_task.cur.offset, rgf.c_task.T.offset]
@@ -96,6 +96,8 @@ def test_context_without_gpu_fails_cleanly(harness):
 
 def test_fortran_interface_file_binds_every_drop_in():
     src = open(os.path.join(ROOT, "fortran", "rgf_iface.f90")).read()
-    for name in ("rgf_green_rgf_rs", "rgf_rgf_g", "rgf_solve_energies", "rgf_ctx_create"):
+    for name in ("rgf_green_rgf_rs", "rgf_rgf_g", "rgf_green_rgf_cms", "rgf_solve_energies",
+                 "rgf_ctx_create"):
         assert f'bind(C, name="{name}")' in src
     assert "subroutine green_RGF_RS" in src and "subroutine RGF_G" in src
+    assert "subroutine green_RGF_CMS" in src

@@ -50,7 +50,7 @@ def rgf():
     return R
 
 
-def gpu_solve(R, Hii, H1i, E, opts, sl=None, sr=None, mu=MU, temp=None, outputs="all"):
+def gpu_solve(R, Hii, H1i, E, opts, sl=None, sr=None, mu=MU, temp=None, outputs="all", Sii=None):
     temp = temp or _temp()
     nx, nm, _ = Hii.shape
     nen = len(E)
@@ -63,7 +63,7 @@ def gpu_solve(R, Hii, H1i, E, opts, sl=None, sr=None, mu=MU, temp=None, outputs=
         rc = ctx.solve_energies(Hii, H1i, np.ascontiguousarray(E, float), mu, temp, sigma_lesser=sl,
                                 sigma_r=sr, ldos=out["ldos"], ndens=out["ndens"], pdens=out["pdens"],
                                 GRi1=out["GRi1"], cur=out["cur"], tr=out["tr"], tre=out["tre"],
-                                T=out["T"], info=out["info"])
+                                T=out["T"], info=out["info"], Sii=Sii)
     out["rc"] = rc
     return out
 
@@ -119,7 +119,9 @@ def test_fp64_matches_golden(rgf, path):
                        consistent=bool(z["consistent"]), boltz=float(z["boltz"]))
     sl = z["sig_lesser"] if z["has_sigma"] else None
     sr = z["sig_r"] if z["has_sigma"] else None
-    g = gpu_solve(rgf, z["Hii"], z["H1i"], z["E"], opts, sl, sr, mu=tuple(z["mu"]), temp=tuple(z["temp"]))
+    Sii = z["Sii"] if "has_overlap" in z.files else None
+    g = gpu_solve(rgf, z["Hii"], z["H1i"], z["E"], opts, sl, sr, mu=tuple(z["mu"]), temp=tuple(z["temp"]),
+                  Sii=Sii)
     keys = ("ldos", "ndens", "pdens", "GRi1", "cur", "tr", "tre", "T")
     r = {k: z[k] for k in keys}
     x = {k: z["exact_" + k] for k in keys}

@@ -211,8 +211,9 @@ def test_oracle_reproduces_golden(oracle_mod, path):
                   consistent=bool(z["consistent"]), boltz=float(z["boltz"]))
     sl = z["sig_lesser"] if z["has_sigma"] else None
     sr = z["sig_r"] if z["has_sigma"] else None
+    Sii = z["Sii"] if "has_overlap" in z.files else None
     r = O.rgf_batch(z["Hii"], z["H1i"], z["E"], z["mu"], z["temp"], opts, sig_lesser=sl, sig_r=sr,
-                    threads=2)
+                    threads=2, Sii=Sii)
     for k in ("ldos", "ndens", "GRi1"):
         assert rel_err(r[k], z[k]) < 1e-12, k
     assert rel_err(r["pdens"], z["pdens"], scale=np.max(np.abs(z["ldos"]))) < 1e-12
@@ -273,3 +274,117 @@ def test_perturbed_inputs_stay_hermitian_and_close():
     assert np.max(np.abs(P - d.Hii) / np.maximum(np.abs(d.Hii), 1e-300)) <= 2.0 ** -51
     assert np.max(np.abs(Q - d.H1i) / np.maximum(np.abs(d.H1i), 1e-300)) <= 2.0 ** -51
     assert not np.array_equal(P, d.Hii)
+
+
+# ---------------------------------------------------------------- green_RGF_CMS
+@pytest.mark.parametrize("consistent", [False, True])
+@pytest.mark.parametrize("nm,nx,scatter", [(8, 5, True), (12, 3, False), (6, 2, True)])
+def test_cms_cpp_matches_numpy_restatement(oracle_mod, consistent, nm, nx, scatter):
+    O = oracle_mod
+    d = S.make_device(nm, nx, seed=nm * 10 + nx)
+    Sii = S.make_overlap(nm, nx, seed=nx)
+    E = np.array([-1.9, -0.3, 0.6, 2.2])
+    sl = sr = None
+    if scatter:
+        sl, sr = random_sigma(nm, nx, len(E), seed=17)
+    opts = O.Opts(consistent=consistent)
+    r = O.rgf_batch(d.Hii, d.H1i, E, MU, _temp(), opts, sig_lesser=sl, sig_r=sr, threads=2, Sii=Sii)
+    Hb, H1b, Sb = O.to_blocks(d.Hii), O.to_blocks(d.H1i), O.to_blocks(Sii)
+    for ie, e in enumerate(E):
+        t = O.rgf_numpy(Hb, H1b, e, MU, _temp(), opts,
+                        sigl=None if sl is None else O.to_blocks(sl[ie]),
+                        sigr=None if sr is None else O.to_blocks(sr[ie]), Sb=Sb)
+        for k in ("ldos", "ndens", "GRi1"):
+            assert rel_err(O.to_blocks(r[k][ie]), t[k]) < 1e-9, k
+        assert rel_err(O.to_blocks(r["pdens"][ie]), t["pdens"],
+                       scale=max(np.max(np.abs(t["ldos"])), np.max(np.abs(t["ndens"])))) < 1e-9
+        cur_scale = nm * np.max(np.abs(H1b)) * np.max(np.abs(t["ndens"]))
+        assert rel_err(O.to_blocks(r["cur"][ie]), t["cur"], scale=cur_scale) < 1e-9
+        assert abs(r["T"][ie] - t["T"]) < 1e-9 * max(1.0, abs(t["T"]))
+        tr_scale = max(np.max(np.abs(r["tr"])), 1e-300)
+        assert abs(r["tr"][ie] - t["tr"]) < 1e-8 * tr_scale + 1e-14 * nm
+        assert abs(r["tre"][ie] - t["tre"]) < 1e-8 * tr_scale + 1e-14 * nm
+        assert tuple(r["stats"][ie][["sancho_iters_left", "sancho_iters_right"]]) == t["iters"]
+
+
+def test_cms_with_unit_overlap_is_rs_except_the_greater_recursion(oracle_mod):
+    """With S = I, green_RGF_CMS computes what green_RGF_RS computes (bit for
+    bit: the overlap products are exact), except G^>_ll for l < nx, which it
+    recurses through the never-filled Glp instead of using the identity
+    G^> = G^< + G^R - G^A, and GGi1, which uses that running G^>."""
+    O = oracle_mod
+    nm, nx = 8, 5
+    d = S.make_device(nm, nx, seed=5)
+    Sii = S._to_fortran_blocks(np.broadcast_to(np.eye(nm, dtype=complex), (nx, nm, nm)).copy())
+    E = np.array([-0.8, 0.35])
+    sl, sr = random_sigma(nm, nx, len(E), seed=2)
+    outs = ("ldos", "ndens", "pdens", "cur", "GRi1", "GLi1", "GGi1")
+    rs = O.rgf_batch(d.Hii, d.H1i, E, MU, _temp(), O.Opts(), sig_lesser=sl, sig_r=sr, outputs=outs)
+    cms = O.rgf_batch(d.Hii, d.H1i, E, MU, _temp(), O.Opts(), sig_lesser=sl, sig_r=sr, outputs=outs,
+                      Sii=Sii)
+    for k in ("ldos", "ndens", "cur", "GRi1", "GLi1", "tr", "tre", "T"):
+        assert np.array_equal(rs[k], cms[k]), k
+    assert np.array_equal(rs["pdens"][:, -1], cms["pdens"][:, -1])
+    assert not np.allclose(rs["pdens"][:, :-1], cms["pdens"][:, :-1])
+    assert np.array_equal(rs["GGi1"][:, -2], cms["GGi1"][:, -2])  # both use the closure's G^> there
+
+
+@pytest.mark.parametrize("nm,nx", [(4, 2), (6, 4)])
+def test_cms_dense_inverse_known_answer(oracle_mod, nm, nx):
+    """Consistent-mode CMS equals (E S - H - Sigma)^-1 of the whole device."""
+    O = oracle_mod
+    d = S.make_device(nm, nx, seed=21 + nm)
+    Sii = S.make_overlap(nm, nx, seed=3)
+    Hb, H1b, Sb = O.to_blocks(d.Hii), O.to_blocks(d.H1i), O.to_blocks(Sii)
+    E = np.array([-1.1, 0.7])
+    sl, sr = random_sigma(nm, nx, len(E), seed=4)
+    opts = O.Opts(consistent=True, eta_dev=1e-4)
+    r = O.rgf_batch(d.Hii, d.H1i, E, MU, _temp(), opts, sig_lesser=sl, sig_r=sr, threads=1, Sii=Sii)
+    for ie, e in enumerate(E):
+        t = O.rgf_numpy(Hb, H1b, e, MU, _temp(), opts, sigl=O.to_blocks(sl[ie]),
+                        sigr=O.to_blocks(sr[ie]), Sb=Sb)
+        G = O.dense_green(Hb, H1b, e, t["sigmal"], t["sigmar"], eta_dev=opts.eta_dev,
+                          sigr=O.to_blocks(sr[ie]), Sb=Sb)
+        ldos, gri1 = O.to_blocks(r["ldos"][ie]), O.to_blocks(r["GRi1"][ie])
+        for l in range(nx):
+            s = slice(l * nm, (l + 1) * nm)
+            assert rel_err(ldos[l], G[s, s], scale=np.max(np.abs(G))) < 1e-10
+            if l < nx - 1:
+                s1 = slice((l + 1) * nm, (l + 2) * nm)
+                assert rel_err(gri1[l], G[s, s1], scale=np.max(np.abs(G))) < 1e-10
+        N = nm * nx
+        Sl = np.zeros((N, N), complex)
+        fl = O.ferm((e - MU[0]) / (opts.boltz * _temp()[0]))
+        fr = O.ferm((e - MU[1]) / (opts.boltz * _temp()[0]))
+        Sl[:nm, :nm] = -(t["sigmal"] - t["sigmal"].conj().T) * fl
+        Sl[-nm:, -nm:] = -(t["sigmar"] - t["sigmar"].conj().T) * fr
+        slb = O.to_blocks(sl[ie])
+        for l in range(nx):
+            Sl[l * nm:(l + 1) * nm, l * nm:(l + 1) * nm] += slb[l] @ Sb[l]
+        Gless = G @ Sl @ G.conj().T
+        nd = O.to_blocks(r["ndens"][ie])
+        for l in range(nx):
+            s = slice(l * nm, (l + 1) * nm)
+            assert rel_err(nd[l], Gless[s, s], scale=np.max(np.abs(Gless))) < 1e-10
+        gL = 1j * (t["sigmal"] - t["sigmal"].conj().T)
+        gR = 1j * (t["sigmar"] - t["sigmar"].conj().T)
+        GN1 = G[-nm:, :nm]
+        T = np.real(np.trace(gL @ GN1.conj().T @ gR @ GN1))
+        assert abs(r["T"][ie] - T) < 1e-10 * max(1.0, abs(T))
+
+
+def test_cms_sancho_fixed_point_with_overlap(oracle_mod):
+    O = oracle_mod
+    rng = np.random.default_rng(8)
+    nm = 6
+    X = rng.normal(size=(nm, nm)) + 1j * rng.normal(size=(nm, nm))
+    H00 = 0.1 * (X + X.conj().T)
+    H10 = -1.0 * (np.eye(nm) + 0.1 * rng.normal(size=(nm, nm)))
+    S00 = O.to_blocks(S.make_overlap(nm, 1, seed=9))[0]
+    opts = O.Opts()
+    for E in (-0.7, 0.3, 1.1):
+        G, _, it, st = O.sancho_numpy(E, H00, H10, opts, S00)
+        assert st == 0 and it < opts.sancho_nmax
+        z = complex(E, opts.eta_lead)
+        R = G - np.linalg.inv(z * S00 - H00 - H10.conj().T @ G @ H10)
+        assert np.linalg.norm(R) < 1e-8 * np.linalg.norm(G)
