@@ -58,6 +58,9 @@ def parse():
     p.add_argument("--adjoint", action="store_true",
                    help="time the adjoint (dT/dV_l, dT/ds, dI/dV_l) against forward solves on the "
                         "adjoint workload (nb=64, Nx=200, per-block potential U[-0.2,0.2] eV)")
+    p.add_argument("--w", action="store_true",
+                   help="time the screened-interaction solve (green_rgf_calc_w) on the GW workload "
+                        "(nb=64, Nx=40, Coulomb V, 2048 polarization sets per step)")
     p.add_argument("--single", action="store_true",
                    help="one device-resident solve and exit (for profiler captures; prints no JSON)")
     return p.parse_args()
@@ -474,9 +477,78 @@ def run_adjoint(args):
     print(json.dumps(line), flush=True)
 
 
+def run_w(args):
+    """GW screened-interaction workload: nb = 64, Nx = 40, bare Coulomb V
+    (1/(r + 0.3 nm) on a seeded orbital grid, seed 99), seeded physical
+    polarizations (P^R complex symmetric, P^< / P^> anti-Hermitian); one step
+    = rgf_w_solve_energies over --nen polarization sets (default 2048: the
+    energies of one q-point), W^<, W^>, W^R out, device-resident.  Roofline
+    numerator: the reference routine's own products for NBC = 0 (46 Nx - 20
+    nb^3 products + Nx inversions per solve, including its LL / LG blocks and
+    XR recursion, which the GPU skips because nothing returned uses them)."""
+    import torch
+    from liteqt_b200 import rgf
+    from liteqt_b200 import synthetic as S
+    nb, nx, nen = 64, 40, (args.nen if args.nen != 296 else 2048)
+    Vii, V1i = S.make_coulomb(nb, nx, seed=99)
+    # a pool of 64 distinct polarization sets, tiled to nen (the solve cost does
+    # not depend on the values)
+    pool = S.make_polarization(nb, nx, 64, seed=7)
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    reps = (nen + 63) // 64
+    P = [torch.from_numpy(np.concatenate([x] * reps)[:nen]).to(dev) for x in pool]
+    Vd, V1d = torch.from_numpy(Vii).to(dev), torch.from_numpy(V1i).to(dev)
+    W = [torch.empty_like(P[0]) for _ in range(3)]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    ctx = rgf.Context(rgf.Options())
+    peak = zgemm_peak_tflops(torch, dev)
+
+    def step():
+        ctx.w_solve_energies(Vd, V1d, P[0], P[1], P[2], WL=W[0], WG=W[1], WR=W[2], stream=stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize(dev)
+        clocks = ClockSampler(0)
+        clocks.start()
+        ms, kms = [], []
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            s0 = torch.cuda.Event(enable_timing=True)
+            e0 = torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            step()
+            e0.record(stream)
+            e0.synchronize()
+            ms.append(s0.elapsed_time(e0))
+            kms.append(ctx.stats()["last_kernel_ms"])
+        clk = clocks.stop()
+    st = ctx.stats()
+    ctx.close()
+    alg = nen * 8.0 * nb ** 3 * ((46 * nx - 20) + nx)
+    kern_s = float(np.mean(kms)) * 1e-3
+    line = {"metric": "RGF_W solves/s (W^R, W^<, W^> diagonal blocks)", "value": nen / (np.mean(ms) * 1e-3),
+            "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": float(np.mean(ms)), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"rgf_w_nb{nb}_nx{nx}", "nb": nb, "nx": nx, "solves_per_step": nen,
+                       "V": "Coulomb 1.44/(r+0.3 nm) eV, seed 99", "P": "seeded physical polarizations",
+                       "l2": "flushed between timed steps (256 MiB write)"},
+            "roofline": {"bound": "tensor", "achieved": alg / kern_s / 1e12, "peak": peak, "unit": "TFLOP/s",
+                         "frac": alg / kern_s / 1e12 / peak, "traffic": None,
+                         "executed_tflops": st["last_flops"] / kern_s / 1e12,
+                         "peak_source": "cuBLAS ZGEMM 4096^3 measured live on this GPU"},
+            "gpu_launches_total": int(st["launches"]), "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
-    if args.adjoint:
+    if args.w:
+        run_w(args)
+    elif args.adjoint:
         run_adjoint(args)
     elif args.single:
         run_single(args)

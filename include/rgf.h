@@ -260,6 +260,55 @@ RGF_API int rgf_adjoint_energies(rgf_ctx* ctx, const rgf_device* device, int64_t
                                  double spindeg, double* dIdV, double* dIds,
                                  rgf_task_info* info, void* stream);
 
+/* Screened interaction W (green_rgf_calc_w, src/green_rgf.f90:3399-3831 ==
+ * RGF_W, src/rgf_mod.f90:242-674) for the GW loop: W^R = (I - V P^R)^-1 V and
+ * W^<, W^> from W^R and P^<, P^> by the routine's own formula, per
+ * (q, energy) task, all tasks in one persistent launch.  This is the form
+ * every call site uses (green_rgf.f90:846, :1551, :3008): NBC = 0 and no
+ * off-diagonal P blocks.  V is the device's bare interaction: Vii diagonal
+ * blocks, V1i(:,:,l) = V_{l+1,l} (and V_{l,l+1} = V1i(:,:,l)^H); its W^R
+ * off-diagonal block formula assumes V real symmetric and P^R complex
+ * symmetric, as the physical inputs are. */
+typedef struct rgf_w_device {
+  int64_t nm, nx;
+  const rgf_c16* Vii;
+  const rgf_c16* V1i;
+} rgf_w_device;
+
+typedef struct rgf_w_task {
+  int32_t device;          /* index into the rgf_w_device array */
+  int32_t reserved;
+  const rgf_c16* PL;       /* P^< diagonal blocks (nm,nm,nx) */
+  const rgf_c16* PG;       /* P^> */
+  const rgf_c16* PR;       /* P^R */
+  rgf_c16* WL;             /* W^< diagonal blocks (nm,nm,nx) */
+  rgf_c16* WG;             /* W^> */
+  rgf_c16* WR;             /* W^R */
+  rgf_c16* WRi1;           /* W^R_{l,l+1} (blocks 1..nx-1; block nx untouched), or NULL */
+} rgf_w_task;
+
+RGF_API int rgf_w_solve_batch(rgf_ctx* ctx, const rgf_w_device* devices, int32_t n_devices,
+                              const rgf_w_task* tasks, int64_t n_tasks, rgf_task_info* info,
+                              void* stream);
+
+/* All energies of one q-point in the drivers' layout p(nm,nm,nx,nen)
+ * (green_rgf.f90:836-850): PL/PG/PR and WL/WG/WR strided by nm*nm*nx;
+ * WRi1 may be NULL. */
+RGF_API int rgf_w_solve_energies(rgf_ctx* ctx, const rgf_w_device* device, int64_t nen,
+                                 const rgf_c16* PL, const rgf_c16* PG, const rgf_c16* PR,
+                                 rgf_c16* WL, rgf_c16* WG, rgf_c16* WR, rgf_c16* WRi1,
+                                 rgf_task_info* info, void* stream);
+
+/* Drop-in for green_rgf_calc_w / RGF_W with the reference's argument list
+ * (scalars by reference).  NBC other than 0 or present PL1i / PG1i / PR1i
+ * (never used by the reference's drivers) return RGF_E_UNSUPPORTED; WLi1 /
+ * WGi1 are not written, as in the reference. */
+RGF_API int rgf_green_rgf_calc_w(rgf_ctx* ctx, const int64_t* NBC, const int64_t* nm, const int64_t* nx,
+                                 const rgf_c16* Vii, const rgf_c16* V1i, const rgf_c16* PL,
+                                 const rgf_c16* PG, const rgf_c16* PR, rgf_c16* WL, rgf_c16* WG,
+                                 rgf_c16* WR, const rgf_c16* PL1i, const rgf_c16* PG1i,
+                                 const rgf_c16* PR1i, rgf_c16* WLi1, rgf_c16* WGi1, rgf_c16* WRi1);
+
 /* Terminal current of one energy sweep: sum(tr)*dE*e0/tpi/hbar*e0*spindeg/nk
  * (green_rgf.f90:2938), summed on the device in a fixed order. */
 RGF_API int rgf_terminal_current(rgf_ctx* ctx, const double* tr, int64_t nen, double dE, double spindeg,

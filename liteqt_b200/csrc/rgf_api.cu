@@ -987,3 +987,195 @@ extern "C" int rgf_autotune(rgf_ctx* c, const rgf_device* v, rgf_tune_result* re
   }
   return RGF_OK;
 }
+
+// ------------------------------------------------------------- W solves
+extern "C" int rgf_w_solve_batch(rgf_ctx* c, const rgf_w_device* devices, int32_t n_devices,
+                                 const rgf_w_task* tasks, int64_t n_tasks, rgf_task_info* info,
+                                 void* stream_) {
+  if (!c) return fail(RGF_E_ARG, "ctx is NULL");
+  if (n_tasks < 0 || (n_tasks > 0 && (!tasks || !devices || n_devices < 1)))
+    return fail(RGF_E_ARG, "invalid task list");
+  if (n_tasks == 0) return RGF_OK;
+  if (n_tasks > (int64_t)INT32_MAX) return fail(RGF_E_ARG, "too many tasks in one batch");
+  for (int32_t d = 0; d < n_devices; d++) {
+    const rgf_w_device& v = devices[d];
+    if (v.nm < 8 || v.nm > kMaxNb || v.nm % 8 != 0)
+      return fail(RGF_E_UNSUPPORTED, "device %d: nm=%lld unsupported (multiple of 8 in [8,%d])", d,
+                  (long long)v.nm, kMaxNb);
+    if (v.nx < 2) return fail(RGF_E_ARG, "device %d: nx=%lld < 2", d, (long long)v.nx);
+    if (!v.Vii || !v.V1i) return fail(RGF_E_ARG, "device %d: Vii/V1i is NULL", d);
+  }
+  for (int64_t t = 0; t < n_tasks; t++) {
+    const rgf_w_task& k = tasks[t];
+    if (k.device < 0 || k.device >= n_devices)
+      return fail(RGF_E_ARG, "task %lld: device index %d out of range", (long long)t, k.device);
+    if (!k.PL || !k.PG || !k.PR || !k.WL || !k.WG || !k.WR)
+      return fail(RGF_E_ARG, "task %lld: PL/PG/PR and WL/WG/WR are required", (long long)t);
+  }
+  RGF_CUDA(cudaSetDevice(c->device));
+  cudaStream_t st = stream_ ? (cudaStream_t)stream_ : c->stream;
+  Stage sg;
+  for (int32_t d = 0; d < n_devices; d++) {
+    const size_t bytes = (size_t)devices[d].nm * devices[d].nm * devices[d].nx * sizeof(rgf_c16);
+    sg.add(devices[d].Vii, bytes, true, false);
+    sg.add(devices[d].V1i, bytes, true, false);
+  }
+  for (int64_t t = 0; t < n_tasks; t++) {
+    const rgf_w_task& k = tasks[t];
+    const rgf_w_device& v = devices[k.device];
+    const size_t cb = (size_t)v.nm * v.nm * v.nx * sizeof(rgf_c16);
+    sg.add(k.PL, cb, true, false);
+    sg.add(k.PG, cb, true, false);
+    sg.add(k.PR, cb, true, false);
+    sg.add(k.WL, cb, false, true);
+    sg.add(k.WG, cb, false, true);
+    sg.add(k.WR, cb, false, true);
+    sg.add(k.WRi1, cb, true, true);  // block nx is left untouched
+  }
+  sg.layout();
+  int rc = c->stage.reserve(std::max<size_t>(sg.total, 256));
+  if (rc) return rc;
+  char* sbase = (char*)c->stage.p;
+  for (const auto& s : sg.segs)
+    if (s.copy_in) RGF_CUDA(cudaMemcpyAsync(sbase + s.off, s.host, s.bytes, cudaMemcpyHostToDevice, st));
+  std::vector<DDev> ddev(n_devices);
+  for (int32_t d = 0; d < n_devices; d++) {
+    std::memset(&ddev[d], 0, sizeof(DDev));
+    ddev[d].nm = devices[d].nm;
+    ddev[d].nx = devices[d].nx;
+    ddev[d].Hii = (const double2*)sg.resolve(devices[d].Vii, sbase);
+    ddev[d].H1i = (const double2*)sg.resolve(devices[d].V1i, sbase);
+  }
+  std::vector<DWTask> dt(n_tasks);
+  std::vector<int32_t> order(n_tasks);
+  std::vector<double> cost(n_tasks);
+  int64_t slot = 0;
+  size_t smem = 0;
+  uint64_t nb_mask = 0;
+  for (int64_t t = 0; t < n_tasks; t++) {
+    const rgf_w_task& k = tasks[t];
+    const rgf_w_device& v = devices[k.device];
+    DWTask& o = dt[t];
+    o.dev = k.device;
+    o.pad = 0;
+    o.PL = (const double2*)sg.resolve(k.PL, sbase);
+    o.PG = (const double2*)sg.resolve(k.PG, sbase);
+    o.PR = (const double2*)sg.resolve(k.PR, sbase);
+    o.WL = (double2*)sg.resolve(k.WL, sbase);
+    o.WG = (double2*)sg.resolve(k.WG, sbase);
+    o.WR = (double2*)sg.resolve(k.WR, sbase);
+    o.WRi1 = (double2*)sg.resolve(k.WRi1, sbase);
+    order[t] = (int32_t)t;
+    cost[t] = (double)v.nm * v.nm * v.nm * (double)v.nx;
+    slot = std::max<int64_t>(slot, slot_elems_for(v.nm, v.nx));
+    smem = std::max(smem, variant_smem(c->variant[v.nm / 8], (int)v.nm));
+    nb_mask |= 1ull << (v.nm / 8);
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return cost[a] > cost[b]; });
+  int grid = c->sm_count * launch_ctas_per_sm(c, smem, nb_mask);
+  if ((int64_t)grid > n_tasks) grid = (int)n_tasks;
+  if ((rc = c->work.reserve(sizeof(double2) * (size_t)slot * grid))) return rc;
+  if ((rc = c->devs.reserve(sizeof(DDev) * n_devices))) return rc;
+  if ((rc = c->tasks.reserve(sizeof(DWTask) * n_tasks + sizeof(int32_t) * n_tasks))) return rc;
+  if ((rc = c->info.reserve(sizeof(DInfo) * n_tasks))) return rc;
+  if ((rc = c->queue.reserve(sizeof(int32_t) * 64))) return rc;
+  int32_t* order_d = (int32_t*)((char*)c->tasks.p + sizeof(DWTask) * n_tasks);
+  RGF_CUDA(cudaMemcpyAsync(c->devs.p, ddev.data(), sizeof(DDev) * n_devices, cudaMemcpyHostToDevice, st));
+  RGF_CUDA(cudaMemcpyAsync(c->tasks.p, dt.data(), sizeof(DWTask) * n_tasks, cudaMemcpyHostToDevice, st));
+  RGF_CUDA(cudaMemcpyAsync(order_d, order.data(), sizeof(int32_t) * n_tasks, cudaMemcpyHostToDevice, st));
+  RGF_CUDA(cudaMemsetAsync(c->info.p, 0, sizeof(DInfo) * n_tasks, st));
+  RGF_CUDA(cudaMemsetAsync(c->queue.p, 0, sizeof(int32_t), st));
+  KParams p;
+  fill_params(c, p);
+  p.devs = (const DDev*)c->devs.p;
+  p.n_tasks = n_tasks;
+  p.order = order_d;
+  p.queue = (int32_t*)c->queue.p;
+  p.work = (double2*)c->work.p;
+  p.slot_elems = slot;
+  p.info = (DInfo*)c->info.p;
+  p.wtasks = (const DWTask*)c->tasks.p;
+  RGF_CUDA(cudaEventRecord(c->ev0, st));
+  cudaError_t e = launch_solver(p, grid, smem, st);
+  if (e != cudaSuccess) return fail(RGF_E_CUDA, "W launch failed: %s", cudaGetErrorString(e));
+  c->stats.launches++;
+  RGF_CUDA(cudaEventRecord(c->ev1, st));
+  for (const auto& s : sg.segs)
+    if (s.copy_out)
+      RGF_CUDA(cudaMemcpyAsync(const_cast<char*>(s.host), sbase + s.off, s.bytes, cudaMemcpyDeviceToHost, st));
+  std::vector<DInfo> hinfo(n_tasks);
+  RGF_CUDA(cudaMemcpyAsync(hinfo.data(), c->info.p, sizeof(DInfo) * n_tasks, cudaMemcpyDeviceToHost, st));
+  RGF_CUDA(cudaStreamSynchronize(st));
+  int worst = 0;
+  double flops = 0.0;
+  for (int64_t t = 0; t < n_tasks; t++) {
+    worst |= hinfo[t].status;
+    const double nb = (double)devices[tasks[t].device].nm;
+    flops += 8.0 * nb * nb * nb * (double)(hinfo[t].n_gemm + hinfo[t].n_inv);
+  }
+  float kms = 0.0f;
+  RGF_CUDA(cudaEventElapsedTime(&kms, c->ev0, c->ev1));
+  c->stats.last_kernel_ms = kms;
+  c->stats.last_flops = flops;
+  c->stats.last_tasks = n_tasks;
+  if (info) std::memcpy(info, hinfo.data(), sizeof(DInfo) * n_tasks);
+  if (worst & RGF_ST_BAD_TASK) return fail(RGF_E_ARG, "a task was rejected on the device");
+  return worst ? RGF_E_STATUS : RGF_OK;
+}
+
+extern "C" int rgf_w_solve_energies(rgf_ctx* ctx, const rgf_w_device* device, int64_t nen,
+                                    const rgf_c16* PL, const rgf_c16* PG, const rgf_c16* PR,
+                                    rgf_c16* WL, rgf_c16* WG, rgf_c16* WR, rgf_c16* WRi1,
+                                    rgf_task_info* info, void* stream) {
+  if (!ctx || !device || nen < 0 || !PL || !PG || !PR || !WL || !WG || !WR)
+    return fail(RGF_E_ARG, "invalid argument");
+  const size_t per = (size_t)device->nm * device->nm * device->nx;
+  std::vector<rgf_w_task> tasks(nen);
+  for (int64_t e = 0; e < nen; e++) {
+    rgf_w_task& t = tasks[e];
+    std::memset(&t, 0, sizeof(t));
+    t.PL = PL + e * per;
+    t.PG = PG + e * per;
+    t.PR = PR + e * per;
+    t.WL = WL + e * per;
+    t.WG = WG + e * per;
+    t.WR = WR + e * per;
+    t.WRi1 = WRi1 ? WRi1 + e * per : nullptr;
+  }
+  return rgf_w_solve_batch(ctx, device, 1, tasks.data(), nen, info, stream);
+}
+
+extern "C" int rgf_green_rgf_calc_w(rgf_ctx* ctx, const int64_t* NBC, const int64_t* nm, const int64_t* nx,
+                                    const rgf_c16* Vii, const rgf_c16* V1i, const rgf_c16* PL,
+                                    const rgf_c16* PG, const rgf_c16* PR, rgf_c16* WL, rgf_c16* WG,
+                                    rgf_c16* WR, const rgf_c16* PL1i, const rgf_c16* PG1i,
+                                    const rgf_c16* PR1i, rgf_c16* WLi1, rgf_c16* WGi1, rgf_c16* WRi1) {
+  (void)WLi1;  // not written by the reference either
+  (void)WGi1;
+  if (!NBC || !nm || !nx) return fail(RGF_E_ARG, "NULL scalar argument");
+  if (*NBC != 0)
+    return fail(RGF_E_UNSUPPORTED, "NBC=%lld: only the NBC = 0 form (every call site) is built", (long long)*NBC);
+  if (PL1i || PG1i || PR1i)
+    return fail(RGF_E_UNSUPPORTED, "off-diagonal polarization blocks are not supported (no call site passes them)");
+  int rc = RGF_OK;
+  if (!ctx) {
+    ctx = default_ctx(8.61734e-05, &rc);
+    if (!ctx) return rc;
+  }
+  rgf_w_device d;
+  d.nm = *nm;
+  d.nx = *nx;
+  d.Vii = Vii;
+  d.V1i = V1i;
+  rgf_w_task t;
+  std::memset(&t, 0, sizeof(t));
+  t.PL = PL;
+  t.PG = PG;
+  t.PR = PR;
+  t.WL = WL;
+  t.WG = WG;
+  t.WR = WR;
+  t.WRi1 = WRi1;
+  rc = rgf_w_solve_batch(ctx, &d, 1, &t, 1, nullptr, nullptr);
+  return rc == RGF_E_STATUS ? RGF_OK : rc;
+}

@@ -30,7 +30,7 @@ __global__ void __launch_bounds__(kThreads, 2) rgf_solver_kernel(KParams p) {
     __syncthreads();
     if (q >= p.n_tasks) break;
     const int64_t t = p.order ? p.order[q] : q;
-    const int dev = p.adj ? p.adj[t].dev : p.tasks[t].dev;
+    const int dev = p.adj ? p.adj[t].dev : (p.wtasks ? p.wtasks[t].dev : p.tasks[t].dev);
     const int64_t n = p.devs[dev].nm, nx = p.devs[dev].nx;
     int v = KV_NONE;
     if (n >= 8 && n <= kMaxNb && n % 8 == 0) v = p.variant[n / 8];

@@ -84,6 +84,20 @@ enum KVariant : int {
 };
 constexpr int kVariantSlots = kMaxNb / 8 + 1;  // indexed by nb / 8
 
+// One screened-interaction task (green_rgf_calc_w): the device's Vii / V1i
+// sit in DDev's Hii / H1i; polarization inputs and W outputs here.
+struct DWTask {
+  int32_t dev;
+  int32_t pad;
+  const double2* PL;
+  const double2* PG;
+  const double2* PR;
+  double2* WL;
+  double2* WG;
+  double2* WR;
+  double2* WRi1;   // blocks 0..nx-2, or NULL
+};
+
 struct KParams {
   KOpts o;
   const DDev* devs;
@@ -95,6 +109,7 @@ struct KParams {
   int64_t slot_elems;      // complex elements per slot (>= slot_elems_for(nb, nx) of every task)
   DInfo* info;             // per task
   const DAdj* adj;         // non-null: run the adjoint instead of the drop-in solve
+  const DWTask* wtasks;    // non-null: run W solves (green_rgf_calc_w)
   int8_t variant[kVariantSlots];  // kernel variant per block size (nb / 8), KV_NONE = unsupported
 };
 

@@ -548,6 +548,138 @@ struct Solver {
   // enters through dSigma/dE.  s scales the interior couplings H1i(:,:,m),
   // m = 2..nx-1 (1-based).  Reverse sweep with sqrt(nx) checkpoints of the
   // left-connected g_l and of the running column c_l = g^L_{l,1}.
+  // green_rgf_calc_w (green_rgf.f90:3399-3831) == RGF_W (rgf_mod.f90:242-674)
+  // with NBC = 0 and no off-diagonal P blocks (every call site).  V = the
+  // device's (Vii, V1i); M = I - V P^R is formed block by block as needed:
+  //   right-to-left  xlr_l = (M_ll - M_{l,l+1} xlr_{l+1} M_{l+1,l})^-1,
+  //                  Wlr_l = xlr_l (V_ll - M_{l,l+1} xlr_{l+1} V_{l+1,l})   (:3710-3722)
+  //   left-to-right  WR_l = Wlr_l - xlr_l M_{l,l-1} Wo_{l-1},
+  //                  Wo_l = (V1i_l^T - WR_l M1i_l^T) xlr_{l+1}^T              (:3740-3778)
+  //   W^< / W^>      WR P WR^H + Wi_j P Wi_j^T (-1) + Wi_m^T P Wi_m (-1)      (:3786-3829)
+  // with Wi = i Im(Wo) (the routine zeroes the real part), j = l (l = nx-1:
+  // nx-2), m = max(l-1, 0).  Plain transposes are materialised in epilogues
+  // or one pass (the tensor-core GEMM takes N and C operands).  The
+  // routine's LL / LG, wln / wlp and XR are never returned and are not
+  // formed.  xlr lives in Gl(l), Wlr in Gln(l).
+  __device__ void run_w(const DWTask& tk, const DDev& dv, DInfo* info) {
+    const int nn = n;
+    const double2* Vii = dv.Hii;
+    const double2* V1i = dv.H1i;
+    auto blk = [&](const double2* base, int l) { return base + (size_t)l * n2; };
+    auto wblk = [&](double2* base, int l) { return base + (size_t)l * n2; };
+    const double2* PR = tk.PR;
+    // ---- right-to-left: xlr, Wlr
+    {
+      const int l = nx - 1;
+      gemm(blk(Vii, l), false, blk(PR, l), false, [&](int i, int j, double2 v) {   // M_ll = I - V P^R
+        X[i + j * nn] = (i == j) ? make_double2(1.0 - v.x, -v.y) : make_double2(-v.x, -v.y);
+      });
+      invert_X(Gl(l));
+      gemm_store(Gl(l), false, blk(Vii, l), false, Gln(l));
+    }
+    for (int l = nx - 2; l >= 0; l--) {
+      gemm(blk(V1i, l), true, blk(PR, l + 1), false, [&](int i, int j, double2 v) {
+        tmp(T_F1)[i + j * nn] = make_double2(-v.x, -v.y);                         // M_{l,l+1}
+      });
+      gemm_store(tmp(T_F1), false, Gl(l + 1), false, tmp(T_F2));                  // B = M_{l,l+1} xlr_{l+1}
+      gemm_store(tmp(T_F2), false, blk(V1i, l), false, tmp(T_F3));                // B V_{l+1,l}
+      // X is only written by the epilogue of the last product before the
+      // inverse: for nb <= 64 it shares shared memory with the GEMM staging
+      gemm(blk(Vii, l), false, blk(PR, l), false, [&](int i, int j, double2 v) {   // M_ll
+        tmp(T_SA)[i + j * nn] = (i == j) ? make_double2(1.0 - v.x, -v.y) : make_double2(-v.x, -v.y);
+      });
+      gemm(tmp(T_F3), false, blk(PR, l), false, [&](int i, int j, double2 v) {     // - B M_{l+1,l} = + B V P
+        const int idx = i + j * nn;
+        X[idx] = cadd(tmp(T_SA)[idx], v);
+      });
+      invert_X(Gl(l));
+      for_each_elem(n, [&](int, int, int idx) { tmp(T_F4)[idx] = csub(blk(Vii, l)[idx], tmp(T_F3)[idx]); });
+      __syncthreads();
+      gemm_store(Gl(l), false, tmp(T_F4), false, Gln(l));                         // Wlr_l
+    }
+    // ---- left-to-right: WR, Wo; W^< and W^> block by block
+    double2* WRc = tmp(T_G00A);
+    double2 *M1c = tmp(T_H10A), *M1p = tmp(T_H10B), *M1T = tmp(T_H01A);
+    double2 *Woc = tmp(T_GNA), *Wop = tmp(T_GNB);
+    double2 *Wic = tmp(T_Q1), *NWTc = tmp(T_Q2), *Wip = tmp(T_Q3), *NWTp = tmp(T_Q4);
+    double2* xT = tmp(T_R5);
+    for (int l = 0; l < nx; l++) {
+      double2* wr_out = wblk(tk.WR, l);
+      if (l == 0) {
+        for_each_elem(n, [&](int, int, int idx) {
+          const double2 w = Gln(0)[idx];
+          WRc[idx] = w;
+          wr_out[idx] = w;
+        });
+        __syncthreads();
+      } else {
+        gemm_store(Gl(l), false, M1p, false, tmp(T_F1));                          // xlr_l M_{l,l-1}
+        gemm(tmp(T_F1), false, Wop, false, [&](int i, int j, double2 v) {
+          const int idx = i + j * nn;
+          const double2 w = csub(Gln(l)[idx], v);
+          WRc[idx] = w;
+          wr_out[idx] = w;
+        });
+      }
+      if (l < nx - 1) {
+        gemm(blk(V1i, l), false, blk(PR, l), false, [&](int i, int j, double2 v) {  // M_{l+1,l} and its transpose
+          const double2 m = make_double2(-v.x, -v.y);
+          M1c[i + j * nn] = m;
+          M1T[j + i * nn] = m;
+        });
+        for_each_elem(n, [&](int i, int j, int idx) { xT[j + i * nn] = Gl(l + 1)[idx]; });
+        __syncthreads();
+        gemm(WRc, false, M1T, false, [&](int i, int j, double2 v) {               // C = V1i^T - WR M1i^T
+          const int idx = i + j * nn;
+          tmp(T_F2)[idx] = csub(blk(V1i, l)[j + i * nn], v);
+        });
+        double2* wo_out = tk.WRi1 ? wblk(tk.WRi1, l) : nullptr;
+        gemm(tmp(T_F2), false, xT, false, [&](int i, int j, double2 v) {          // Wo_l = C xlr_{l+1}^T
+          const int idx = i + j * nn;
+          Woc[idx] = v;
+          if (wo_out) wo_out[idx] = v;
+          const double2 wi = make_double2(0.0 * v.x, v.y);                        // real part zeroed
+          Wic[idx] = wi;
+          NWTc[j + i * nn] = make_double2(-wi.x, -wi.y);                          // -(Wi)^T
+        });
+      }
+      // W^< / W^> of block l (the off-diagonal terms use Wi_j, Wi_m)
+      const double2 *Wj, *NWTj, *Wm, *NWTm;
+      const int jp = l < nx - 1 ? l + 1 : l;
+      if (l < nx - 1) { Wj = Wic; NWTj = NWTc; } else { Wj = Wip; NWTj = NWTp; }
+      if (l == 0) { Wm = Wic; NWTm = NWTc; } else { Wm = Wip; NWTm = NWTp; }
+      for (int which = 0; which < 2; which++) {
+        const double2* P = which == 0 ? tk.PL : tk.PG;
+        double2* out = wblk(which == 0 ? tk.WL : tk.WG, l);
+        gemm_store(WRc, false, blk(P, l), false, tmp(T_F1));                      // WR P
+        gemm_store(tmp(T_F1), false, WRc, true, out);                             // WR P WR^H
+        gemm_store(Wj, false, blk(P, jp), false, tmp(T_F1));                      // Wi_j P_j'
+        gemm(tmp(T_F1), false, NWTj, false, [&](int i, int j, double2 v) {
+          const int idx = i + j * nn;
+          out[idx] = cadd(out[idx], v);
+        });
+        gemm_store(NWTm, false, blk(P, (l > 0 ? l - 1 : 0)), false, tmp(T_F1));   // -Wi_m^T P_m
+        gemm(tmp(T_F1), false, Wm, false, [&](int i, int j, double2 v) {
+          const int idx = i + j * nn;
+          out[idx] = cadd(out[idx], v);
+        });
+      }
+      double2* t;
+      t = M1c; M1c = M1p; M1p = t;
+      t = Woc; Woc = Wop; Wop = t;
+      t = Wic; Wic = Wip; Wip = t;
+      t = NWTc; NWTc = NWTp; NWTp = t;
+    }
+    if (info && threadIdx.x == 0) {
+      info->status = status;
+      info->sancho_iters_left = 0;
+      info->sancho_iters_right = 0;
+      info->n_gemm = n_gemm;
+      info->n_inv = n_inv;
+    }
+    __syncthreads();
+  }
+
   __device__ void run_adjoint(const DAdj& tk, const DDev& dv, DInfo* info) {
     const int nn = n;
     const double E = tk.E;
@@ -771,7 +903,7 @@ template <class Ops>
 __device__ __forceinline__ void solve_task(const KParams& p, int64_t t, double2* slot, Smem& sm,
                                            double2* dyn_smem) {
   DInfo* info = p.info ? p.info + t : nullptr;
-  const int dev = p.adj ? p.adj[t].dev : p.tasks[t].dev;
+  const int dev = p.adj ? p.adj[t].dev : (p.wtasks ? p.wtasks[t].dev : p.tasks[t].dev);
   const DDev dv = p.devs[dev];
   const int n = (int)dv.nm;
   const size_t n2 = (size_t)n * n;
@@ -779,6 +911,7 @@ __device__ __forceinline__ void solve_task(const KParams& p, int64_t t, double2*
   Ops ops(sm.inv, dyn_smem, temps + (size_t)T_INV * n2, temps + (size_t)T_RT * n2, n);
   Solver<Ops> s(p.o, dv.nx, sm, ops, slot, n, (int)dv.nx);
   if (p.adj) s.run_adjoint(p.adj[t], dv, info);
+  else if (p.wtasks) s.run_w(p.wtasks[t], dv, info);
   else s.run(p.tasks[t], dv, info);
 }
 

@@ -48,6 +48,7 @@ EXPORTS = (
     "rgf_ctx_get_stats", "rgf_adjoint_energies", "rgf_solve_energies_noalloc",
     "rgf_noalloc_last_error", "rgf_calc_block_current", "rgf_plan_create", "rgf_plan_execute",
     "rgf_plan_destroy", "rgf_autotune", "rgf_variant_name", "rgf_green_rgf_cms",
+    "rgf_w_solve_batch", "rgf_w_solve_energies", "rgf_green_rgf_calc_w",
 )
 
 # kernel variant ids (rgf_variant_name)
@@ -89,6 +90,17 @@ class c_task(ctypes.Structure):
         ("cur", ctypes.c_void_p), ("tr", ctypes.c_void_p), ("tre", ctypes.c_void_p),
         ("T", ctypes.c_void_p),
     ]
+
+
+class c_w_device(ctypes.Structure):
+    _fields_ = [("nm", ctypes.c_int64), ("nx", ctypes.c_int64), ("Vii", ctypes.c_void_p),
+                ("V1i", ctypes.c_void_p)]
+
+
+class c_w_task(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("reserved", ctypes.c_int32), ("PL", ctypes.c_void_p),
+                ("PG", ctypes.c_void_p), ("PR", ctypes.c_void_p), ("WL", ctypes.c_void_p),
+                ("WG", ctypes.c_void_p), ("WR", ctypes.c_void_p), ("WRi1", ctypes.c_void_p)]
 
 
 class c_stats(ctypes.Structure):
@@ -133,6 +145,12 @@ def load(path: str = LIB_PATH):
     L.rgf_rgf_g.argtypes = [P] * 20
     L.rgf_green_rgf_cms.argtypes = [P] * 21
     L.rgf_green_rgf_cms.restype = ctypes.c_int
+    L.rgf_w_solve_batch.argtypes = [P, ctypes.POINTER(c_w_device), ctypes.c_int32,
+                                    ctypes.POINTER(c_w_task), ctypes.c_int64, P, P]
+    L.rgf_w_solve_energies.argtypes = [P, ctypes.POINTER(c_w_device), ctypes.c_int64] + [P] * 9
+    L.rgf_green_rgf_calc_w.argtypes = [P] * 18
+    for name in ("rgf_w_solve_batch", "rgf_w_solve_energies", "rgf_green_rgf_calc_w"):
+        getattr(L, name).restype = ctypes.c_int
     L.rgf_solve_energies.argtypes = [P, ctypes.POINTER(c_device), ctypes.c_int64] + [P] * 13
     L.rgf_terminal_current.argtypes = [P, P, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_int64, P]
@@ -348,6 +366,19 @@ class Context:
         return {"nb": r.nb, "variant": VARIANTS[r.variant], "ctas_per_sm": r.ctas_per_sm,
                 "candidates": cands}
 
+    def w_solve_energies(self, Vii, V1i, PL, PG, PR, *, WL, WG, WR, WRi1=None, info=None,
+                         stream=None, allow_status=True):
+        """rgf_w_solve_energies: W^<, W^>, W^R (and W^R_{l,l+1}) of every
+        energy of one q-point; arrays (nen, nx, nm, nm), host or device."""
+        nx, nm = int(Vii.shape[0]), int(Vii.shape[1])
+        d = c_w_device()
+        d.nm, d.nx = nm, nx
+        d.Vii, d.V1i = _ptr(Vii), _ptr(V1i)
+        nen = int(PL.shape[0])
+        rc = load().rgf_w_solve_energies(self.h, ctypes.byref(d), nen, _ptr(PL), _ptr(PG), _ptr(PR),
+                                         _ptr(WL), _ptr(WG), _ptr(WR), _ptr(WRi1), _ptr(info), stream)
+        return _check(rc, allow_status)
+
     def solve_batch(self, devices, tasks, info=None, stream=None, allow_status=True):
         """rgf_solve_batch with ctypes c_device / c_task arrays."""
         nd, nt = len(devices), len(tasks)
@@ -419,6 +450,22 @@ def green_RGF_CMS(TEMP, nm, nx, E, mu, Sii, Hii, H1i, sigma_lesser_ph, sigma_gre
     return _drop_in(load().rgf_green_rgf_cms, False, TEMP, nm, nx, E, mu, Hii, H1i,
                     sigma_lesser_ph, sigma_greater_ph, sigma_r_ph, ndens, pdens, ldos, tr, tre,
                     cur, GRi1, GLi1, GGi1, ctx, Sii=Sii)
+
+
+def green_rgf_calc_w(NBC, nm, nx, Vii, V1i, PL, PG, PR, WL, WG, WR, PL1i=None, PG1i=None, PR1i=None,
+                     WLi1=None, WGi1=None, WRi1=None, ctx=None):
+    """Drop-in for green_rgf_calc_w (src/green_rgf.f90:3399) / RGF_W
+    (src/rgf_mod.f90:242): same argument order; WL, WG, WR (and WRi1) are
+    written in place."""
+    nbc = ctypes.c_int64(int(NBC))
+    nm_ = ctypes.c_int64(int(nm))
+    nx_ = ctypes.c_int64(int(nx))
+    h = ctx.h if ctx is not None else None
+    P = _ptr
+    _check(load().rgf_green_rgf_calc_w(h, ctypes.addressof(nbc), ctypes.addressof(nm_),
+                                       ctypes.addressof(nx_), P(Vii), P(V1i), P(PL), P(PG), P(PR),
+                                       P(WL), P(WG), P(WR), P(PL1i), P(PG1i), P(PR1i), P(WLi1),
+                                       P(WGi1), P(WRi1)))
 
 
 def _drop_in(fn, rgf_g_order, TEMP, nm, nx, E, mu, Hii, H1i, sl, sg, sr, ndens, pdens, ldos, tr,

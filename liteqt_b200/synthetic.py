@@ -83,6 +83,52 @@ def make_overlap(nm: int, nx: int, seed: int = 4321, sigma: float = 0.05) -> np.
     return _to_fortran_blocks(Sb)
 
 
+def make_coulomb(nm: int, nx: int, seed: int = 99, a: float = 0.3, cell: float = 0.5,
+                 width: float = 2.0, e2: float = 1.44) -> tuple[np.ndarray, np.ndarray]:
+    """Bare Coulomb interaction of the GW workloads as block-tridiagonal
+    blocks: orbital positions seeded uniformly in cells of `cell` nm along the
+    chain (block l at x in [l*cell, (l+1)*cell)) and `width` nm across,
+    V_ij = e2 / (|r_i - r_j| + a) eV (e2 = e^2/(4 pi eps0) = 1.44 eV nm,
+    a = 0.3 nm), truncated to the diagonal blocks and the first
+    off-diagonal blocks.  Returns (Vii, V1i) in the Fortran block layout;
+    V1i[l] is V_{l+1,l} (zero for l = nx-1), real, so V is real symmetric."""
+    rng = np.random.default_rng(seed)
+    pos = np.empty((nx, nm, 3))
+    for l in range(nx):
+        pos[l, :, 0] = rng.uniform(l * cell, (l + 1) * cell, nm)
+        pos[l, :, 1:] = rng.uniform(0.0, width, (nm, 2))
+
+    def block(p, q):
+        r = np.linalg.norm(p[:, None, :] - q[None, :, :], axis=-1)
+        return e2 / (r + a)
+    Vb = np.array([block(pos[l], pos[l]) for l in range(nx)], dtype=np.complex128)
+    V1b = np.zeros((nx, nm, nm), np.complex128)
+    for l in range(nx - 1):
+        V1b[l] = block(pos[l + 1], pos[l])
+    return _to_fortran_blocks(Vb), _to_fortran_blocks(V1b)
+
+
+def make_polarization(nm: int, nx: int, nen: int, seed: int = 7, scale: float = 0.05):
+    """Seeded polarization blocks (PL, PG, PR), each (nen, nx, nm, nm) in the
+    Fortran block layout, with the symmetries of the physical P: P^R complex
+    symmetric with a negative-semidefinite imaginary part, P^< and P^>
+    anti-Hermitian and complex symmetric (i times a real symmetric matrix,
+    P^< with a non-negative, P^> with a non-positive spectrum)."""
+    rng = np.random.default_rng(seed)
+    out = [np.empty((nen, nx, nm, nm), np.complex128) for _ in range(3)]
+    for e in range(nen):
+        for l in range(nx):
+            X = rng.normal(0.0, 1.0, (nm, nm))
+            Y = rng.normal(0.0, 1.0, (nm, nm))
+            A = (X + X.T) / np.sqrt(2 * nm)
+            B = Y @ Y.T / nm                       # real symmetric PSD
+            f = rng.uniform(0.0, 1.0)
+            out[2][e, l] = scale * (A - 1j * B)    # P^R
+            out[0][e, l] = 1j * scale * 2 * f * B   # P^<
+            out[1][e, l] = -1j * scale * 2 * (1 - f) * B  # P^>
+    return tuple(out)
+
+
 def uniform_chain(nm: int, nx: int, t: float = -1.0, eps: float = 0.0) -> Device:
     """nm decoupled identical 1D chains: H_ll = eps*I, H_{l,l-1} = t*I.
     Its exact transmission is nm inside the band |E - eps| < 2|t|."""

@@ -133,6 +133,9 @@ def lib():
         L.oracle_rgf_batch.argtypes = [ctypes.POINTER(OracleOpts), ctypes.c_int64, ctypes.c_int64,
                                        ctypes.c_int64] + [P] * 19 + [ctypes.c_int, ctypes.c_int]
         L.oracle_rgf_batch.restype = ctypes.c_int
+        L.oracle_rgf_w_batch.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64] + [P] * 10 + \
+            [ctypes.c_int, ctypes.c_int]
+        L.oracle_rgf_w_batch.restype = ctypes.c_int
         L.oracle_calc_n_electron.argtypes = [P, P, ctypes.c_int64, P, ctypes.c_int64,
                                              ctypes.c_int64, ctypes.c_int64, P, P, P]
         L.oracle_calc_n_electron.restype = None
@@ -203,6 +206,80 @@ def rgf_batch(Hii, H1i, E, mu, temp, opts: Opts | None = None, sig_lesser=None, 
                                 int(extended))
     out.update(tr=tr, tre=tre, T=T, stats=stats, status=rc)
     return out
+
+
+def rgf_w_batch(Vii, V1i, PL, PG, PR, threads: int | None = None, extended: bool = False):
+    """green_rgf_calc_w / RGF_W (NBC = 0, no off-diagonal P) over a batch.
+
+    Vii, V1i: (nx, nm, nm) Fortran block layout; PL, PG, PR: (nE, nx, nm, nm).
+    Returns dict WL, WG, WR, WRi1 (nE, nx, nm, nm; WRi1 block nx zero) and
+    'stats'."""
+    nx, nm, _ = Vii.shape
+    Vii = _fortran3(Vii, nm, nx)
+    V1i = _fortran3(V1i, nm, nx)
+    PL, PG, PR = (np.ascontiguousarray(a, np.complex128) for a in (PL, PG, PR))
+    nE = PL.shape[0]
+    out = {k: np.zeros((nE, nx, nm, nm), np.complex128) for k in ("WL", "WG", "WR", "WRi1")}
+    stats = np.zeros(nE, STAT_DTYPE)
+    rc = lib().oracle_rgf_w_batch(nm, nx, nE, _p(Vii), _p(V1i), _p(PL), _p(PG), _p(PR), _p(out["WL"]),
+                                  _p(out["WG"]), _p(out["WR"]), _p(out["WRi1"]), _p(stats),
+                                  int(threads or os.cpu_count() or 1), int(extended))
+    out.update(stats=stats, status=rc)
+    return out
+
+
+def rgf_w_numpy(Vb, V1b, PLb, PGb, PRb):
+    """One W solve of green_rgf_calc_w (NBC = 0, no off-diagonal P) on
+    mathematical blocks (l = 0..nx-1; V1b[l] is V1i(:,:,l+1) = V_{l+1,l})."""
+    nx, nm, _ = Vb.shape
+    I = np.eye(nm)
+    M = [I - Vb[i] @ PRb[i] for i in range(nx)]
+    M1i = [-V1b[i] @ PRb[i] for i in range(nx - 1)]
+    Mi1 = [-V1b[i].conj().T @ PRb[i + 1] for i in range(nx - 1)]
+    xlr = [None] * nx
+    Wlr = [None] * nx
+    xlr[-1] = np.linalg.inv(M[-1])
+    Wlr[-1] = xlr[-1] @ Vb[-1]
+    for i in range(nx - 2, -1, -1):
+        B = Mi1[i] @ xlr[i + 1]
+        xlr[i] = np.linalg.inv(M[i] - B @ M1i[i])
+        Wlr[i] = xlr[i] @ (Vb[i] - B @ V1b[i])
+    WR = [None] * nx
+    Wo = [None] * (nx - 1)
+    WR[0] = Wlr[0]
+    Wo[0] = (V1b[0].T - WR[0] @ M1i[0].T) @ xlr[1].T
+    for i in range(1, nx):
+        WR[i] = Wlr[i] - xlr[i] @ M1i[i - 1] @ Wo[i - 1]
+        if i < nx - 1:
+            Wo[i] = (V1b[i].T - WR[i] @ M1i[i].T) @ xlr[i + 1].T
+    Wi = [1j * w.imag for w in Wo]
+    WL, WG = [], []
+    for P, out in ((PLb, WL), (PGb, WG)):
+        for i in range(nx):
+            jo, jp = (i, i + 1) if i < nx - 1 else (nx - 2, nx - 1)
+            m = max(i - 1, 0)
+            out.append(WR[i] @ P[i] @ WR[i].conj().T + Wi[jo] @ P[jp] @ (-Wi[jo]).T
+                       + Wi[m].T @ P[m] @ (-Wi[m]))
+    return dict(WR=np.array(WR), WRi1=np.array(Wo), WL=np.array(WL), WG=np.array(WG))
+
+
+def dense_w(Vb, V1b, PRb):
+    """Known answer: W^R = (I - V P^R)^-1 V of the whole (truncated) device,
+    V block-tridiagonal with V_{l+1,l} = V1b[l], V_{l,l+1} = V1b[l]^H and
+    P^R block-diagonal."""
+    nx, nm, _ = Vb.shape
+    N = nx * nm
+    V = np.zeros((N, N), complex)
+    P = np.zeros((N, N), complex)
+    for l in range(nx):
+        s = slice(l * nm, (l + 1) * nm)
+        V[s, s] = Vb[l]
+        P[s, s] = PRb[l]
+        if l < nx - 1:
+            s1 = slice((l + 1) * nm, (l + 2) * nm)
+            V[s1, s] = V1b[l]
+            V[s, s1] = V1b[l].conj().T
+    return np.linalg.solve(np.eye(N) - V @ P, V)
 
 
 def calc_n_electron(G_lesser, G_greater, E, midgap):

@@ -638,6 +638,147 @@ extern "C" int oracle_rgf_batch(const OracleOpts* opts, int64_t nm, int64_t nx, 
   return worst.load();
 }
 
+// ---------------------------------------------------------------- RGF_W
+// green_rgf_calc_w (green_rgf.f90:3399-3831) == RGF_W (rgf_mod.f90:242-674)
+// with NBC = 0 and the off-diagonal P blocks absent, as at every call site
+// (green_rgf.f90:846, :1551, :3008).  W^R = (I - V P^R)^-1 V by a
+// right-to-left sweep of left-connected blocks and a left-to-right sweep;
+// W^< / W^> from WR and the imaginary part of the off-diagonal blocks
+// (:3803-3829), with the routine's transposes and index max(ix-1,1) as they
+// are.  The routine's LL / LG blocks (:3495-3560), its wln / wlp (:3702-3708)
+// and its XR recursion (:3752-3757) feed nothing that is returned and are not
+// restated.  WRi1 (if non-null) receives blocks 1..nx-1 of the full complex
+// off-diagonal block; block nx is left untouched.
+namespace {
+
+template <typename R>
+int rgf_w_energy(int64_t nm64, int64_t nx64, const cd* Vii_in, const cd* V1i_in, const cd* PL_in,
+                 const cd* PG_in, const cd* PR_in, cd* WL_out, cd* WG_out, cd* WR_out, cd* WRi1_out,
+                 OracleStat* st) {
+  typedef std::complex<R> C;
+  typedef std::complex<double> cdd;
+  OracleStat dummy{};
+  if (!st) st = &dummy;
+  std::memset(st, 0, sizeof(*st));
+  if (nm64 < 1 || nx64 < 2 || nm64 > 4096) { st->status = ST_BAD_ARGS; return ST_BAD_ARGS; }
+  const int nm = (int)nm64, nx = (int)nx64;
+  const size_t n2 = nn(nm), nall = n2 * (size_t)nx;
+  Work<R> w(nm, st);
+  std::vector<C> Vii(Vii_in, Vii_in + nall), V1i(V1i_in, V1i_in + nall), PL(PL_in, PL_in + nall),
+      PG(PG_in, PG_in + nall), PR(PR_in, PR_in + nall);
+  auto b = [&](std::vector<C>& v, int l) { return v.data() + (size_t)(l - 1) * n2; };  // 1-based
+  std::vector<C> M(nall), M1i(nall), Mi1(nall), xlr(nall), Wlr(nall), WR(nall), WRi1(nall);
+  std::vector<C> A(n2), B(n2), Cm(n2), D(n2), T1(n2);
+  // S = V P^R; M = I - S, M1i = -S_{i+1,i}, Mi1 = -S_{i,i+1} (:3450-3485)
+  for (int ix = 1; ix <= nx; ix++) {
+    w.gemm('n', 'n', b(Vii, ix), b(PR, ix), A.data());
+    for (size_t k = 0; k < n2; k++) b(M, ix)[k] = -A[k];
+    for (int i = 0; i < nm; i++) b(M, ix)[i + (size_t)i * nm] += C(1, 0);
+  }
+  for (int i = 1; i <= nx - 1; i++) {
+    w.gemm('n', 'n', b(V1i, i), b(PR, i), A.data());
+    for (size_t k = 0; k < n2; k++) b(M1i, i)[k] = -A[k];
+    w.gemm('c', 'n', b(V1i, i), b(PR, i + 1), A.data());
+    for (size_t k = 0; k < n2; k++) b(Mi1, i)[k] = -A[k];
+  }
+  std::copy(b(M1i, nx - 1), b(M1i, nx - 1) + n2, b(M1i, nx));
+  std::copy(b(Mi1, nx - 1), b(Mi1, nx - 1) + n2, b(Mi1, nx));
+  // right-to-left pass (:3710-3722)
+  std::copy(b(M, nx), b(M, nx) + n2, A.begin());
+  w.invert(A.data());
+  std::copy(A.begin(), A.end(), b(xlr, nx));
+  w.gemm('n', 'n', A.data(), b(Vii, nx), b(Wlr, nx));
+  for (int ix = nx - 1; ix >= 1; ix--) {
+    w.gemm('n', 'n', b(Mi1, ix), b(xlr, ix + 1), B.data());
+    w.gemm('n', 'n', B.data(), b(M1i, ix), Cm.data());
+    for (size_t k = 0; k < n2; k++) A[k] = b(M, ix)[k] - Cm[k];
+    w.invert(A.data());
+    std::copy(A.begin(), A.end(), b(xlr, ix));
+    w.gemm('n', 'n', B.data(), b(V1i, ix), Cm.data());
+    for (size_t k = 0; k < n2; k++) D[k] = b(Vii, ix)[k] - Cm[k];
+    w.gemm('n', 'n', A.data(), D.data(), b(Wlr, ix));
+  }
+  // left-to-right pass (:3740-3778)
+  auto offdiag = [&](int ix) {  // WRi1_(ix) = (V1i(ix)^T - WR(ix) M1i(ix)^T) xlr(ix+1)^T
+    w.gemm('n', 't', b(WR, ix), b(M1i, ix), B.data());
+    for (int j = 0; j < nm; j++)
+      for (int i = 0; i < nm; i++) Cm[i + (size_t)j * nm] = b(V1i, ix)[j + (size_t)i * nm] - B[i + (size_t)j * nm];
+    w.gemm('n', 't', Cm.data(), b(xlr, ix + 1), b(WRi1, ix));
+  };
+  std::copy(b(Wlr, 1), b(Wlr, 1) + n2, b(WR, 1));
+  offdiag(1);
+  for (int ix = 2; ix <= nx; ix++) {
+    w.gemm('n', 'n', b(xlr, ix), b(M1i, ix - 1), B.data());
+    w.gemm('n', 'n', B.data(), b(WRi1, ix - 1), Cm.data());
+    for (size_t k = 0; k < n2; k++) b(WR, ix)[k] = b(Wlr, ix)[k] - Cm[k];
+    if (ix < nx) offdiag(ix);
+  }
+  if (WRi1_out)
+    for (size_t k = 0; k < n2 * (size_t)(nx - 1); k++)
+      WRi1_out[k] = cdd((double)WRi1[k].real(), (double)WRi1[k].imag());
+  // W^< and W^> (:3786-3829): the off-diagonal blocks enter with their real
+  // part zeroed
+  for (size_t k = 0; k < nall; k++) WRi1[k] = C(R(0) * WRi1[k].real(), WRi1[k].imag());
+  auto wlg = [&](std::vector<C>& P, cd* out) {
+    for (int ix = 1; ix <= nx; ix++) {
+      w.gemm('n', 'n', b(WR, ix), b(P, ix), A.data());
+      w.gemm('n', 'c', A.data(), b(WR, ix), B.data());
+      const int jo = ix < nx ? ix : ix - 1, jp = ix < nx ? ix + 1 : nx;
+      for (size_t k = 0; k < n2; k++) T1[k] = -b(WRi1, jo)[k];
+      w.gemm('n', 'n', b(WRi1, jo), b(P, jp), A.data());
+      w.gemm('n', 't', A.data(), T1.data(), Cm.data());
+      for (size_t k = 0; k < n2; k++) B[k] += Cm[k];
+      const int m = ix - 1 > 1 ? ix - 1 : 1;
+      for (size_t k = 0; k < n2; k++) T1[k] = -b(WRi1, m)[k];
+      w.gemm('t', 'n', b(WRi1, m), b(P, m), A.data());
+      w.gemm('n', 'n', A.data(), T1.data(), Cm.data());
+      for (size_t k = 0; k < n2; k++) B[k] += Cm[k];
+      if (out)
+        for (size_t k = 0; k < n2; k++)
+          out[(size_t)(ix - 1) * n2 + k] = cdd((double)B[k].real(), (double)B[k].imag());
+    }
+  };
+  wlg(PL, WL_out);
+  wlg(PG, WG_out);
+  if (WR_out)
+    for (size_t k = 0; k < nall; k++) WR_out[k] = cdd((double)WR[k].real(), (double)WR[k].imag());
+  return st->status;
+}
+
+}  // namespace
+
+// Batch of W solves: one device (Vii, V1i) and nE polarization sets
+// (PL, PG, PR strided by nm*nm*nx), one per worker thread.
+extern "C" int oracle_rgf_w_batch(int64_t nm, int64_t nx, int64_t nE, const cd* Vii, const cd* V1i,
+                                  const cd* PL, const cd* PG, const cd* PR, cd* WL, cd* WG, cd* WR,
+                                  cd* WRi1, OracleStat* stats, int n_threads, int extended) {
+  const size_t per = (size_t)nm * nm * nx;
+  std::atomic<int64_t> next(0);
+  std::atomic<int> worst(0);
+  auto worker = [&]() {
+    for (;;) {
+      const int64_t e = next.fetch_add(1);
+      if (e >= nE) break;
+      OracleStat st{};
+      auto off = [&](cd* p) { return p ? p + e * per : nullptr; };
+      const int s = extended
+          ? rgf_w_energy<long double>(nm, nx, Vii, V1i, PL + e * per, PG + e * per, PR + e * per,
+                                      off(WL), off(WG), off(WR), off(WRi1), &st)
+          : rgf_w_energy<double>(nm, nx, Vii, V1i, PL + e * per, PG + e * per, PR + e * per, off(WL),
+                                 off(WG), off(WR), off(WRi1), &st);
+      if (stats) stats[e] = st;
+      int cur_w = worst.load();
+      while ((s | cur_w) != cur_w && !worst.compare_exchange_weak(cur_w, s | cur_w)) {}
+    }
+  };
+  if (n_threads < 1) n_threads = 1;
+  std::vector<std::thread> pool;
+  for (int t = 1; t < n_threads; t++) pool.emplace_back(worker);
+  worker();
+  for (auto& t : pool) t.join();
+  return worst.load();
+}
+
 // calc_n_electron (green_rgf.f90:3920-3945) for one k-point set laid out as
 // (nm,nm,nx,nen,nk).  nelec/pelec have nx entries.
 extern "C" void oracle_calc_n_electron(const cd* G_lesser, const cd* G_greater, int64_t nen,

@@ -388,3 +388,67 @@ def test_cms_sancho_fixed_point_with_overlap(oracle_mod):
         z = complex(E, opts.eta_lead)
         R = G - np.linalg.inv(z * S00 - H00 - H10.conj().T @ G @ H10)
         assert np.linalg.norm(R) < 1e-8 * np.linalg.norm(G)
+
+
+# ---------------------------------------------------------------- RGF_W
+def _rand_blocks(rng, nx, nm, scale):
+    return np.array([rng.normal(0, scale, (nm, nm)) + 1j * rng.normal(0, scale, (nm, nm)) for _ in range(nx)])
+
+
+@pytest.mark.parametrize("nm,nx", [(6, 2), (6, 5), (10, 4)])
+def test_w_cpp_matches_numpy_restatement(oracle_mod, nm, nx):
+    """General (non-symmetric) inputs: the C++ and NumPy restatements of
+    green_rgf_calc_w agree, transposes and quirks included."""
+    O = oracle_mod
+    rng = np.random.default_rng(nm + nx)
+    Vb = np.array([np.eye(nm) + b + b.conj().T for b in _rand_blocks(rng, nx, nm, 0.15)])
+    V1b = _rand_blocks(rng, nx, nm, 0.2)
+    nE = 3
+    P = [np.array([_rand_blocks(rng, nx, nm, 0.2) for _ in range(nE)]) for _ in range(3)]
+    F = lambda a: np.array([O.from_blocks(x) for x in a]) if a.ndim == 4 else O.from_blocks(a)
+    r = O.rgf_w_batch(F(Vb), F(V1b), F(P[0]), F(P[1]), F(P[2]), threads=2)
+    for e in range(nE):
+        t = O.rgf_w_numpy(Vb, V1b, P[0][e], P[1][e], P[2][e])
+        for k in ("WR", "WL", "WG"):
+            assert rel_err(O.to_blocks(r[k][e]), t[k]) < 1e-12, k
+        assert rel_err(O.to_blocks(r["WRi1"][e])[:-1], t["WRi1"]) < 1e-12
+        assert np.all(r["WRi1"][e][-1] == 0)
+    st = r["stats"][0]
+    # S blocks 3 nx - 2, right-to-left 4 (nx - 1) + 1, left-to-right 4 (nx - 1), W^< / W^> 12 nx
+    assert st["n_inv"] == nx and st["n_gemm"] == 23 * nx - 9
+
+
+@pytest.mark.parametrize("nm,nx", [(5, 3), (8, 6)])
+def test_w_dense_known_answer(oracle_mod, nm, nx):
+    """Coulomb V (real symmetric) and complex-symmetric P^R, the case the
+    routine's transposes assume: W^R_ll and W^R_{l,l+1} equal the blocks of
+    (I - V P^R)^-1 V of the whole device."""
+    O = oracle_mod
+    Vii, V1i = S.make_coulomb(nm, nx, seed=nm)
+    PL, PG, PR = S.make_polarization(nm, nx, 2, seed=nx)
+    r = O.rgf_w_batch(Vii, V1i, PL, PG, PR, threads=1)
+    Vb, V1b = O.to_blocks(Vii), O.to_blocks(V1i)
+    for e in range(2):
+        W = O.dense_w(Vb, V1b, O.to_blocks(PR[e]))
+        WR, Wo = O.to_blocks(r["WR"][e]), O.to_blocks(r["WRi1"][e])
+        sc = np.max(np.abs(W))
+        for l in range(nx):
+            s = slice(l * nm, (l + 1) * nm)
+            assert np.max(np.abs(WR[l] - W[s, s])) < 1e-12 * sc
+            if l < nx - 1:
+                s1 = slice((l + 1) * nm, (l + 2) * nm)
+                assert np.max(np.abs(Wo[l] - W[s, s1])) < 1e-12 * sc
+
+
+def test_w_lesser_formula_and_symmetry(oracle_mod):
+    """W^< from the routine's formula: with the off-diagonal blocks' real part
+    zeroed, WL_ll = WR P^< WR^H + neighbour terms; for anti-Hermitian P^< the
+    result is anti-Hermitian."""
+    O = oracle_mod
+    nm, nx = 6, 4
+    Vii, V1i = S.make_coulomb(nm, nx, seed=3)
+    PL, PG, PR = S.make_polarization(nm, nx, 1, seed=5)
+    r = O.rgf_w_batch(Vii, V1i, PL, PG, PR, threads=1)
+    WL = O.to_blocks(r["WL"][0])
+    for l in range(nx):
+        assert np.max(np.abs(WL[l] + WL[l].conj().T)) < 1e-12 * np.max(np.abs(WL[l]))
