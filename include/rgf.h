@@ -309,6 +309,35 @@ RGF_API int rgf_green_rgf_calc_w(rgf_ctx* ctx, const int64_t* NBC, const int64_t
                                  rgf_c16* WR, const rgf_c16* PL1i, const rgf_c16* PG1i,
                                  const rgf_c16* PR1i, rgf_c16* WLi1, rgf_c16* WGi1, rgf_c16* WRi1);
 
+/* The energy / k convolutions of the GW loop of green_rgf_solve_gw_3d
+ * (src/green_rgf.f90:2944-3092), as the reference computes them: direct
+ * banded sums (|i - j| <= ndiag) over energies and k-points, with
+ * nopmax = nen/2 - 10 energy offsets, k - q taken with the reference's nk/2
+ * shift, dE = En(2) - En(1).  All arrays (nm,nm,nx,nen,nk), nk = nky*nkz,
+ * host or device memory.  imag_only = 1 reads G with its real part zeroed, as
+ * the reference zeroes it before these steps (:2940-2942).
+ *
+ * rgf_gw_polarization: P^<, P^>, P^R (:2944-2999), zero outside the band and
+ * outside the nopmax window.
+ * rgf_gw_self_energy: the new Sigma^<, Sigma^>, Sigma^R from G and W
+ * (:3020-3065), Sigma^R's imaginary part from Sigma^> - Sigma^< (:3068),
+ * symmetrisation (:3070-3081), mixing into Sigma_*_gw with alpha_mix
+ * (:3083-3085) and the copies of blocks 3 / nx-2 into the two edge blocks of
+ * each side (:3087-3092); Sigma_*_gw are updated in place (nx >= 3).
+ * Error text: rgf_gw_last_error(). */
+RGF_API int rgf_gw_polarization(rgf_ctx* ctx, int64_t nm, int64_t nx, int64_t nen, int64_t nky,
+                                int64_t nkz, int64_t ndiag, double dE, double spindeg,
+                                int32_t imag_only, const rgf_c16* G_lesser, const rgf_c16* G_greater,
+                                const rgf_c16* G_r, rgf_c16* P_lesser, rgf_c16* P_greater,
+                                rgf_c16* P_retarded, void* stream);
+RGF_API int rgf_gw_self_energy(rgf_ctx* ctx, int64_t nm, int64_t nx, int64_t nen, int64_t nky,
+                               int64_t nkz, int64_t ndiag, double dE, double alpha_mix,
+                               int32_t imag_only, const rgf_c16* G_lesser, const rgf_c16* G_greater,
+                               const rgf_c16* G_r, const rgf_c16* W_lesser, const rgf_c16* W_greater,
+                               const rgf_c16* W_retarded, rgf_c16* Sigma_lesser_gw,
+                               rgf_c16* Sigma_greater_gw, rgf_c16* Sigma_r_gw, void* stream);
+RGF_API const char* rgf_gw_last_error(void);
+
 /* Terminal current of one energy sweep: sum(tr)*dE*e0/tpi/hbar*e0*spindeg/nk
  * (green_rgf.f90:2938), summed on the device in a fixed order. */
 RGF_API int rgf_terminal_current(rgf_ctx* ctx, const double* tr, int64_t nen, double dE, double spindeg,

@@ -49,6 +49,7 @@ EXPORTS = (
     "rgf_noalloc_last_error", "rgf_calc_block_current", "rgf_plan_create", "rgf_plan_execute",
     "rgf_plan_destroy", "rgf_autotune", "rgf_variant_name", "rgf_green_rgf_cms",
     "rgf_w_solve_batch", "rgf_w_solve_energies", "rgf_green_rgf_calc_w",
+    "rgf_gw_polarization", "rgf_gw_self_energy", "rgf_gw_last_error",
 )
 
 # kernel variant ids (rgf_variant_name)
@@ -151,6 +152,12 @@ def load(path: str = LIB_PATH):
     L.rgf_green_rgf_calc_w.argtypes = [P] * 18
     for name in ("rgf_w_solve_batch", "rgf_w_solve_energies", "rgf_green_rgf_calc_w"):
         getattr(L, name).restype = ctypes.c_int
+    I64, D = ctypes.c_int64, ctypes.c_double
+    L.rgf_gw_polarization.argtypes = [P] + [I64] * 6 + [D, D, ctypes.c_int32] + [P] * 7
+    L.rgf_gw_self_energy.argtypes = [P] + [I64] * 6 + [D, D, ctypes.c_int32] + [P] * 10
+    L.rgf_gw_polarization.restype = ctypes.c_int
+    L.rgf_gw_self_energy.restype = ctypes.c_int
+    L.rgf_gw_last_error.restype = ctypes.c_char_p
     L.rgf_solve_energies.argtypes = [P, ctypes.POINTER(c_device), ctypes.c_int64] + [P] * 13
     L.rgf_terminal_current.argtypes = [P, P, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_int64, P]
@@ -378,6 +385,28 @@ class Context:
         rc = load().rgf_w_solve_energies(self.h, ctypes.byref(d), nen, _ptr(PL), _ptr(PG), _ptr(PR),
                                          _ptr(WL), _ptr(WG), _ptr(WR), _ptr(WRi1), _ptr(info), stream)
         return _check(rc, allow_status)
+
+    def gw_polarization(self, GL, GG, GR, *, PL, PG, PR, nky, nkz, ndiag, dE, spindeg, imag_only=True,
+                        stream=None):
+        """rgf_gw_polarization; arrays (nk, nen, nx, nm, nm) (the Fortran
+        (nm,nm,nx,nen,nk) layout), host or device."""
+        nk, nen, nx, nm = (int(v) for v in GL.shape[:4])
+        rc = load().rgf_gw_polarization(self.h, nm, nx, nen, int(nky), int(nkz), int(ndiag), float(dE),
+                                        float(spindeg), int(imag_only), _ptr(GL), _ptr(GG), _ptr(GR),
+                                        _ptr(PL), _ptr(PG), _ptr(PR), stream)
+        if rc != RGF_OK:
+            raise RgfError(rc, load().rgf_gw_last_error().decode())
+
+    def gw_self_energy(self, GL, GG, GR, WL, WG, WR, *, SL, SG, SR, nky, nkz, ndiag, dE, alpha_mix,
+                       imag_only=True, stream=None):
+        """rgf_gw_self_energy; SL / SG / SR (the running self-energies) are
+        updated in place."""
+        nk, nen, nx, nm = (int(v) for v in GL.shape[:4])
+        rc = load().rgf_gw_self_energy(self.h, nm, nx, nen, int(nky), int(nkz), int(ndiag), float(dE),
+                                       float(alpha_mix), int(imag_only), _ptr(GL), _ptr(GG), _ptr(GR),
+                                       _ptr(WL), _ptr(WG), _ptr(WR), _ptr(SL), _ptr(SG), _ptr(SR), stream)
+        if rc != RGF_OK:
+            raise RgfError(rc, load().rgf_gw_last_error().decode())
 
     def solve_batch(self, devices, tasks, info=None, stream=None, allow_status=True):
         """rgf_solve_batch with ctypes c_device / c_task arrays."""

@@ -136,6 +136,13 @@ def lib():
         L.oracle_rgf_w_batch.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64] + [P] * 10 + \
             [ctypes.c_int, ctypes.c_int]
         L.oracle_rgf_w_batch.restype = ctypes.c_int
+        I64 = ctypes.c_int64
+        L.oracle_gw_polarization.argtypes = [I64] * 6 + [ctypes.c_double, ctypes.c_double, ctypes.c_int] + \
+            [P] * 6 + [ctypes.c_int]
+        L.oracle_gw_polarization.restype = None
+        L.oracle_gw_self_energy.argtypes = [I64] * 6 + [ctypes.c_double, ctypes.c_double, ctypes.c_int] + \
+            [P] * 9 + [ctypes.c_int]
+        L.oracle_gw_self_energy.restype = None
         L.oracle_calc_n_electron.argtypes = [P, P, ctypes.c_int64, P, ctypes.c_int64,
                                              ctypes.c_int64, ctypes.c_int64, P, P, P]
         L.oracle_calc_n_electron.restype = None
@@ -280,6 +287,104 @@ def dense_w(Vb, V1b, PRb):
             V[s1, s] = V1b[l]
             V[s, s1] = V1b[l].conj().T
     return np.linalg.solve(np.eye(N) - V @ P, V)
+
+
+def gw_polarization(GL, GG, GR, nky, nkz, ndiag, dE, spindeg, imag_only=True, threads=None):
+    """P^<, P^>, P^R of green_rgf_solve_gw_3d (green_rgf.f90:2944-2999).
+    G arrays (nk, nen, nx, nm, nm): the NumPy view of the Fortran
+    (nm,nm,nx,nen,nk) layout.  Returns (PL, PG, PR) in the same layout."""
+    GL, GG, GR = (np.ascontiguousarray(a, np.complex128) for a in (GL, GG, GR))
+    nk, nen, nx, nm, _ = GL.shape
+    out = [np.zeros_like(GL) for _ in range(3)]
+    lib().oracle_gw_polarization(nm, nx, nen, nky, nkz, ndiag, float(dE), float(spindeg), int(imag_only),
+                                 _p(GL), _p(GG), _p(GR), _p(out[0]), _p(out[1]), _p(out[2]),
+                                 int(threads or os.cpu_count() or 1))
+    return tuple(out)
+
+
+def gw_self_energy(GL, GG, GR, WL, WG, WR, SL, SG, SR, nky, nkz, ndiag, dE, alpha_mix, imag_only=True,
+                   threads=None):
+    """New GW self-energies, Sigma^R's imaginary part, symmetrisation, mixing
+    into SL / SG / SR (updated in place) and the edge copies
+    (green_rgf.f90:3020-3092).  Same layout as gw_polarization."""
+    GL, GG, GR, WL, WG, WR = (np.ascontiguousarray(a, np.complex128) for a in (GL, GG, GR, WL, WG, WR))
+    for a in (SL, SG, SR):
+        assert a.flags["C_CONTIGUOUS"] and a.dtype == np.complex128
+    nk, nen, nx, nm, _ = GL.shape
+    lib().oracle_gw_self_energy(nm, nx, nen, nky, nkz, ndiag, float(dE), float(alpha_mix), int(imag_only),
+                                _p(GL), _p(GG), _p(GR), _p(WL), _p(WG), _p(WR), _p(SL), _p(SG), _p(SR),
+                                int(threads or os.cpu_count() or 1))
+
+
+def _kd(ik, iq, nky, nkz):
+    """0-based k - q index with the reference's nk/2 shift (green_rgf.f90:2968-2977)."""
+    iky, ikz = divmod(ik, nkz)
+    iqy, iqz = divmod(iq, nkz)
+    ikzd = (ikz - iqz + nkz // 2 - 1) % nkz if nkz > 1 else 0
+    ikyd = (iky - iqy + nky // 2 - 1) % nky if nky > 1 else 0
+    return ikzd + ikyd * nkz
+
+
+def gw_polarization_numpy(GLm, GGm, GRm, nky, nkz, ndiag, dE, spindeg):
+    """Independent vectorised restatement (small cases).  Arrays indexed
+    [ik, ie, ix, i, j] with mathematical (row i, column j) blocks; real
+    parts already zeroed by the caller."""
+    nk, nen, nx, nm, _ = GLm.shape
+    nopmax = nen // 2 - 10
+    i, j = np.indices((nm, nm))
+    band = np.abs(i - j) <= ndiag
+    PL, PG, PR = (np.zeros_like(GLm) for _ in range(3))
+    T = lambda X: np.swapaxes(X, -1, -2)
+    for nop in range(-nopmax, nopmax + 1):
+        iop = nop + nen // 2 - 1
+        lo, hi = max(nop + 1, 1) - 1, min(nen, nen + nop)   # 0-based ie range [lo, hi)
+        for iq in range(nk):
+            for ik in range(nk):
+                kd = _kd(ik, iq, nky, nkz)
+                a = slice(lo, hi)
+                b = slice(lo - nop, hi - nop)
+                PL[iq, iop] += np.sum(GLm[ik, a] * T(GGm[kd, b]), axis=0)
+                PG[iq, iop] += np.sum(GGm[ik, a] * T(GLm[kd, b]), axis=0)
+                PR[iq, iop] += np.sum(GLm[ik, a] * np.conj(GRm[kd, b]) + GRm[ik, a] * T(GLm[kd, b]), axis=0)
+    f = complex(0.0, -dE / 2.0 / 3.14159265359) * spindeg / nk
+    return tuple(np.where(band, X, 0) * f for X in (PL, PG, PR))
+
+
+def gw_self_energy_numpy(GLm, GGm, GRm, WLm, WGm, WRm, SLm, SGm, SRm, nky, nkz, ndiag, dE, alpha_mix):
+    """Independent vectorised restatement of gw_self_energy on [ik, ie, ix,
+    i, j] mathematical blocks (G real parts already zeroed).  Returns the
+    updated (SL, SG, SR)."""
+    nk, nen, nx, nm, _ = GLm.shape
+    nopmax = nen // 2 - 10
+    i, j = np.indices((nm, nm))
+    band = np.abs(i - j) <= ndiag
+    nL, nG, nR = (np.zeros_like(GLm) for _ in range(3))
+    for ie in range(1, nen + 1):
+        for ik in range(nk):
+            for nop in range(-nopmax, nopmax + 1):
+                if not (ie > max(nop, 1) and ie < nen + nop):
+                    continue
+                iop = nop + nen // 2 - 1
+                for iq in range(nk):
+                    kd = _kd(ik, iq, nky, nkz)
+                    g, gg, gr = GLm[kd, ie - nop - 1], GGm[kd, ie - nop - 1], GRm[kd, ie - nop - 1]
+                    nL[ik, ie - 1] += g * WLm[iq, iop]
+                    nG[ik, ie - 1] += gg * WGm[iq, iop]
+                    nR[ik, ie - 1] += g * WRm[iq, iop] + gr * WLm[iq, iop] + gr * WRm[iq, iop]
+    f = complex(0.0, dE / 2.0 / 3.14159265359) / nk
+    nL, nG, nR = (np.where(band, X, 0) * f for X in (nL, nG, nR))
+    nR = nR.real + 1j * (nG - nL).imag / 2.0
+    sym = lambda X: (X + np.swapaxes(X, -1, -2)) / 2.0
+    nL, nG, nR = sym(nL), sym(nG), sym(nR)
+    out = []
+    for S, N in ((SLm, nL), (SGm, nG), (SRm, nR)):
+        S = S + alpha_mix * (N - S)
+        S[:, :, 0] = S[:, :, 2]
+        S[:, :, 1] = S[:, :, 2]
+        S[:, :, nx - 1] = S[:, :, nx - 3]
+        S[:, :, nx - 2] = S[:, :, nx - 3]
+        out.append(S)
+    return tuple(out)
 
 
 def calc_n_electron(G_lesser, G_greater, E, midgap):

@@ -779,6 +779,167 @@ extern "C" int oracle_rgf_w_batch(int64_t nm, int64_t nx, int64_t nE, const cd* 
   return worst.load();
 }
 
+// ---------------------------------------------------------- GW convolutions
+// The polarization and GW self-energy of green_rgf_solve_gw_3d
+// (green_rgf.f90:2944-3092): banded (|i-j| <= ndiag) direct energy / k sums,
+// accumulated in the reference's loop order per element.  All arrays are
+// (nm,nm,nx,nen,nk) column-major; nk = nky*nkz, ik = ikz + (iky-1)*nkz.
+// imag_only: read G with its real part zeroed (the reference zeroes it in
+// place before P, :2940-2942, and Sigma then sees the same arrays).
+namespace {
+
+const double kPiGW = 3.14159265359;  // the module's pi (green_rgf.f90:23)
+
+struct GWIdx {
+  int64_t nm, nx, nen, nky, nkz;
+  size_t at(int64_t i, int64_t j, int64_t ix, int64_t ie, int64_t ik) const {  // 1-based
+    return (size_t)(i - 1) + (size_t)nm * ((j - 1) + (size_t)nm * ((ix - 1) + (size_t)nx * ((ie - 1) + (size_t)nen * (ik - 1))));
+  }
+  int64_t kd(int64_t iky, int64_t ikz, int64_t iqy, int64_t iqz) const {  // :2968-2977
+    int64_t ikzd = ikz - iqz + nkz / 2, ikyd = iky - iqy + nky / 2;
+    if (ikzd < 1) ikzd += nkz;
+    if (ikzd > nkz) ikzd -= nkz;
+    if (ikyd < 1) ikyd += nky;
+    if (ikyd > nky) ikyd -= nky;
+    if (nky == 1) ikyd = 1;
+    if (nkz == 1) ikzd = 1;
+    return ikzd + (ikyd - 1) * nkz;
+  }
+};
+
+inline cd gread(const cd* G, size_t k, int imag_only) {
+  return imag_only ? cd(0.0 * G[k].real(), G[k].imag()) : G[k];
+}
+
+}  // namespace
+
+extern "C" void oracle_gw_polarization(int64_t nm, int64_t nx, int64_t nen, int64_t nky, int64_t nkz,
+                                       int64_t ndiag, double dEn, double spindeg, int imag_only,
+                                       const cd* GL, const cd* GG, const cd* GR, cd* PL, cd* PG,
+                                       cd* PR, int n_threads) {
+  const GWIdx X{nm, nx, nen, nky, nkz};
+  const int64_t nk = nky * nkz, nopmax = nen / 2 - 10;
+  const size_t total = (size_t)nm * nm * nx * nen * nk;
+  std::fill(PL, PL + total, cd(0, 0));
+  std::fill(PG, PG + total, cd(0, 0));
+  std::fill(PR, PR + total, cd(0, 0));
+  std::atomic<int64_t> next(-nopmax);
+  auto worker = [&]() {
+    for (;;) {
+      const int64_t nop = next.fetch_add(1);
+      if (nop > nopmax) break;
+      const int64_t iop = nop + nen / 2;
+      for (int64_t iqy = 1; iqy <= nky; iqy++)
+        for (int64_t iqz = 1; iqz <= nkz; iqz++) {
+          const int64_t iq = iqz + (iqy - 1) * nkz;
+          for (int64_t ix = 1; ix <= nx; ix++)
+            for (int64_t i = 1; i <= nm; i++) {
+              const int64_t l = std::max<int64_t>(i - ndiag, 1), h = std::min<int64_t>(nm, i + ndiag);
+              for (int64_t iky = 1; iky <= nky; iky++)
+                for (int64_t ikz = 1; ikz <= nkz; ikz++) {
+                  const int64_t ik = ikz + (iky - 1) * nkz, ikd = X.kd(iky, ikz, iqy, iqz);
+                  for (int64_t ie = std::max<int64_t>(nop + 1, 1); ie <= std::min<int64_t>(nen, nen + nop); ie++)
+                    for (int64_t j = l; j <= h; j++) {
+                      const size_t o = X.at(i, j, ix, iop, iq);
+                      const size_t a = X.at(i, j, ix, ie, ik), bt = X.at(j, i, ix, ie - nop, ikd),
+                                   b = X.at(i, j, ix, ie - nop, ikd);
+                      PL[o] += gread(GL, a, imag_only) * gread(GG, bt, imag_only);
+                      PG[o] += gread(GG, a, imag_only) * gread(GL, bt, imag_only);
+                      PR[o] += gread(GL, a, imag_only) * std::conj(gread(GR, b, imag_only)) +
+                               gread(GR, a, imag_only) * gread(GL, bt, imag_only);
+                    }
+                }
+            }
+        }
+    }
+  };
+  if (n_threads < 1) n_threads = 1;
+  std::vector<std::thread> pool;
+  for (int t = 1; t < n_threads; t++) pool.emplace_back(worker);
+  worker();
+  for (auto& t : pool) t.join();
+  const cd dE = cd(0.0, -1.0 * dEn / 2.0 / kPiGW) * spindeg / (double)nk;  // :2996
+  for (size_t k = 0; k < total; k++) { PL[k] *= dE; PG[k] *= dE; PR[k] *= dE; }
+}
+
+// New self-energies (:3020-3068), then Sigma^R's imaginary part from
+// Sigma^> - Sigma^<, symmetrisation, mixing into the *_gw arrays and the
+// edge-block copies (:3069-3092).  SL / SG / SR are the *_gw arrays (inout).
+extern "C" void oracle_gw_self_energy(int64_t nm, int64_t nx, int64_t nen, int64_t nky, int64_t nkz,
+                                      int64_t ndiag, double dEn, double alpha_mix, int imag_only,
+                                      const cd* GL, const cd* GG, const cd* GR, const cd* WL,
+                                      const cd* WG, const cd* WR, cd* SL, cd* SG, cd* SR,
+                                      int n_threads) {
+  const GWIdx X{nm, nx, nen, nky, nkz};
+  const int64_t nk = nky * nkz, nopmax = nen / 2 - 10;
+  const size_t total = (size_t)nm * nm * nx * nen * nk;
+  std::vector<cd> nL(total, cd(0, 0)), nG(total, cd(0, 0)), nR(total, cd(0, 0));
+  std::atomic<int64_t> next(1);
+  auto worker = [&]() {
+    for (;;) {
+      const int64_t ie = next.fetch_add(1);
+      if (ie > nen) break;
+      for (int64_t iky = 1; iky <= nky; iky++)
+        for (int64_t ikz = 1; ikz <= nkz; ikz++)
+          for (int64_t nop = -nopmax; nop <= nopmax; nop++) {
+            if (!(ie > std::max<int64_t>(nop, 1) && ie < nen + nop)) continue;
+            const int64_t ik = ikz + (iky - 1) * nkz, iop = nop + nen / 2;
+            for (int64_t iqy = 1; iqy <= nky; iqy++)
+              for (int64_t iqz = 1; iqz <= nkz; iqz++) {
+                const int64_t iq = iqz + (iqy - 1) * nkz, ikd = X.kd(iky, ikz, iqy, iqz);
+                for (int64_t ix = 1; ix <= nx; ix++)
+                  for (int64_t i = 1; i <= nm; i++) {
+                    const int64_t l = std::max<int64_t>(i - ndiag, 1), h = std::min<int64_t>(nm, i + ndiag);
+                    for (int64_t j = l; j <= h; j++) {
+                      const size_t o = X.at(i, j, ix, ie, ik), g = X.at(i, j, ix, ie - nop, ikd),
+                                   w = X.at(i, j, ix, iop, iq);
+                      nL[o] += gread(GL, g, imag_only) * WL[w];
+                      nG[o] += gread(GG, g, imag_only) * WG[w];
+                      nR[o] += gread(GL, g, imag_only) * WR[w] + gread(GR, g, imag_only) * WL[w] +
+                               gread(GR, g, imag_only) * WR[w];
+                    }
+                  }
+              }
+          }
+    }
+  };
+  if (n_threads < 1) n_threads = 1;
+  std::vector<std::thread> pool;
+  for (int t = 1; t < n_threads; t++) pool.emplace_back(worker);
+  worker();
+  for (auto& t : pool) t.join();
+  const cd dE = cd(0.0, dEn / 2.0 / kPiGW) / (double)nk;  // :3064
+  for (size_t k = 0; k < total; k++) {
+    nL[k] *= dE;
+    nG[k] *= dE;
+    nR[k] *= dE;
+  }
+  for (size_t k = 0; k < total; k++) nR[k] = cd(nR[k].real(), (nG[k] - nL[k]).imag() / 2.0);  // :3068
+  const size_t n2 = (size_t)nm * nm;
+  std::vector<cd> B(n2);
+  for (size_t blk = 0; blk < total / n2; blk++)  // symmetrise each (ix, ie, ik) block (:3070-3081)
+    for (std::vector<cd>* A : {&nR, &nL, &nG}) {
+      cd* a = A->data() + blk * n2;
+      for (int64_t j = 0; j < nm; j++)
+        for (int64_t i = 0; i < nm; i++) B[i + j * nm] = a[j + i * nm];
+      for (size_t k = 0; k < n2; k++) a[k] = (a[k] + B[k]) / 2.0;
+    }
+  for (size_t k = 0; k < total; k++) {  // mixing (:3083-3085)
+    SR[k] = SR[k] + alpha_mix * (nR[k] - SR[k]);
+    SL[k] = SL[k] + alpha_mix * (nL[k] - SL[k]);
+    SG[k] = SG[k] + alpha_mix * (nG[k] - SG[k]);
+  }
+  auto copy_block = [&](cd* A, int64_t dst, int64_t src) {  // A(:,:,dst,:,:) = A(:,:,src,:,:)
+    for (int64_t ik = 1; ik <= nk; ik++)
+      for (int64_t ie = 1; ie <= nen; ie++)
+        std::copy(A + X.at(1, 1, src, ie, ik), A + X.at(1, 1, src, ie, ik) + n2, A + X.at(1, 1, dst, ie, ik));
+  };
+  for (int64_t ix = 1; ix <= 2; ix++)  // :3087-3091
+    for (cd* A : {SR, SL, SG}) copy_block(A, ix, 3);
+  for (int64_t ix = 1; ix <= 2; ix++)
+    for (cd* A : {SR, SL, SG}) copy_block(A, nx - ix + 1, nx - 2);
+}
+
 // calc_n_electron (green_rgf.f90:3920-3945) for one k-point set laid out as
 // (nm,nm,nx,nen,nk).  nelec/pelec have nx entries.
 extern "C" void oracle_calc_n_electron(const cd* G_lesser, const cd* G_greater, int64_t nen,

@@ -452,3 +452,42 @@ def test_w_lesser_formula_and_symmetry(oracle_mod):
     WL = O.to_blocks(r["WL"][0])
     for l in range(nx):
         assert np.max(np.abs(WL[l] + WL[l].conj().T)) < 1e-12 * np.max(np.abs(WL[l]))
+
+
+# ------------------------------------------------------------ GW convolutions
+def _gw_inputs(rng, nk, nen, nx, nm, n):
+    return [rng.normal(size=(nk, nen, nx, nm, nm)) + 1j * rng.normal(size=(nk, nen, nx, nm, nm))
+            for _ in range(n)]
+
+
+def _swap(X):
+    return np.ascontiguousarray(np.swapaxes(X, -1, -2))
+
+
+@pytest.mark.parametrize("nky,nkz,ndiag", [(1, 1, 0), (2, 2, 2), (1, 3, 1), (3, 1, 4)])
+def test_gw_polarization_cpp_matches_numpy(oracle_mod, nky, nkz, ndiag):
+    O = oracle_mod
+    rng = np.random.default_rng(nky * 10 + nkz)
+    nk, nen, nx, nm = nky * nkz, 30, 3, 5
+    G = _gw_inputs(rng, nk, nen, nx, nm, 3)
+    P = O.gw_polarization(*[_swap(g) for g in G], nky, nkz, ndiag, 0.01, 2.0, imag_only=True, threads=2)
+    Pn = O.gw_polarization_numpy(*[1j * g.imag for g in G], nky, nkz, ndiag, 0.01, 2.0)
+    for a, b in zip(P, Pn):
+        assert rel_err(_swap(a), b) < 1e-13
+
+
+@pytest.mark.parametrize("nky,nkz,ndiag,nx", [(1, 2, 1, 6), (2, 1, 3, 4), (1, 1, 0, 3)])
+def test_gw_self_energy_cpp_matches_numpy(oracle_mod, nky, nkz, ndiag, nx):
+    O = oracle_mod
+    rng = np.random.default_rng(nx + ndiag)
+    nk, nen, nm = nky * nkz, 28, 4
+    G = _gw_inputs(rng, nk, nen, nx, nm, 3)
+    W = _gw_inputs(rng, nk, nen, nx, nm, 3)
+    S = [np.zeros((nk, nen, nx, nm, nm), complex) for _ in range(3)]
+    Sf = [_swap(s) for s in S]
+    O.gw_self_energy(*[_swap(g) for g in G], *[_swap(w) for w in W], *Sf, nky, nkz, ndiag, 0.02, 0.7,
+                     imag_only=True, threads=2)
+    Sn = O.gw_self_energy_numpy(*[1j * g.imag for g in G], *W, *S, nky, nkz, ndiag, 0.02, 0.7)
+    for a, b in zip(Sf, Sn):
+        assert rel_err(_swap(a), b) < 1e-13
+        assert np.max(np.abs(b)) > 0
