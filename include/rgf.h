@@ -338,6 +338,17 @@ RGF_API int rgf_gw_self_energy(rgf_ctx* ctx, int64_t nm, int64_t nx, int64_t nen
                                rgf_c16* Sigma_greater_gw, rgf_c16* Sigma_r_gw, void* stream);
 RGF_API const char* rgf_gw_last_error(void);
 
+/* Local transpose of the GW loop's energy <-> (i,j) redistribution
+ * (energies_to_ijs_2 / ijs_to_energies_2, src/green_rgf.f90:243-329):
+ * dst = RESHAPE(src, dst_shape, ORDER=order) with Fortran's meaning, for pure
+ * transposes (dst_shape(order(k)) = src_shape(k)); order is 1-based, ndim <= 8.
+ * src and dst are device arrays of complex(8); stream-ordered, returns after
+ * the launch.  The MPI_Alltoall between the two transposes is NCCL's
+ * all-to-all (liteqt_b200/redistribute.py). */
+RGF_API int rgf_permute_c16(rgf_ctx* ctx, const rgf_c16* src, rgf_c16* dst, int32_t ndim,
+                            const int64_t* src_shape, const int32_t* order, void* stream);
+RGF_API const char* rgf_permute_last_error(void);
+
 /* Terminal current of one energy sweep: sum(tr)*dE*e0/tpi/hbar*e0*spindeg/nk
  * (green_rgf.f90:2938), summed on the device in a fixed order. */
 RGF_API int rgf_terminal_current(rgf_ctx* ctx, const double* tr, int64_t nen, double dE, double spindeg,

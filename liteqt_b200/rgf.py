@@ -49,7 +49,8 @@ EXPORTS = (
     "rgf_noalloc_last_error", "rgf_calc_block_current", "rgf_plan_create", "rgf_plan_execute",
     "rgf_plan_destroy", "rgf_autotune", "rgf_variant_name", "rgf_green_rgf_cms",
     "rgf_w_solve_batch", "rgf_w_solve_energies", "rgf_green_rgf_calc_w",
-    "rgf_gw_polarization", "rgf_gw_self_energy", "rgf_gw_last_error",
+    "rgf_gw_polarization", "rgf_gw_self_energy", "rgf_gw_last_error", "rgf_permute_c16",
+    "rgf_permute_last_error",
 )
 
 # kernel variant ids (rgf_variant_name)
@@ -158,6 +159,9 @@ def load(path: str = LIB_PATH):
     L.rgf_gw_polarization.restype = ctypes.c_int
     L.rgf_gw_self_energy.restype = ctypes.c_int
     L.rgf_gw_last_error.restype = ctypes.c_char_p
+    L.rgf_permute_c16.argtypes = [P, P, P, ctypes.c_int32, P, P, P]
+    L.rgf_permute_c16.restype = ctypes.c_int
+    L.rgf_permute_last_error.restype = ctypes.c_char_p
     L.rgf_solve_energies.argtypes = [P, ctypes.POINTER(c_device), ctypes.c_int64] + [P] * 13
     L.rgf_terminal_current.argtypes = [P, P, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_int64, P]
@@ -407,6 +411,16 @@ class Context:
                                        _ptr(WL), _ptr(WG), _ptr(WR), _ptr(SL), _ptr(SG), _ptr(SR), stream)
         if rc != RGF_OK:
             raise RgfError(rc, load().rgf_gw_last_error().decode())
+
+    def permute(self, src, dst, src_shape, order, stream=None):
+        """rgf_permute_c16: dst = RESHAPE(src, ORDER=order) (Fortran meaning,
+        1-based order) of flat complex128 device tensors."""
+        shp = (ctypes.c_int64 * len(src_shape))(*[int(v) for v in src_shape])
+        odr = (ctypes.c_int32 * len(order))(*[int(v) for v in order])
+        rc = load().rgf_permute_c16(self.h, _ptr(src), _ptr(dst), len(src_shape), ctypes.addressof(shp),
+                                    ctypes.addressof(odr), stream)
+        if rc != RGF_OK:
+            raise RgfError(rc, load().rgf_permute_last_error().decode())
 
     def solve_batch(self, devices, tasks, info=None, stream=None, allow_status=True):
         """rgf_solve_batch with ctypes c_device / c_task arrays."""
