@@ -402,6 +402,39 @@ RGF_API int rgf_calc_block_current(rgf_ctx* ctx, const rgf_c16* H, const rgf_c16
                                    int64_t ns, int64_t nm, int64_t nx, double* tot_cur,
                                    double* tot_ecur, double* jdens);
 
+/* The reference's output writers, so a driver keeps writing identical files
+ * (src/green_rgf.f90:4541-4896, :2937-2939).  Sums run on the GPU in each
+ * routine's loop order; text follows the routine's FORMAT ('(4E18.4)',
+ * '(3E18.4)', '(2E18.4)', '(I4,2E16.6)'; a blank line for `write(11,*)`);
+ * files are named dataset // STRING(i) // '.dat' (STRING: 4 digits,
+ * zero-padded) or dataset // '_' // STRING(i) // '.dat' as each routine does.
+ * Arrays host or device; append as the optional argument.
+ *   rgf_write_spectrum: write_spectrum (summed_over_k = 0, nk = 1) and
+ *     write_spectrum_summed_over_k (summed_over_k = 1), G(NB*NS,NB*NS,length,nen,nk);
+ *   rgf_write_dos: write_dos_summed_over_k;
+ *   rgf_write_current_spectrum: write_current_spectrum (kz_summed = 0,
+ *     cur(NB,NB,length,nen), name with '_') and ..._summed_over_kz (kz_summed = 1,
+ *     cur(NB,NB,length,nen,nk));
+ *   rgf_write_current_summed_over_k: cur(NB,NB,nx,nk);
+ *   rgf_write_transmission_spectrum: write_transmission_spectrum (nk = 0,
+ *     tr(nen), name with '_') and write_transmission_spectrum_k (tr(nen,nk));
+ *   rgf_write_id_iteration: one line of Id_iteration.dat (appended). */
+RGF_API int rgf_write_spectrum(rgf_ctx* ctx, const char* dataset, int32_t iter, const rgf_c16* G, int64_t nen,
+                               const double* en, int64_t nk, int64_t length, int64_t NB, int64_t NS, double Lx,
+                               const double* coeff, int32_t summed_over_k, int32_t append);
+RGF_API int rgf_write_dos(rgf_ctx* ctx, const char* dataset, int32_t iter, const rgf_c16* G, int64_t nen,
+                          const double* en, int64_t nk, int64_t length, int64_t NB, int64_t NS, double Lx,
+                          int32_t append);
+RGF_API int rgf_write_current_spectrum(rgf_ctx* ctx, const char* dataset, int32_t iter, const double* cur,
+                                       int64_t nen, const double* en, int64_t nk, int64_t length, int64_t NB,
+                                       double Lx, int32_t kz_summed, int32_t append);
+RGF_API int rgf_write_current_summed_over_k(rgf_ctx* ctx, const char* dataset, int32_t iter, const double* cur,
+                                            int64_t nx, int64_t NB, double Lx, int64_t nk);
+RGF_API int rgf_write_transmission_spectrum(const char* dataset, int32_t iter, const double* tr, int64_t nen,
+                                            const double* en, int64_t nk, int32_t append);
+RGF_API int rgf_write_id_iteration(const char* path, int32_t iter, double current_left, double current_right);
+RGF_API const char* rgf_io_last_error(void);
+
 /* Last error message of the calling thread ("" if none). */
 RGF_API const char* rgf_last_error(void);
 

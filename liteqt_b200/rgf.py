@@ -50,7 +50,9 @@ EXPORTS = (
     "rgf_plan_destroy", "rgf_autotune", "rgf_variant_name", "rgf_green_rgf_cms",
     "rgf_w_solve_batch", "rgf_w_solve_energies", "rgf_green_rgf_calc_w",
     "rgf_gw_polarization", "rgf_gw_self_energy", "rgf_gw_last_error", "rgf_permute_c16",
-    "rgf_permute_last_error",
+    "rgf_permute_last_error", "rgf_write_spectrum", "rgf_write_dos", "rgf_write_current_spectrum",
+    "rgf_write_current_summed_over_k", "rgf_write_transmission_spectrum", "rgf_write_id_iteration",
+    "rgf_io_last_error",
 )
 
 # kernel variant ids (rgf_variant_name)
@@ -162,6 +164,17 @@ def load(path: str = LIB_PATH):
     L.rgf_permute_c16.argtypes = [P, P, P, ctypes.c_int32, P, P, P]
     L.rgf_permute_c16.restype = ctypes.c_int
     L.rgf_permute_last_error.restype = ctypes.c_char_p
+    S, I32 = ctypes.c_char_p, ctypes.c_int32
+    L.rgf_write_spectrum.argtypes = [P, S, I32, P, I64, P, I64, I64, I64, I64, D, P, I32, I32]
+    L.rgf_write_dos.argtypes = [P, S, I32, P, I64, P, I64, I64, I64, I64, D, I32]
+    L.rgf_write_current_spectrum.argtypes = [P, S, I32, P, I64, P, I64, I64, I64, D, I32, I32]
+    L.rgf_write_current_summed_over_k.argtypes = [P, S, I32, P, I64, I64, D, I64]
+    L.rgf_write_transmission_spectrum.argtypes = [S, I32, P, I64, P, I64, I32]
+    L.rgf_write_id_iteration.argtypes = [S, I32, D, D]
+    for name in ("rgf_write_spectrum", "rgf_write_dos", "rgf_write_current_spectrum",
+                 "rgf_write_current_summed_over_k", "rgf_write_transmission_spectrum", "rgf_write_id_iteration"):
+        getattr(L, name).restype = ctypes.c_int
+    L.rgf_io_last_error.restype = ctypes.c_char_p
     L.rgf_solve_energies.argtypes = [P, ctypes.POINTER(c_device), ctypes.c_int64] + [P] * 13
     L.rgf_terminal_current.argtypes = [P, P, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_int64, P]
