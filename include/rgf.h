@@ -79,7 +79,11 @@ typedef struct rgf_opts {
   int32_t precision;       /* RGF_PREC_FP64 or RGF_PREC_MIXED */
   int32_t want_T;          /* also compute Caroli T(E) (green.f90:2571-2580) */
   int32_t verbose;         /* 1: print "SEVERE warning" lines like the reference */
-  int32_t reserved[7];
+  int32_t zero_copy;       /* 1 (default): outputs in pinned host memory that the solver only
+                              writes (all but `cur`) are written by the kernels through their
+                              device mapping, so the transfer overlaps the solve; 0: staged in
+                              device memory and copied back after the launch */
+  int32_t reserved[6];
 } rgf_opts;
 
 typedef struct rgf_ctx rgf_ctx;

@@ -102,6 +102,7 @@ extern "C" void rgf_opts_default(rgf_opts* o) {
   o->precision = RGF_PREC_FP64;
   o->want_T = 1;
   o->verbose = 0;
+  o->zero_copy = 1;
 }
 
 extern "C" const char* rgf_last_error(void) { return g_last_error.c_str(); }
@@ -197,12 +198,37 @@ struct Stage {
     size_t off;
     bool copy_in, copy_out;
   };
+  // Pinned (page-locked, mapped) host outputs the kernels only write are not
+  // staged: the kernels write them through their device mapping, so the
+  // device-to-host transfer overlaps the solve instead of following it.
+  struct Direct {
+    const char* host;
+    size_t bytes;
+    char* dev;
+  };
   std::vector<Item> items;
   std::vector<Seg> segs;
+  std::vector<Direct> direct;
   size_t total = 0;
+  bool zero_copy = true;
 
-  void add(const void* p, size_t bytes, bool copy_in, bool copy_out) {
-    if (!p || bytes == 0 || is_device_ptr(p)) return;
+  void add(const void* p, size_t bytes, bool copy_in, bool copy_out, bool write_only = false) {
+    if (!p || bytes == 0) return;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+      cudaGetLastError();
+      a.type = cudaMemoryTypeUnregistered;
+    }
+    if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) return;
+    if (zero_copy && write_only && copy_out && a.type == cudaMemoryTypeHost && a.devicePointer &&
+        a.hostPointer) {
+      const char* h = (const char*)p;
+      const char* base = (const char*)a.hostPointer;
+      if (h >= base) {
+        direct.push_back({h, bytes, (char*)a.devicePointer + (h - base)});
+        return;
+      }
+    }
     items.push_back({(const char*)p, bytes, copy_in, copy_out});
   }
   void layout() {
@@ -230,6 +256,8 @@ struct Stage {
   void* resolve(const void* p, char* dbase) const {
     if (!p) return nullptr;
     const char* h = (const char*)p;
+    for (const Direct& d : direct)
+      if (h >= d.host && h < d.host + d.bytes) return d.dev + (h - d.host);
     size_t lo = 0, hi = segs.size();
     while (lo < hi) {  // last segment with host <= h
       const size_t mid = (lo + hi) / 2;
@@ -333,6 +361,7 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
 
   // ---- staging of host arrays
   Stage sg;
+  sg.zero_copy = c->opts.zero_copy != 0;
   for (int32_t d = 0; d < n_devices; d++) {
     const size_t bytes = (size_t)devices[d].nm * devices[d].nm * devices[d].nx * sizeof(rgf_c16);
     sg.add(devices[d].Hii, bytes, true, false);
@@ -346,16 +375,18 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
     const size_t rb = (size_t)v.nm * v.nm * v.nx * sizeof(double);
     sg.add(k.sigma_lesser, cb, true, false);
     sg.add(k.sigma_r, cb, true, false);
-    sg.add(k.ldos, cb, false, true);
-    sg.add(k.ndens, cb, false, true);
-    sg.add(k.pdens, cb, false, true);
-    sg.add(k.GRi1, cb, true, true);   // block nx is left untouched, as in the reference
-    sg.add(k.GLi1, cb, true, true);
-    sg.add(k.GGi1, cb, true, true);
+    // the solver writes these and never reads them back (cur is read-modify-
+    // written, so it is always staged)
+    sg.add(k.ldos, cb, false, true, true);
+    sg.add(k.ndens, cb, false, true, true);
+    sg.add(k.pdens, cb, false, true, true);
+    sg.add(k.GRi1, cb, true, true, true);   // block nx is left untouched, as in the reference
+    sg.add(k.GLi1, cb, true, true, true);
+    sg.add(k.GGi1, cb, true, true, true);
     sg.add(k.cur, rb, false, true);
-    sg.add(k.tr, sizeof(double), false, true);
-    sg.add(k.tre, sizeof(double), false, true);
-    if (want_T) sg.add(k.T, sizeof(double), false, true);
+    sg.add(k.tr, sizeof(double), false, true, true);
+    sg.add(k.tre, sizeof(double), false, true, true);
+    if (want_T) sg.add(k.T, sizeof(double), false, true, true);
   }
   sg.layout();
   rc = c->stage.reserve(std::max<size_t>(sg.total, 256));
@@ -1015,6 +1046,7 @@ extern "C" int rgf_w_solve_batch(rgf_ctx* c, const rgf_w_device* devices, int32_
   RGF_CUDA(cudaSetDevice(c->device));
   cudaStream_t st = stream_ ? (cudaStream_t)stream_ : c->stream;
   Stage sg;
+  sg.zero_copy = c->opts.zero_copy != 0;
   for (int32_t d = 0; d < n_devices; d++) {
     const size_t bytes = (size_t)devices[d].nm * devices[d].nm * devices[d].nx * sizeof(rgf_c16);
     sg.add(devices[d].Vii, bytes, true, false);
@@ -1027,10 +1059,10 @@ extern "C" int rgf_w_solve_batch(rgf_ctx* c, const rgf_w_device* devices, int32_
     sg.add(k.PL, cb, true, false);
     sg.add(k.PG, cb, true, false);
     sg.add(k.PR, cb, true, false);
-    sg.add(k.WL, cb, false, true);
+    sg.add(k.WL, cb, false, true);   // accumulated in place while W^< forms: staged
     sg.add(k.WG, cb, false, true);
-    sg.add(k.WR, cb, false, true);
-    sg.add(k.WRi1, cb, true, true);  // block nx is left untouched
+    sg.add(k.WR, cb, false, true, true);
+    sg.add(k.WRi1, cb, true, true, true);  // block nx is left untouched
   }
   sg.layout();
   int rc = c->stage.reserve(std::max<size_t>(sg.total, 256));

@@ -72,7 +72,7 @@ class c_opts(ctypes.Structure):
         ("boltz", ctypes.c_double), ("sancho_tol", ctypes.c_double),
         ("sancho_nmax", ctypes.c_int32), ("consistent", ctypes.c_int32),
         ("precision", ctypes.c_int32), ("want_T", ctypes.c_int32),
-        ("verbose", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7),
+        ("verbose", ctypes.c_int32), ("zero_copy", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6),
     ]
 
 
@@ -228,6 +228,7 @@ class Options:
     precision: int = RGF_PREC_FP64
     want_T: bool = True
     verbose: bool = False
+    zero_copy: bool = True
 
     def c(self) -> c_opts:
         o = c_opts()
@@ -242,6 +243,7 @@ class Options:
         o.precision = int(self.precision)
         o.want_T = int(self.want_T)
         o.verbose = int(self.verbose)
+        o.zero_copy = int(self.zero_copy)
         return o
 
 

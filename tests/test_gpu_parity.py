@@ -333,3 +333,29 @@ def test_calc_block_current_matches_oracle(rgf, ns):
     tc2, te2, jd2 = O.calc_block_current(H, G, E, 2.0, nb, ns, jdens=True)
     for a, b in ((tc, tc2), (te, te2), (jd, jd2)):
         assert np.allclose(a, b, rtol=1e-13, atol=1e-13 * np.max(np.abs(b)))
+
+
+@pytest.mark.parametrize("zero_copy", [True, False])
+def test_pinned_host_outputs_match_device_outputs(rgf, zero_copy):
+    """Outputs in pinned host memory (written by the kernels through their
+    device mapping when zero_copy is on, staged otherwise) are bit-identical
+    to device-resident outputs; `cur` (read back by the solver) is staged."""
+    import torch
+    nm, nx = 32, 5
+    d = S.make_device(nm, nx, seed=61)
+    E = S.energy_grid(6, -2.0, 2.0)
+    shape = (len(E), nx, nm, nm)
+    dev = torch.device("cuda", 0)
+    keys_c = ("ldos", "ndens", "pdens", "GRi1")
+    dv = {k: torch.zeros(shape, dtype=torch.complex128, device=dev) for k in keys_c}
+    dv["cur"] = torch.zeros(shape, dtype=torch.float64, device=dev)
+    for k in ("tr", "tre", "T"):
+        dv[k] = torch.zeros(len(E), dtype=torch.float64, device=dev)
+    pin = {k: torch.zeros(v.shape, dtype=v.dtype).pin_memory() for k, v in dv.items()}
+    Hd, H1d = torch.from_numpy(d.Hii).to(dev), torch.from_numpy(d.H1i).to(dev)
+    with rgf.Context(rgf.Options(zero_copy=zero_copy)) as ctx:
+        ctx.solve_energies(Hd, H1d, E, MU, _temp(), **dv)
+        ctx.solve_energies(d.Hii, d.H1i, E, MU, _temp(), **{k: v.numpy() for k, v in pin.items()})
+    torch.cuda.synchronize()
+    for k in dv:
+        assert np.array_equal(pin[k].numpy(), dv[k].cpu().numpy()), k
