@@ -439,15 +439,10 @@ struct Solver {
       double2* GN0 = tmp(T_F1);
       gemm_store(tmp(T_Q1), false, G00, false, GN0, tk.GRi1 ? wblk(tk.GRi1, l) : nullptr);  // G_{l,l+1}
       gemm_store(GN0, false, Hb, false, tmp(T_R5));                  // GN0 H10
-      {
-        double2* ld = tk.ldos ? wblk(tk.ldos, l) : nullptr;
-        gemm(tmp(T_R5), false, gl, false, [&](int i, int j, double2 v) {
-          const int idx = i + j * nn;
-          const double2 w = cadd(gl[idx], v);                         // G_ll = Gl + C
-          G00n[idx] = w;
-          if (ld) ld[idx] = w;
-        });
-      }
+      gemm(tmp(T_R5), false, gl, false, [&](int i, int j, double2 v) {
+        const int idx = i + j * nn;
+        G00n[idx] = cadd(gl[idx], v);                                 // G_ll = Gl + C
+      });
       gemm_store(tmp(T_Q2), false, Hb, false, tmp(T_R7));           // Gl H10^H G< H10
       gemm(tmp(T_R7), false, gl, true, [&](int i, int j, double2 v) {
         const int idx = i + j * nn;
@@ -457,16 +452,24 @@ struct Solver {
         const int idx = i + j * nn;
         Gnn[idx] = cadd(Gnn[idx], v);                               // Gn += GN0 H10 Gl<
       });
+      gemm(tmp(T_Q3), false, GN0, true, [&](int i, int j, double2 v) {
+        const int idx = i + j * nn;
+        Gnn[idx] = cadd(Gnn[idx], v);                               // Gn += Gl< H10^H GN0^H
+      });
       {
+        // the block outputs leave in one contiguous pass each (sequential
+        // stores, which matters when they are host memory written through its
+        // device mapping) rather than from the product epilogues
+        double2* ld = tk.ldos ? wblk(tk.ldos, l) : nullptr;
         double2* nd = tk.ndens ? wblk(tk.ndens, l) : nullptr;
         double2* pd = (tk.pdens && !cms) ? wblk(tk.pdens, l) : nullptr;
-        gemm(tmp(T_Q3), false, GN0, true, [&](int i, int j, double2 v) {
-          const int idx = i + j * nn;
-          const double2 w = cadd(Gnn[idx], v);                      // Gn += Gl< H10^H GN0^H
-          Gnn[idx] = w;
-          if (nd) nd[idx] = w;
-          if (pd) pd[idx] = cadd(w, csub(G00n[idx], cconj(G00n[j + i * nn])));
-        });
+        if (ld || nd || pd)
+          for_each_elem(n, [&](int i, int j, int idx) {
+            const double2 g = G00n[idx], w = Gnn[idx];
+            if (ld) ld[idx] = g;
+            if (nd) nd[idx] = w;
+            if (pd) pd[idx] = cadd(w, csub(g, cconj(G00n[j + i * nn])));
+          });
       }
       if (cms && (tk.pdens || tk.GGi1)) {
         // green_RGF_CMS's G^> (:4353-4369) with its never-filled Glp (zero):
