@@ -15,10 +15,12 @@
 // order (P: k then E; S: w then q).  Layout (nm,nm,nx,nen,nk) column-major,
 // k = kz + ky*nkz.
 //
-// Memory pattern: a warp takes 32 consecutive energy offsets w (P) or
-// energies E (S) of one (i, j, ix, k) element, so one operand is the same
-// address across the warp and the other slides along the energy axis --
-// consecutive iterations re-read what the neighbouring lane read, from L1.
+// Memory pattern: when an element's energy series fit in shared memory
+// (6 nen complex values for P, 6 nen nk for S, up to 200 KB) a CTA stages
+// them once and sums from shared memory (the *_staged kernels); otherwise
+// the direct kernels have a warp take 32 consecutive energy offsets w (P) or
+// energies E (S) of one element, so one operand is the same address across
+// the warp and the other slides along the energy axis.
 #include <cstdio>
 
 #include "rgf_device.cuh"
@@ -125,6 +127,138 @@ __global__ void __launch_bounds__(kGWThreads) gw_s_kernel(GWDims d, int imag_onl
   NL[o] = rgf::cmul(al, scale);
   NG[o] = rgf::cmul(ag, scale);
   NR[o] = rgf::cmul(ar, scale);
+}
+
+// Shared-memory staged forms of the two sums, used when the staged energy
+// series fit: a CTA owns one banded element (i, j, ix) and one q (P) or k
+// (Sigma) and all its energy offsets / energies (NPT per thread).  The
+// operands that the direct kernels read scattered along the energy axis are
+// read once per CTA into shared memory; every output keeps the reference's
+// order of summation (P: k, then E; Sigma: w, then q).
+constexpr int kStThreads = 256;
+
+template <int NPT>
+__global__ void __launch_bounds__(kStThreads) gw_p_staged_kernel(GWDims d, int imag_only, double2 scale,
+                                                                  const double2* GL, const double2* GG,
+                                                                  const double2* GR, double2* PL, double2* PG,
+                                                                  double2* PR) {
+  extern __shared__ __align__(16) double2 sh[];
+  const int64_t nen = d.nen;
+  double2 *aL = sh, *aG = sh + nen, *aR = sh + 2 * nen, *bG = sh + 3 * nen, *bL = sh + 4 * nen,
+          *bR = sh + 5 * nen;
+  const int64_t i = blockIdx.x % d.nm, jb = blockIdx.x / d.nm;
+  const int64_t j = i - d.ndiag + jb;
+  if (j < 0 || j >= d.nm) return;                      // uniform over the CTA
+  const int64_t ix = blockIdx.y, iq = blockIdx.z;
+  const int64_t nk = d.nky * d.nkz;
+  double2 al[NPT], ag[NPT], ar[NPT];
+#pragma unroll
+  for (int c = 0; c < NPT; c++) al[c] = ag[c] = ar[c] = rgf::czero();
+  for (int64_t ik = 0; ik < nk; ik++) {
+    const int64_t ikd = d.kd(ik, iq);
+    __syncthreads();
+    for (int64_t e = threadIdx.x; e < nen; e += kStThreads) {
+      const size_t a = d.at(i, j, ix, e, ik), bt = d.at(j, i, ix, e, ikd), b = d.at(i, j, ix, e, ikd);
+      aL[e] = gread(GL, a, imag_only);
+      aG[e] = gread(GG, a, imag_only);
+      aR[e] = gread(GR, a, imag_only);
+      bG[e] = gread(GG, bt, imag_only);
+      bL[e] = gread(GL, bt, imag_only);
+      bR[e] = gread(GR, b, imag_only);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < NPT; c++) {
+      const int64_t nop = -d.nopmax + threadIdx.x + (int64_t)kStThreads * c;
+      if (nop > d.nopmax) continue;
+      const int64_t lo = (nop + 1 > 1 ? nop + 1 : 1) - 1;
+      const int64_t hi = d.nen < d.nen + nop ? d.nen : d.nen + nop;
+      for (int64_t ie = lo; ie < hi; ie++) {
+        const int64_t e2 = ie - nop;
+        const double2 gl = aL[ie], glt = bL[e2];
+        al[c] = cfma(al[c], gl, bG[e2]);
+        ag[c] = cfma(ag[c], aG[ie], glt);
+        ar[c] = rgf::cadd(ar[c], rgf::cadd(rgf::cmul(gl, rgf::cconj(bR[e2])), rgf::cmul(aR[ie], glt)));
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < NPT; c++) {
+    const int64_t nop = -d.nopmax + threadIdx.x + (int64_t)kStThreads * c;
+    if (nop > d.nopmax) continue;
+    const size_t o = d.at(i, j, ix, nop + d.nen / 2 - 1, iq);
+    PL[o] = rgf::cmul(al[c], scale);
+    PG[o] = rgf::cmul(ag[c], scale);
+    PR[o] = rgf::cmul(ar[c], scale);
+  }
+}
+
+template <int NPT>
+__global__ void __launch_bounds__(kStThreads) gw_s_staged_kernel(GWDims d, int imag_only, double2 scale,
+                                                                  const double2* GL, const double2* GG,
+                                                                  const double2* GR, const double2* WL,
+                                                                  const double2* WG, const double2* WR,
+                                                                  double2* NL, double2* NG, double2* NR) {
+  extern __shared__ __align__(16) double2 sh[];
+  const int64_t nen = d.nen, nk = d.nky * d.nkz, ne = nen * nk;
+  double2 *gL = sh, *gG = sh + ne, *gR = sh + 2 * ne, *wL = sh + 3 * ne, *wG = sh + 4 * ne, *wR = sh + 5 * ne;
+  const int64_t i = blockIdx.x % d.nm, jb = blockIdx.x / d.nm;
+  const int64_t j = i - d.ndiag + jb;
+  if (j < 0 || j >= d.nm) return;
+  const int64_t ix = blockIdx.y, ik = blockIdx.z;
+  // g(e, q) = G(i,j,ix,e,k-q), w(e, q) = W(i,j,ix,e,q) for every q
+  for (int64_t t = threadIdx.x; t < ne; t += kStThreads) {
+    const int64_t e = t % nen, iq = t / nen;
+    const size_t g = d.at(i, j, ix, e, d.kd(ik, iq)), w = d.at(i, j, ix, e, iq);
+    gL[t] = gread(GL, g, imag_only);
+    gG[t] = gread(GG, g, imag_only);
+    gR[t] = gread(GR, g, imag_only);
+    wL[t] = WL[w];
+    wG[t] = WG[w];
+    wR[t] = WR[w];
+  }
+  __syncthreads();
+  double2 al[NPT], ag[NPT], ar[NPT];
+#pragma unroll
+  for (int c = 0; c < NPT; c++) al[c] = ag[c] = ar[c] = rgf::czero();
+  for (int64_t nop = -d.nopmax; nop <= d.nopmax; nop++) {
+    const int64_t iop = nop + nen / 2 - 1;
+    for (int64_t iq = 0; iq < nk; iq++) {
+      const double2 wl = wL[iop + nen * iq], wg = wG[iop + nen * iq], wr = wR[iop + nen * iq];
+#pragma unroll
+      for (int c = 0; c < NPT; c++) {
+        const int64_t ie1 = 1 + threadIdx.x + (int64_t)kStThreads * c;
+        if (ie1 > nen || !(ie1 > (nop > 1 ? nop : 1) && ie1 < nen + nop)) continue;
+        const int64_t g = ie1 - nop - 1 + nen * iq;
+        const double2 gl = gL[g], gr = gR[g];
+        al[c] = cfma(al[c], gl, wl);
+        ag[c] = cfma(ag[c], gG[g], wg);
+        ar[c] = rgf::cadd(ar[c], rgf::cadd(rgf::cadd(rgf::cmul(gl, wr), rgf::cmul(gr, wl)), rgf::cmul(gr, wr)));
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < NPT; c++) {
+    const int64_t ie1 = 1 + threadIdx.x + (int64_t)kStThreads * c;
+    if (ie1 > nen) continue;
+    const size_t o = d.at(i, j, ix, ie1 - 1, ik);
+    NL[o] = rgf::cmul(al[c], scale);
+    NG[o] = rgf::cmul(ag[c], scale);
+    NR[o] = rgf::cmul(ar[c], scale);
+  }
+}
+
+constexpr size_t kGWStagedSmemMax = 200 * 1024;
+
+// Launch a staged kernel with NPT = the smallest of 1, 2, 4, 8 covering
+// `count` values per CTA; false if none fits (the caller then uses the
+// direct kernel).
+template <class L1, class L2, class L4, class L8>
+bool launch_npt(int64_t count, size_t smem, L1 l1, L2 l2, L4 l4, L8 l8) {
+  if (smem > kGWStagedSmemMax) return false;
+  const int64_t npt = (count + kStThreads - 1) / kStThreads;
+  if (npt <= 1) l1(); else if (npt <= 2) l2(); else if (npt <= 4) l4(); else if (npt <= 8) l8(); else return false;
+  return true;
 }
 
 // Sigma^R imaginary part from Sigma^> - Sigma^<, symmetrisation and mixing
@@ -238,11 +372,22 @@ extern "C" int rgf_gw_polarization(rgf_ctx* ctx, int64_t nm, int64_t nx, int64_t
   GWDims d{nm, nx, nen, nky, nkz, ndiag, nen / 2 - 10};
   if (d.nopmax >= 0) {
     const double2 scale = make_double2(0.0, -1.0 * dE / 2.0 / kPiGW * spindeg / (double)nk);
-    dim3 grid((unsigned)((2 * d.nopmax + 1 + kGWThreads - 1) / kGWThreads), (unsigned)(nm * (2 * ndiag + 1)),
-              (unsigned)(nx * nk));
-    gw_p_kernel<<<grid, kGWThreads, 0, st>>>(d, imag_only, scale, (const double2*)gl.dev,
-                                             (const double2*)gg.dev, (const double2*)gr.dev,
-                                             (double2*)pl.dev, (double2*)pg.dev, (double2*)pr.dev);
+    const double2 *a = (const double2*)gl.dev, *b = (const double2*)gg.dev, *c = (const double2*)gr.dev;
+    double2 *o1 = (double2*)pl.dev, *o2 = (double2*)pg.dev, *o3 = (double2*)pr.dev;
+    const dim3 sgrid((unsigned)(nm * (2 * ndiag + 1)), (unsigned)nx, (unsigned)nk);
+    const size_t smem = 6 * sizeof(double2) * (size_t)nen;
+    auto go = [&](auto kern) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      kern<<<sgrid, kStThreads, smem, st>>>(d, imag_only, scale, a, b, c, o1, o2, o3);
+    };
+    const bool staged = launch_npt(
+        2 * d.nopmax + 1, smem, [&] { go(gw_p_staged_kernel<1>); }, [&] { go(gw_p_staged_kernel<2>); },
+        [&] { go(gw_p_staged_kernel<4>); }, [&] { go(gw_p_staged_kernel<8>); });
+    if (!staged) {
+      dim3 grid((unsigned)((2 * d.nopmax + 1 + kGWThreads - 1) / kGWThreads), (unsigned)(nm * (2 * ndiag + 1)),
+                (unsigned)(nx * nk));
+      gw_p_kernel<<<grid, kGWThreads, 0, st>>>(d, imag_only, scale, a, b, c, o1, o2, o3);
+    }
   }
   e = cudaGetLastError();
   for (View* v : {&pl, &pg, &pr})
@@ -287,12 +432,22 @@ extern "C" int rgf_gw_self_energy(rgf_ctx* ctx, int64_t nm, int64_t nx, int64_t 
   GWDims d{nm, nx, nen, nky, nkz, ndiag, nen / 2 - 10};
   if (d.nopmax >= 0) {
     const double2 scale = make_double2(0.0, dE / 2.0 / kPiGW / (double)nk);
-    dim3 grid((unsigned)((nen + kGWThreads - 1) / kGWThreads), (unsigned)(nm * (2 * ndiag + 1)),
-              (unsigned)(nx * nk));
-    gw_s_kernel<<<grid, kGWThreads, 0, st>>>(d, imag_only, scale, (const double2*)gl.dev,
-                                             (const double2*)gg.dev, (const double2*)gr.dev,
-                                             (const double2*)wl.dev, (const double2*)wg.dev,
-                                             (const double2*)wr.dev, NL, NG, NR);
+    const double2 *a = (const double2*)gl.dev, *b = (const double2*)gg.dev, *c = (const double2*)gr.dev;
+    const double2 *w1 = (const double2*)wl.dev, *w2 = (const double2*)wg.dev, *w3 = (const double2*)wr.dev;
+    const dim3 sgrid((unsigned)(nm * (2 * ndiag + 1)), (unsigned)nx, (unsigned)nk);
+    const size_t smem = 6 * sizeof(double2) * (size_t)nen * (size_t)nk;
+    auto go = [&](auto kern) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      kern<<<sgrid, kStThreads, smem, st>>>(d, imag_only, scale, a, b, c, w1, w2, w3, NL, NG, NR);
+    };
+    const bool staged = launch_npt(
+        nen, smem, [&] { go(gw_s_staged_kernel<1>); }, [&] { go(gw_s_staged_kernel<2>); },
+        [&] { go(gw_s_staged_kernel<4>); }, [&] { go(gw_s_staged_kernel<8>); });
+    if (!staged) {
+      dim3 grid((unsigned)((nen + kGWThreads - 1) / kGWThreads), (unsigned)(nm * (2 * ndiag + 1)),
+                (unsigned)(nx * nk));
+      gw_s_kernel<<<grid, kGWThreads, 0, st>>>(d, imag_only, scale, a, b, c, w1, w2, w3, NL, NG, NR);
+    }
   }
   const int tpb = 256;
   gw_s_post_kernel<<<(unsigned)((nel + tpb - 1) / tpb), tpb, 0, st>>>(

@@ -27,8 +27,11 @@ def _arrays(rng, nk, nen, nx, nm, n):
             for _ in range(n)]
 
 
+# the last case is too long in energy for the shared-memory staged kernels
+# (the direct kernels run)
 @pytest.mark.parametrize("nky,nkz,ndiag,nm,nx,nen,imag", [(1, 1, 0, 6, 3, 40, True), (2, 2, 2, 8, 4, 48, True),
-                                                       (1, 3, 1, 5, 3, 64, False), (3, 1, 8, 8, 5, 33, True)])
+                                                       (1, 3, 1, 5, 3, 64, False), (3, 1, 8, 8, 5, 33, True),
+                                                       (1, 1, 0, 2, 3, 2200, True)])
 def test_gw_polarization_matches_oracle(rgf, nky, nkz, ndiag, nm, nx, nen, imag):
     from oracle import oracle as O
     rng = np.random.default_rng(nm * nen)
@@ -44,7 +47,8 @@ def test_gw_polarization_matches_oracle(rgf, nky, nkz, ndiag, nm, nx, nen, imag)
         assert np.array_equal(g == 0, r == 0)   # band and window structure
 
 
-@pytest.mark.parametrize("nky,nkz,ndiag,nm,nx,nen", [(1, 2, 1, 6, 6, 40), (2, 1, 3, 5, 4, 36), (1, 1, 0, 4, 3, 30)])
+@pytest.mark.parametrize("nky,nkz,ndiag,nm,nx,nen", [(1, 2, 1, 6, 6, 40), (2, 1, 3, 5, 4, 36), (1, 1, 0, 4, 3, 30),
+                                                  (1, 1, 0, 2, 3, 2200)])
 def test_gw_self_energy_matches_oracle(rgf, nky, nkz, ndiag, nm, nx, nen):
     from oracle import oracle as O
     rng = np.random.default_rng(nx * 100 + nen)
