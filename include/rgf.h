@@ -439,6 +439,23 @@ RGF_API int rgf_write_transmission_spectrum(const char* dataset, int32_t iter, c
 RGF_API int rgf_write_id_iteration(const char* path, int32_t iter, double current_left, double current_right);
 RGF_API const char* rgf_io_last_error(void);
 
+/* Reader of the Wannier Hamiltonian file (w90_load_from_file,
+ * src/wannierHam.f90:68-130): nvb and spin degeneracy, the three cell vectors,
+ * n entries (x, y, z cell offsets, orbital m, orbital n, Re H, Im H) read as
+ * Fortran list-directed input; with axis (3 values, 1-based, or NULL) the cell
+ * vectors and the first three columns are permuted as the reference's
+ * lreorder_axis does.  info receives the dimensions (nb, nx, ny, x/y ranges)
+ * and the derived Lx, Ly, Lz, b1, b2; Hr (NULL: dimensions only) receives
+ * Hr(nb,nb,nx,ny), complex(8) column-major, zero where the file has no entry.
+ * Host-only. */
+typedef struct rgf_ham_info {
+  int32_t nvb, spin_deg, nb, nx, ny, xmin, xmax, ymin, ymax, n_entries;
+  double cell[9];          /* (alpha, beta, gamm) as columns, Angstrom */
+  double Lx, Ly, Lz;
+  double b1[3], b2[3];
+} rgf_ham_info;
+RGF_API int rgf_read_ham_dat(const char* path, const int32_t* axis, rgf_ham_info* info, rgf_c16* Hr);
+
 /* Last error message of the calling thread ("" if none). */
 RGF_API const char* rgf_last_error(void);
 

@@ -10,8 +10,10 @@
 // dataset // STRING(i) // '.dat' with STRING the reference's 4-digit
 // zero-padded number (green.f90:3174-3188), or dataset // '_' // STRING(i)
 // for the writers that insert the underscore.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -308,5 +310,172 @@ extern "C" int rgf_write_id_iteration(const char* path, int32_t iter, double cur
   std::fprintf(f, "%s%s%s\n", fortran_I(iter, 4).c_str(), fortran_E(current_left, 16, 6).c_str(),
                fortran_E(current_right, 16, 6).c_str());
   std::fclose(f);
+  return RGF_OK;
+}
+
+// ------------------------------------------------------------ ham_dat reader
+// w90_load_from_file (src/wannierHam.f90:68-130): the Wannier Hamiltonian
+// file the drivers read.  Fortran list-directed input: each READ starts at a
+// new record and takes as many values as it needs, continuing over records;
+// values are separated by blanks or commas.  A `comment` read takes one
+// value and skips the rest of its record.
+namespace {
+
+struct FortranListReader {
+  std::vector<std::string> records;
+  size_t rec = 0;
+  std::vector<std::string> pending;  // values left in the current record
+  bool open(const char* path) {
+    FILE* f = std::fopen(path, "r");
+    if (!f) return false;
+    char buf[4096];
+    std::string line;
+    while (std::fgets(buf, sizeof(buf), f)) {
+      line += buf;
+      if (!line.empty() && line.back() == '\n') {
+        records.push_back(line);
+        line.clear();
+      }
+    }
+    if (!line.empty()) records.push_back(line);
+    std::fclose(f);
+    return true;
+  }
+  static std::vector<std::string> split(const std::string& s) {
+    std::vector<std::string> v;
+    std::string cur;
+    for (char c : s) {
+      if (c == ' ' || c == '\t' || c == ',' || c == '\n' || c == '\r') {
+        if (!cur.empty()) { v.push_back(cur); cur.clear(); }
+      } else {
+        cur += c;
+      }
+    }
+    if (!cur.empty()) v.push_back(cur);
+    return v;
+  }
+  // one READ statement of n values
+  bool read(size_t n, std::vector<std::string>& out) {
+    out.clear();
+    pending.clear();
+    while (out.size() < n) {
+      if (pending.empty()) {
+        if (rec >= records.size()) return false;
+        pending = split(records[rec++]);
+        std::reverse(pending.begin(), pending.end());
+        continue;
+      }
+      out.push_back(pending.back());
+      pending.pop_back();
+    }
+    return true;
+  }
+};
+
+double fortran_real(const std::string& s) {
+  std::string t = s;
+  for (char& c : t)
+    if (c == 'd' || c == 'D') c = 'e';   // Fortran double-precision exponent letter
+  return std::strtod(t.c_str(), nullptr);
+}
+
+}  // namespace
+
+extern "C" int rgf_read_ham_dat(const char* path, const int32_t* axis, rgf_ham_info* info, rgf_c16* Hr) {
+  if (!path || !info) return io_fail(RGF_E_ARG, "invalid argument");
+  FortranListReader rd;
+  if (!rd.open(path)) return io_fail(RGF_E_ARG, "cannot open the Hamiltonian file");
+  std::vector<std::string> v;
+  auto bad = [&]() { return io_fail(RGF_E_ARG, "malformed Hamiltonian file"); };
+  if (!rd.read(2, v)) return bad();
+  std::memset(info, 0, sizeof(*info));
+  info->nvb = (int32_t)std::atol(v[0].c_str());
+  info->spin_deg = (int32_t)std::atol(v[1].c_str());
+  if (!rd.read(1, v)) return bad();  // comment
+  double cell[3][3];                 // cell[c] = alpha, beta, gamm
+  for (int c = 0; c < 3; c++) {
+    if (!rd.read(3, v)) return bad();
+    for (int k = 0; k < 3; k++) cell[c][k] = fortran_real(v[k]);
+  }
+  if (!rd.read(1, v)) return bad();  // comment
+  if (axis) {                        // cell(:,:) = cell(:,axis)
+    double c2[3][3];
+    for (int c = 0; c < 3; c++) {
+      if (axis[c] < 1 || axis[c] > 3) return io_fail(RGF_E_ARG, "axis must be a permutation of 1, 2, 3");
+      for (int k = 0; k < 3; k++) c2[c][k] = cell[axis[c] - 1][k];
+    }
+    std::memcpy(cell, c2, sizeof(cell));
+  }
+  if (!rd.read(1, v)) return bad();
+  const long n = std::atol(v[0].c_str());
+  if (n < 1) return bad();
+  std::vector<double> ham((size_t)n * 7);
+  for (long i = 0; i < n; i++) {
+    if (!rd.read(7, v)) return bad();
+    double row[7];
+    for (int k = 0; k < 7; k++) row[k] = fortran_real(v[k]);
+    if (axis) {  // ham(:,1:3) = ham(:,axis)
+      double r3[3] = {row[axis[0] - 1], row[axis[1] - 1], row[axis[2] - 1]};
+      for (int k = 0; k < 3; k++) row[k] = r3[k];
+    }
+    for (int k = 0; k < 7; k++) ham[(size_t)i * 7 + k] = row[k];
+  }
+  // integer assignments of reals truncate toward zero, as in the reference
+  double mnx = ham[0], mxx = ham[0], mny = ham[1], mxy = ham[1], mxb = ham[3];
+  for (long i = 0; i < n; i++) {
+    const double* r = &ham[(size_t)i * 7];
+    mnx = std::min(mnx, r[0]);
+    mxx = std::max(mxx, r[0]);
+    mny = std::min(mny, r[1]);
+    mxy = std::max(mxy, r[1]);
+    mxb = std::max(mxb, r[3]);
+  }
+  info->xmin = (int32_t)mnx;
+  info->xmax = (int32_t)mxx;
+  info->ymin = (int32_t)mny;
+  info->ymax = (int32_t)mxy;
+  info->nb = (int32_t)mxb;
+  info->nx = info->xmax - info->xmin + 1;
+  info->ny = info->ymax - info->ymin + 1;
+  info->n_entries = (int32_t)n;
+  for (int c = 0; c < 3; c++)
+    for (int k = 0; k < 3; k++) info->cell[k + 3 * c] = cell[c][k];
+  auto dot = [](const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+  auto cross = [](const double* a, const double* b, double* o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+  };
+  const double *alpha = cell[0], *beta = cell[1], *gamm = cell[2];
+  const double na = std::sqrt(dot(alpha, alpha));
+  double xhat[3] = {alpha[0] / na, alpha[1] / na, alpha[2] / na}, yhat[3];
+  cross(xhat, gamm, yhat);
+  for (double& y : yhat) y = -y;
+  const double ny_ = std::sqrt(dot(yhat, yhat));
+  for (double& y : yhat) y = y / ny_;
+  info->Ly = std::fabs(dot(beta, yhat));
+  info->Lx = std::fabs(dot(alpha, xhat));
+  info->Lz = std::sqrt(dot(gamm, gamm));
+  double t[3];
+  cross(beta, gamm, t);
+  const double d1 = dot(alpha, t);
+  for (int k = 0; k < 3; k++) info->b1[k] = t[k] / d1;
+  cross(gamm, alpha, t);
+  const double d2 = dot(beta, t);
+  for (int k = 0; k < 3; k++) info->b2[k] = t[k] / d2;
+  if (Hr) {
+    const int64_t nb = info->nb, nx = info->nx, ny = info->ny;
+    std::memset(Hr, 0, sizeof(rgf_c16) * (size_t)nb * nb * nx * ny);
+    for (long i = 0; i < n; i++) {
+      const double* r = &ham[(size_t)i * 7];
+      const int64_t a = (int64_t)std::floor(r[3]) - 1, b = (int64_t)std::floor(r[4]) - 1;
+      const int64_t x = (int64_t)std::floor(r[0]) - info->xmin, y = (int64_t)std::floor(r[1]) - info->ymin;
+      if (a < 0 || a >= nb || b < 0 || b >= nb || x < 0 || x >= nx || y < 0 || y >= ny)
+        return io_fail(RGF_E_ARG, "orbital or cell index out of range in the Hamiltonian file");
+      rgf_c16& h = Hr[a + nb * (b + nb * (x + nx * y))];
+      h.re = r[5];
+      h.im = r[6];
+    }
+  }
   return RGF_OK;
 }

@@ -52,7 +52,7 @@ EXPORTS = (
     "rgf_gw_polarization", "rgf_gw_self_energy", "rgf_gw_last_error", "rgf_permute_c16",
     "rgf_permute_last_error", "rgf_write_spectrum", "rgf_write_dos", "rgf_write_current_spectrum",
     "rgf_write_current_summed_over_k", "rgf_write_transmission_spectrum", "rgf_write_id_iteration",
-    "rgf_io_last_error",
+    "rgf_io_last_error", "rgf_read_ham_dat",
 )
 
 # kernel variant ids (rgf_variant_name)
@@ -105,6 +105,13 @@ class c_w_task(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("reserved", ctypes.c_int32), ("PL", ctypes.c_void_p),
                 ("PG", ctypes.c_void_p), ("PR", ctypes.c_void_p), ("WL", ctypes.c_void_p),
                 ("WG", ctypes.c_void_p), ("WR", ctypes.c_void_p), ("WRi1", ctypes.c_void_p)]
+
+
+class c_ham_info(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int32) for k in ("nvb", "spin_deg", "nb", "nx", "ny", "xmin", "xmax", "ymin", "ymax",
+                                               "n_entries")] + \
+               [("cell", ctypes.c_double * 9), ("Lx", ctypes.c_double), ("Ly", ctypes.c_double),
+                ("Lz", ctypes.c_double), ("b1", ctypes.c_double * 3), ("b2", ctypes.c_double * 3)]
 
 
 class c_stats(ctypes.Structure):
@@ -175,6 +182,8 @@ def load(path: str = LIB_PATH):
                  "rgf_write_current_summed_over_k", "rgf_write_transmission_spectrum", "rgf_write_id_iteration"):
         getattr(L, name).restype = ctypes.c_int
     L.rgf_io_last_error.restype = ctypes.c_char_p
+    L.rgf_read_ham_dat.argtypes = [S, P, P, P]
+    L.rgf_read_ham_dat.restype = ctypes.c_int
     L.rgf_solve_energies.argtypes = [P, ctypes.POINTER(c_device), ctypes.c_int64] + [P] * 13
     L.rgf_terminal_current.argtypes = [P, P, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_int64, P]

@@ -54,3 +54,19 @@ def write_transmission_spectrum(dataset, i, tr, en, nk=0, append=False):
 
 def write_id_iteration(path, it, current_left, current_right):
     _chk(R.load().rgf_write_id_iteration(path.encode(), int(it), float(current_left), float(current_right)))
+
+
+def read_ham_dat(path, axis=None):
+    """w90_load_from_file (src/wannierHam.f90:68-130).  Returns (info dict,
+    Hr) with Hr the NumPy view (ny, nx, nb, nb) of Hr(nb,nb,nx,ny)."""
+    L = R.load()
+    info = R.c_ham_info()
+    ax = None if axis is None else (R.ctypes.c_int32 * 3)(*[int(a) for a in axis])
+    axp = None if ax is None else R.ctypes.addressof(ax)
+    _chk(L.rgf_read_ham_dat(path.encode(), axp, R.ctypes.byref(info), None))
+    Hr = np.zeros((info.ny, info.nx, info.nb, info.nb), np.complex128)
+    _chk(L.rgf_read_ham_dat(path.encode(), axp, R.ctypes.byref(info), Hr.ctypes.data))
+    d = {k: getattr(info, k) for k, _ in R.c_ham_info._fields_ if k not in ("cell", "b1", "b2")}
+    d["cell"] = np.array(info.cell[:]).reshape(3, 3)   # rows: alpha, beta, gamm
+    d["b1"], d["b2"] = np.array(info.b1[:]), np.array(info.b2[:])
+    return d, Hr
