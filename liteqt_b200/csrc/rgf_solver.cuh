@@ -46,6 +46,7 @@ enum TmpBlock {
   T_G00B, T_GNA, T_GNB, T_Q1, T_Q2, T_Q3, T_Q4, T_R5, T_INV, T_RT,
   T_SRS, T_SLS,  // green_RGF_CMS: sigma_r_ph S_ll, sigma_lesser_ph S_ll of the current block
   T_COUNT,
+  T_X3 = T_SLS,  // backward sweep (T_SLS is only live before it)
   // aliases (lifetimes do not overlap)
   T_R7 = T_F4, T_P1 = T_F1, T_P2 = T_F2, T_P3 = T_F3, T_P4 = T_SIG,
   T_GPN = T_SB, T_X1 = T_SA, T_X2 = T_H10A, T_Y = T_H10B, T_Z = T_H01A,
@@ -395,6 +396,9 @@ struct Solver {
     const bool need_q4 = need_cur || tk.GLi1 != nullptr;
     const bool need_back = tk.ldos || tk.ndens || tk.pdens || tk.GRi1 || tk.GLi1 || tk.GGi1 ||
                            tk.cur || tk.tre;
+    // no scattering Sigma^<: every Gl< is anti-Hermitian by construction
+    // (g Sigma^<_lead g^H and g H Gl< H^H g^H with anti-Hermitian factors)
+    const bool ballistic = sl == nullptr;
     if (need_cur)
       for_each_elem(n, [&](int, int, int idx) { blk2(tk.cur, nx - 1)[idx] = 0.0; });
     for (int l = need_back ? nx - 2 : -1; l >= 0; l--) {
@@ -416,7 +420,8 @@ struct Solver {
       }
       gemm_store(gl, false, Hb, true, tmp(T_Q1));                   // Gl H10^H
       gemm_store(tmp(T_Q1), false, Gn, false, tmp(T_Q2));           // Gl H10^H G<
-      gemm_store(gln, false, Hb, true, tmp(T_Q3));                  // Gl< H10^H
+      if (!ballistic || need_q4)
+        gemm_store(gln, false, Hb, true, tmp(T_Q3));                // Gl< H10^H
       if (need_q4) {
         double2* gli = tk.GLi1 ? wblk(tk.GLi1, l) : nullptr;
         gemm(tmp(T_Q3), false, G00, true, [&](int i, int j, double2 v) {
@@ -448,28 +453,42 @@ struct Solver {
         const int idx = i + j * nn;
         Gnn[idx] = cadd(gln[idx], v);                               // Gn = Gl< + C
       });
-      gemm(tmp(T_R5), false, gln, false, [&](int i, int j, double2 v) {
-        const int idx = i + j * nn;
-        Gnn[idx] = cadd(Gnn[idx], v);                               // Gn += GN0 H10 Gl<
-      });
-      gemm(tmp(T_Q3), false, GN0, true, [&](int i, int j, double2 v) {
-        const int idx = i + j * nn;
-        Gnn[idx] = cadd(Gnn[idx], v);                               // Gn += Gl< H10^H GN0^H
-      });
+      double2* T3 = tmp(T_X3);
+      if (ballistic) {
+        gemm_store(tmp(T_R5), false, gln, false, T3);                // GN0 H10 Gl<
+      } else {
+        gemm(tmp(T_R5), false, gln, false, [&](int i, int j, double2 v) {
+          const int idx = i + j * nn;
+          Gnn[idx] = cadd(Gnn[idx], v);                             // Gn += GN0 H10 Gl<
+        });
+        gemm(tmp(T_Q3), false, GN0, true, [&](int i, int j, double2 v) {
+          const int idx = i + j * nn;
+          Gnn[idx] = cadd(Gnn[idx], v);                             // Gn += Gl< H10^H GN0^H
+        });
+      }
       {
-        // the block outputs leave in one contiguous pass each (sequential
+        // Ballistic: the last term Gl< H10^H GN0^H is -(GN0 H10 Gl<)^H, since
+        // every Gl< is anti-Hermitian when no scattering Sigma^< enters.
+        // The block outputs leave in one contiguous pass each (sequential
         // stores, which matters when they are host memory written through its
-        // device mapping) rather than from the product epilogues
+        // device mapping) rather than from the product epilogues.
         double2* ld = tk.ldos ? wblk(tk.ldos, l) : nullptr;
         double2* nd = tk.ndens ? wblk(tk.ndens, l) : nullptr;
         double2* pd = (tk.pdens && !cms) ? wblk(tk.pdens, l) : nullptr;
-        if (ld || nd || pd)
+        if (ballistic || ld || nd || pd) {
           for_each_elem(n, [&](int i, int j, int idx) {
-            const double2 g = G00n[idx], w = Gnn[idx];
+            const double2 g = G00n[idx];
+            double2 w = Gnn[idx];
+            if (ballistic) {
+              w = cadd(w, csub(T3[idx], cconj(T3[j + i * nn])));
+              Gnn[idx] = w;
+            }
             if (ld) ld[idx] = g;
             if (nd) nd[idx] = w;
             if (pd) pd[idx] = cadd(w, csub(g, cconj(G00n[j + i * nn])));
           });
+          __syncthreads();
+        }
       }
       if (cms && (tk.pdens || tk.GGi1)) {
         // green_RGF_CMS's G^> (:4353-4369) with its never-filled Glp (zero):
