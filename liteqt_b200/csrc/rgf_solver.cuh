@@ -20,6 +20,9 @@
 //   - products the reference forms twice are formed once (17 complex
 //     products per backward block instead of 22; 10 when neither `cur` nor
 //     GLi1 is requested);
+//   - without scattering Sigma^<, g^<_l = g^L_{l,1} Sigma^<_L g^L_{l,1}^H
+//     from the running column (2 products per forward block instead of 4)
+//     and the last backward G^< term is the conjugate transpose of another;
 //   - sums, z*I - H - Sigma assembly, Fermi-weighted Sigma^< and the
 //     G^> = G^< + G^R - G^A identity are fused into the product epilogues;
 //   - the traces tr / tre / T form only the diagonal of the final product;
@@ -221,6 +224,7 @@ struct Solver {
     const double2* H1i = dv.H1i;
     const double2* sl = tk.sig_lesser;
     const double2* sr = tk.sig_r;
+    const bool ballistic = sl == nullptr;                          // no scattering Sigma^<
     auto blk = [&](const double2* base, int l) { return base + (size_t)l * n2; };
     auto wblk = [&](double2* base, int l) { return base + (size_t)l * n2; };
     const bool want_T = o.want_T && tk.T;
@@ -286,18 +290,27 @@ struct Solver {
         X[idx] = csub(zs_minus(z, Sl, i, j, idx, h), v);
       });
       invert_X(Gl(l));
-      gemm_store(H, false, Gln(l - 1), false, tmp(T_F2));           // B = H10 Gln(l-1)
-      gemm(tmp(T_F2), false, H, true, [&](int i, int j, double2 v) { // C = B H10^H + sig<
-        const int idx = i + j * nn;
-        tmp(T_F3)[idx] = sll ? cadd(v, sll[idx]) : v;
-      });
-      gemm_store(Gl(l), false, tmp(T_F3), false, tmp(T_F4));        // B = A C
-      gemm_store(tmp(T_F4), false, Gl(l), true, Gln(l));            // Gln(l) = B A^H
-      if (want_T) {                                                 // g^L_{l,1} = g_l H_{l,l-1} g^L_{l-1,1}
+      if (want_T || ballistic) {                                    // g^L_{l,1} = g_l H_{l,l-1} g^L_{l-1,1}
         gemm_store(H, false, GN1, false, tmp(T_F1));
         gemm_store(Gl(l), false, tmp(T_F1), false, GN1buf[gsel]);
         GN1 = GN1buf[gsel];
         gsel ^= 1;
+      }
+      if (ballistic) {
+        // Without scattering the recursion g<_l = g_l H g<_{l-1} H^H g_l^H
+        // unrolls to g<_l = g^L_{l,1} sig<_L (g^L_{l,1})^H: two products on
+        // the running column instead of four (sig<_L stays in T_SIG until
+        // the right contact).
+        gemm_store(GN1, false, tmp(T_SIG), false, tmp(T_F2));        // B = g^L_{l,1} sig<_L
+        gemm_store(tmp(T_F2), false, GN1, true, Gln(l));             // Gln(l) = B g^L_{l,1}^H
+      } else {
+        gemm_store(H, false, Gln(l - 1), false, tmp(T_F2));         // B = H10 Gln(l-1)
+        gemm(tmp(T_F2), false, H, true, [&](int i, int j, double2 v) { // C = B H10^H + sig<
+          const int idx = i + j * nn;
+          tmp(T_F3)[idx] = sll ? cadd(v, sll[idx]) : v;
+        });
+        gemm_store(Gl(l), false, tmp(T_F3), false, tmp(T_F4));      // B = A C
+        gemm_store(tmp(T_F4), false, Gl(l), true, Gln(l));          // Gln(l) = B A^H
       }
     }
 
@@ -398,7 +411,6 @@ struct Solver {
                            tk.cur || tk.tre;
     // no scattering Sigma^<: every Gl< is anti-Hermitian by construction
     // (g Sigma^<_lead g^H and g H Gl< H^H g^H with anti-Hermitian factors)
-    const bool ballistic = sl == nullptr;
     if (need_cur)
       for_each_elem(n, [&](int, int, int idx) { blk2(tk.cur, nx - 1)[idx] = 0.0; });
     for (int l = need_back ? nx - 2 : -1; l >= 0; l--) {
