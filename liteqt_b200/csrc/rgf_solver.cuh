@@ -17,9 +17,10 @@
 //               from a running left-connected column g^L_{l,1}.
 //
 // Differences in *how* (not what) it is computed:
-//   - products the reference forms twice are formed once (17 complex
-//     products per backward block instead of 22; 10 when neither `cur` nor
-//     GLi1 is requested);
+//   - products the reference forms twice are formed once, and the
+//     reference's H10 Gl^H and (Gl H10^H G< H10) Gl^H reuse Gl H10^H
+//     (15 complex products per backward block instead of 22; 9 when
+//     neither `cur` nor GLi1 is requested);
 //   - without scattering Sigma^<, g^<_l = g^L_{l,1} Sigma^<_L g^L_{l,1}^H
 //     from the running column (2 products per forward block instead of 4)
 //     and the last backward G^< term is the conjugate transpose of another;
@@ -51,7 +52,7 @@ enum TmpBlock {
   T_COUNT,
   T_X3 = T_SLS,  // backward sweep (T_SLS is only live before it)
   // aliases (lifetimes do not overlap)
-  T_R7 = T_F4, T_P1 = T_F1, T_P2 = T_F2, T_P3 = T_F3, T_P4 = T_SIG,
+  T_P2 = T_F2, T_P3 = T_F3, T_P4 = T_SIG,
   T_GPN = T_SB, T_X1 = T_SA, T_X2 = T_H10A, T_Y = T_H10B, T_Z = T_H01A,
   T_GAML = T_H01B, T_GAMR = T_HSS, T_R1 = T_GS,
 };
@@ -418,9 +419,9 @@ struct Solver {
       const double2* gl = Gl(l);
       const double2* gln = Gln(l);
       double* curl = need_cur ? blk2(tk.cur, l) : nullptr;
+      gemm_store(gl, false, Hb, true, tmp(T_Q1));                   // Gl H10^H
       if (need_cur) {
-        gemm_store(Hb, false, gl, true, tmp(T_P1));                 // H10 Gl^H
-        gemm_store(Gn, false, tmp(T_P1), false, tmp(T_P2));         // G<_{l+1} H10 Gl^H
+        gemm_store(Gn, false, tmp(T_Q1), true, tmp(T_P2));          // G<_{l+1} H10 Gl^H = G<_{l+1} Q1^H
         gemm_store(Hb, false, gln, false, tmp(T_P3));               // H10 Gl<
         gemm(G00, false, tmp(T_P3), false, [&](int i, int j, double2 v) {
           const int idx = i + j * nn;
@@ -430,7 +431,6 @@ struct Solver {
           curl[i + j * nn] = v.x;
         });
       }
-      gemm_store(gl, false, Hb, true, tmp(T_Q1));                   // Gl H10^H
       gemm_store(tmp(T_Q1), false, Gn, false, tmp(T_Q2));           // Gl H10^H G<
       if (!ballistic || need_q4)
         gemm_store(gln, false, Hb, true, tmp(T_Q3));                // Gl< H10^H
@@ -460,10 +460,9 @@ struct Solver {
         const int idx = i + j * nn;
         G00n[idx] = cadd(gl[idx], v);                                 // G_ll = Gl + C
       });
-      gemm_store(tmp(T_Q2), false, Hb, false, tmp(T_R7));           // Gl H10^H G< H10
-      gemm(tmp(T_R7), false, gl, true, [&](int i, int j, double2 v) {
+      gemm(tmp(T_Q2), false, tmp(T_Q1), true, [&](int i, int j, double2 v) {
         const int idx = i + j * nn;
-        Gnn[idx] = cadd(gln[idx], v);                               // Gn = Gl< + C
+        Gnn[idx] = cadd(gln[idx], v);                               // Gn = Gl< + Gl H10^H G< H10 Gl^H
       });
       double2* T3 = tmp(T_X3);
       if (ballistic) {
