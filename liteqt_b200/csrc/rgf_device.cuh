@@ -30,12 +30,23 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
 __device__ __forceinline__ double2 czero() { return make_double2(0.0, 0.0); }
-// 1/(a+ib) with scaling so that neither |a| nor |b| overflows when squared.
+// 1/(a+ib) = (a-ib) / (a^2+b^2).  a and b are first scaled by the power of
+// two 2^-e (exact) that brings max(|a|, |b|) into [1/2, 1), so the squares
+// neither overflow nor underflow, and one division forms 1/(a^2+b^2).  Zero,
+// subnormal, infinite and NaN arguments and exponents near the ends of the
+// range take the quotient form with two divisions.
 __device__ __forceinline__ double2 crecip(double2 a) {
   const double s = fmax(fabs(a.x), fabs(a.y));
-  const double ar = a.x / s, ai = a.y / s;
-  const double d = ar * ar + ai * ai;
-  return make_double2(ar / (d * s), -ai / (d * s));
+  const int e = (int)((__double_as_longlong(s) >> 52) & 0x7ff) - 1022;  // s in [2^(e-1), 2^e)
+  if (e < -1020 || e > 1020) {
+    const double ar = a.x / s, ai = a.y / s;
+    const double d = ar * ar + ai * ai;
+    return make_double2(ar / (d * s), -ai / (d * s));
+  }
+  const double sc = __longlong_as_double((long long)(1023 - e) << 52);  // 2^-e
+  const double ar = a.x * sc, ai = a.y * sc;
+  const double r = 1.0 / (ar * ar + ai * ai);
+  return make_double2(ar * r * sc, -ai * r * sc);
 }
 // |re| + |im|: the pivot measure of LAPACK's izamax (dcabs1), used by zgetrf.
 __device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }

@@ -22,6 +22,8 @@
 // sequence and the arithmetic per element are those of the unblocked
 // elimination; only the order of the sums changes.
 #pragma once
+#include <type_traits>
+
 #include "rgf_device.cuh"
 
 namespace rgf {
@@ -50,18 +52,26 @@ struct StagedCfg {
   static constexpr size_t GEMM_SMEM = size_t(NSTAGE) * STAGE * sizeof(double2);
   // inverse: the matrix (nb <= 64) or one panel, then the row / column vectors
   static constexpr size_t INV_MAT = SMEM_INV ? size_t(NB) * NB : size_t(NB) * PW;
-  static constexpr size_t INV_SMEM = (INV_MAT + 2 * size_t(NB) + 8 * size_t(PW)) * sizeof(double2);
+  // after the panel: pivot row + multiplier column + pivot rows of the other
+  // columns, or the register-resident sub-block elimination's scratch
+  static constexpr size_t INV_SCR = (2 * size_t(NB) + 8 * size_t(PW)) > (2 * size_t(NB) + 48 + 2 * size_t(NB) / 32)
+                                        ? (2 * size_t(NB) + 8 * size_t(PW)) : (2 * size_t(NB) + 48 + 2 * size_t(NB) / 32);
+  static constexpr size_t INV_SMEM = (INV_MAT + INV_SCR) * sizeof(double2);
   static constexpr size_t SMEM = GEMM_SMEM > INV_SMEM ? GEMM_SMEM : INV_SMEM;
   static_assert(TM >= 1 && TN >= 1, "tile");
   static_assert(PM % (8 * WARPS_M) == 0 && PN % (8 * WARPS_N) == 0, "tile");
 };
 
-// C = op(A) op(B); epi(i, j, v) once per element by its owner thread.
-// M, N multiples of PM; K multiple of KC.  Caller synchronises afterwards.
-template <int NB, class Epi>
-__device__ __forceinline__ void gemm_staged(int M, int N, int K, const double2* A, int lda, bool cA,
-                                            const double2* B, int ldb, bool cB, double2* stage,
-                                            Epi&& epi, const int16_t* brow = nullptr) {
+struct NoInit {};
+
+// C = C0 + op(A) op(B); epi(i, j, v) once per element by its owner thread.
+// C0 = init(i, j) when an init functor is given (read before the K loop, so
+// its loads overlap the first chunks' copies), else 0.  M, N multiples of PM;
+// K multiple of KC.  Caller synchronises afterwards.
+template <int NB, class Init, class Epi>
+__device__ __forceinline__ void gemm_staged_init(int M, int N, int K, const double2* A, int lda, bool cA,
+                                                 const double2* B, int ldb, bool cB, double2* stage,
+                                                 Init&& init, Epi&& epi, const int16_t* brow) {
   using C = StagedCfg<NB>;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
@@ -98,6 +108,18 @@ __device__ __forceinline__ void gemm_staged(int M, int N, int K, const double2* 
       for (int a = 0; a < C::TM; a++)
 #pragma unroll
         for (int b = 0; b < C::TN; b++) cr[a][b][0] = cr[a][b][1] = ci[a][b][0] = ci[a][b][1] = 0.0;
+      if constexpr (!std::is_same_v<std::decay_t<Init>, NoInit>) {
+#pragma unroll
+        for (int a = 0; a < C::TM; a++)
+#pragma unroll
+          for (int b = 0; b < C::TN; b++)
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+              const double2 v = init(tm0 + wm + 8 * a + g, tn0 + wn + 8 * b + 2 * t + c);
+              cr[a][b][c] = v.x;
+              ci[a][b][c] = v.y;
+            }
+      }
       // prologue: chunks 0 .. NSTAGE-2 in flight; one commit group per chunk
       // (possibly empty), so "all but the newest NSTAGE-1 groups done" means
       // chunk kc has landed
@@ -136,6 +158,128 @@ __device__ __forceinline__ void gemm_staged(int M, int N, int K, const double2* 
   }
 }
 
+template <int NB, class Epi>
+__device__ __forceinline__ void gemm_staged(int M, int N, int K, const double2* A, int lda, bool cA,
+                                            const double2* B, int ldb, bool cB, double2* stage,
+                                            Epi&& epi, const int16_t* brow = nullptr) {
+  gemm_staged_init<NB>(M, N, K, A, lda, cA, B, ldb, cB, stage, NoInit{}, epi, brow);
+}
+
+// Gauss-Jordan elimination of the KB = 8 panel columns sb0.. (pivot rows
+// p0+sb0..) with the sub-block held in registers: thread tid owns row tid % NB
+// and CPT consecutive columns of the sub-block.  Per column:
+//   (1) the owners of the pivot column publish it and reduce the pivot key
+//       per warp (partials to shared memory); barrier;
+//   (2) every thread combines the partials (largest |re|+|im|, first index on
+//       ties, as the unblocked elimination); the two owners of row q form
+//       pinv = 1 / x_qc and the scaled pivot row r_j = x_qj pinv, the owners of
+//       row k publish it, the panel's other columns get the interchange;
+//       barrier;
+//   (3) every thread updates its own elements, x_ij - f_i r_j.
+// The pivot key is the bit pattern of |re|+|im| (monotonic for non-negative
+// doubles) + 2, so the search compares integers: rows above k have key 0 and
+// NaN entries key 1 (never chosen unless the whole column is NaN, then row k,
+// as the scalar search).  The per-element arithmetic is that of the unblocked
+// elimination.  scr: 2 NB + 6 KB + 2 NB/32 complex values of scratch,
+// double-buffered by column parity so one column's readers never race the
+// next column's writers.  Returns with the sub-block written back to the
+// panel and a barrier passed; s.singular is set on a zero pivot.
+template <int NB>
+__device__ __forceinline__ void gj_subblock(double2* panel, int PW, int p0, int sb0, double2* scr,
+                                            int16_t* rmap, SmemInv& s) {
+  constexpr int KB = 8;
+  constexpr int CPT = KB * NB / kThreads;  // sub-block columns per thread
+  constexpr int WPC = NB / 32;             // warps owning one column
+  static_assert(CPT * kThreads == KB * NB && KB % CPT == 0, "sub-block layout");
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int i = tid % NB, h = tid / NB;
+  double2* fraw = scr;          // [2][NB] the pivot column before the step
+  double2* rr = scr + 2 * NB;   // [2][KB] the scaled pivot row r
+  double2* rk = rr + 2 * KB;    // [2][KB] row k of the sub-block before the step
+  unsigned long long* pk = reinterpret_cast<unsigned long long*>(rk + 2 * KB);  // [2][WPC] keys
+  int* pi = reinterpret_cast<int*>(pk + 2 * WPC);                              // [2][WPC] rows
+  double2 x[CPT];
+#pragma unroll
+  for (int m = 0; m < CPT; m++) x[m] = panel[i + (size_t)(sb0 + h * CPT + m) * NB];
+#pragma unroll
+  for (int cc = 0; cc < KB; cc++) {
+    const int k = p0 + sb0 + cc, par = cc & 1;
+    const int hc = cc / CPT, mc = cc % CPT;
+    if (h == hc) {
+      const double2 v = x[mc];
+      fraw[par * NB + i] = v;
+      const double av = cabs1(v);
+      unsigned long long key = 0;
+      if (i >= k) key = (av == av) ? (unsigned long long)__double_as_longlong(av) + 2ull : 1ull;
+      int bi = i;
+#pragma unroll
+      for (int o = 16; o; o >>= 1) {
+        const unsigned long long ok = __shfl_xor_sync(0xffffffffu, key, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ok > key || (ok == key && oi < bi)) { key = ok; bi = oi; }
+      }
+      if (lane == 0) {
+        pk[par * WPC + (warp - hc * WPC)] = key;
+        pi[par * WPC + (warp - hc * WPC)] = bi;
+      }
+    }
+    __syncthreads();
+    unsigned long long key = pk[par * WPC];
+    int q = pi[par * WPC];
+#pragma unroll
+    for (int w = 1; w < WPC; w++) {
+      const unsigned long long ek = pk[par * WPC + w];
+      const int ei = pi[par * WPC + w];
+      if (ek > key || (ek == key && ei < q)) { key = ek; q = ei; }
+    }
+    if (key == 2ull) {  // largest |re|+|im| is zero
+      if (tid == 0) s.singular = 1;
+      break;
+    }
+    if (tid == 0) {
+      s.perm[k] = (int16_t)q;
+      if (q != k) { const int16_t t = rmap[k]; rmap[k] = rmap[q]; rmap[q] = t; }
+    }
+    if (i == q) {
+      const double2 pinv = crecip(fraw[par * NB + q]);
+#pragma unroll
+      for (int m = 0; m < CPT; m++) {
+        const int jj = h * CPT + m;
+        rr[par * KB + jj] = (jj == cc) ? pinv : cmul(x[m], pinv);
+      }
+    }
+    if (i == k) {
+#pragma unroll
+      for (int m = 0; m < CPT; m++) rk[par * KB + h * CPT + m] = x[m];
+    }
+    if (q != k) {  // the panel's other columns: interchange rows k <-> q
+      for (int j = tid; j < PW; j += kThreads) {
+        if (j >= sb0 && j < sb0 + KB) continue;
+        const double2 a = panel[k + (size_t)j * NB];
+        panel[k + (size_t)j * NB] = panel[q + (size_t)j * NB];
+        panel[q + (size_t)j * NB] = a;
+      }
+    }
+    __syncthreads();
+    const double2 f = (i == k) ? czero() : (i == q ? rk[par * KB + cc] : fraw[par * NB + i]);
+#pragma unroll
+    for (int m = 0; m < CPT; m++) {
+      const int jj = h * CPT + m;
+      const double2 r = rr[par * KB + jj];
+      if (i == k) {
+        x[m] = r;
+      } else {
+        const double2 base = (i == q) ? rk[par * KB + jj] : x[m];
+        const double2 xx = (jj == cc) ? czero() : base;
+        x[m] = make_double2(xx.x - (f.x * r.x - f.y * r.y), xx.y - (f.x * r.y + f.y * r.x));
+      }
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < CPT; m++) panel[i + (size_t)(sb0 + h * CPT + m) * NB] = x[m];
+  __syncthreads();
+}
+
 // Blocked Gauss-Jordan inverse of the NB x NB block X0 (global memory, ld
 // NB, destroyed), result into dst (and dst2).  X1: a second global block.
 // The row interchanges of a panel are never applied in place: the panel's
@@ -155,7 +299,7 @@ __device__ int gj_invert_blocked(double2* X0, double2* X1, double2* dst, double2
   double2* rowk = panel + (size_t)NB * PWM;
   double2* fcol = rowk + PWM;
   int16_t* rmap = s.rmap;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
   double2* cur = X0;
   double2* nxt = X1;
   if (tid == 0) s.singular = 0;
@@ -166,79 +310,20 @@ __device__ int gj_invert_blocked(double2* X0, double2* X1, double2* dst, double2
     for (int i = tid; i < NB; i += kThreads) rmap[i] = (int16_t)i;
     __syncthreads();
     // (b) elimination of the panel in sub-blocks of KB columns: each sub-block
-    //     is eliminated unblocked (its row interchanges applied to the whole
-    //     panel at once), then the panel's other columns get the sub-block's
+    //     is eliminated unblocked with its columns in registers (gj_subblock;
+    //     its row interchanges applied to the whole panel), then the panel's
+    //     other columns get the sub-block's
     //     transformation as one rank-KB update (the same U R form as the
     //     panel's own update below), so the panel is read and written once per
     //     sub-block instead of once per column.
     constexpr int KB = 8;
+    static_assert(PWM % KB == 0 && (NB % PWM) % KB == 0, "panels of whole sub-blocks");
     double2* rbuf = fcol + NB;  // KB x PWM pivot rows of the other columns
     for (int sb0 = 0; sb0 < PW && !s.singular; sb0 += KB) {
-      const int kb = (PW - sb0) < KB ? (PW - sb0) : KB;
-      for (int c = sb0; c < sb0 + kb; c++) {
-        const int k = p0 + c;
-        const double2* col = panel + (size_t)c * NB;
-        if (warp == 0) {  // pivot search
-          double best = -1.0;
-          int bi = k;
-          for (int i = k + lane; i < NB; i += 32) {
-            const double v = cabs1(col[i]);
-            if (v > best) { best = v; bi = i; }
-          }
-#pragma unroll
-          for (int o = 16; o; o >>= 1) {
-            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-          }
-          if (lane == 0) {
-            s.piv = bi;
-            s.pivval = col[bi];
-            s.akc = col[k];
-            s.perm[k] = (int16_t)bi;
-            if (best == 0.0) s.singular = 1;
-            if (bi != k) { const int16_t t = rmap[k]; rmap[k] = rmap[bi]; rmap[bi] = t; }
-          }
-        }
-        __syncthreads();
-        if (s.singular) break;
-        const int q = s.piv;
-        const double2 pinv = crecip(s.pivval);
-        // interchange rows k <-> q over the whole panel; scale row k in the
-        // sub-block; multipliers f_i = old column entries
-        for (int e = tid; e < PW + NB; e += kThreads) {
-          if (e < PW) {
-            const int j = e;
-            const double2 a = panel[k + (size_t)j * NB];
-            const double2 b = panel[q + (size_t)j * NB];
-            if (q != k) panel[q + (size_t)j * NB] = a;
-            if (j >= sb0 && j < sb0 + kb) {
-              const double2 r = (j == c) ? pinv : cmul(b, pinv);
-              panel[k + (size_t)j * NB] = r;
-              rowk[j] = r;
-            } else {
-              panel[k + (size_t)j * NB] = b;
-            }
-          } else {
-            const int i = e - PW;
-            fcol[i] = (i == k) ? czero() : (i == q ? s.akc : col[i]);
-          }
-        }
-        __syncthreads();
-        for (int e = tid; e < NB * kb; e += kThreads) {
-          const int jj = e / NB, i = e - jj * NB;
-          const int j = sb0 + jj;
-          if (i == k) continue;
-          const double2 f = fcol[i];
-          const size_t o = i + (size_t)j * NB;
-          const double2 x = (j == c) ? czero() : panel[o];
-          const double2 r = rowk[j];
-          panel[o] = make_double2(x.x - (f.x * r.x - f.y * r.y), x.y - (f.x * r.y + f.y * r.x));
-        }
-        __syncthreads();
-      }
+      const int kb = KB;
+      gj_subblock<NB>(panel, PW, p0, sb0, rowk, rmap, s);
       if (s.singular) break;
-      // rank-kb update of the panel's other columns j (pivot rows R = rows
+      // rank-KB update of the panel's other columns j (pivot rows R = rows
       // p0+sb0.. of those columns, before the update):
       //   X[i, j] = (i in sub-block rows ? 0 : X[i, j]) + sum_t U[i, t] R[t, j]
       const int nrest = PW - kb;
@@ -249,27 +334,37 @@ __device__ int gj_invert_blocked(double2* X0, double2* X1, double2* dst, double2
           rbuf[t + jr * KB] = panel[(p0 + sb0 + t) + (size_t)j * NB];
         }
         __syncthreads();
-        // thread: one row i and a strided subset of the other columns
-        constexpr int TPR = kThreads / NB > 0 ? kThreads / NB : 1;  // threads per row
-        for (int i = tid % NB, part = tid / NB; i < NB && part < TPR; i += NB) {
-          double2 u[KB];
+        // on the FP64 tensor pipe: warp w owns rows 8 TMU w .. (TMU 8-row
+        // subtiles) and walks the 8-column subtiles of the other columns;
+        // K = KB = 8 is two m8n8k4 steps, U's fragments loaded once
+        constexpr int TMU = NB / (8 * (kThreads / 32));
+        const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, t4 = lane & 3;
+        const int wm = warp * 8 * TMU;
+        double2 av[2][TMU];
 #pragma unroll
-          for (int t = 0; t < KB; t++) u[t] = t < kb ? panel[i + (size_t)(sb0 + t) * NB] : czero();
-          const bool prow = i >= p0 + sb0 && i < p0 + sb0 + kb;
-          for (int jr = part; jr < nrest; jr += TPR) {
-            const int j = jr < sb0 ? jr : jr + kb;
-            const size_t o = i + (size_t)j * NB;
-            double2 x = prow ? czero() : panel[o];
+        for (int ks = 0; ks < 2; ks++)
 #pragma unroll
-            for (int t = 0; t < KB; t++) {
-              if (t < kb) {
-                const double2 r = rbuf[t + jr * KB];
-                x.x += u[t].x * r.x - u[t].y * r.y;
-                x.y += u[t].x * r.y + u[t].y * r.x;
-              }
-            }
-            panel[o] = x;
+          for (int a = 0; a < TMU; a++) av[ks][a] = panel[(wm + 8 * a + g) + (size_t)(sb0 + 4 * ks + t4) * NB];
+        for (int b = 0; b < nrest / 8; b++) {
+          double cr[TMU][1][2], ci[TMU][1][2];
+#pragma unroll
+          for (int a = 0; a < TMU; a++) cr[a][0][0] = cr[a][0][1] = ci[a][0][0] = ci[a][0][1] = 0.0;
+#pragma unroll
+          for (int ks = 0; ks < 2; ks++) {
+            const double2 bv[1] = {rbuf[(4 * ks + t4) + (8 * b + g) * KB]};
+            cmma_step<TMU, 1>(cr, ci, av[ks], bv, 1.0, 1.0);
           }
+#pragma unroll
+          for (int a = 0; a < TMU; a++)
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+              const int i = wm + 8 * a + g, jr = 8 * b + 2 * t4 + c;
+              const int j = jr < sb0 ? jr : jr + KB;
+              const bool prow = i >= p0 + sb0 && i < p0 + sb0 + KB;
+              const size_t o = i + (size_t)j * NB;
+              const double2 x = prow ? czero() : panel[o];
+              panel[o] = make_double2(x.x + cr[a][0][c], x.y + ci[a][0][c]);
+            }
         }
         __syncthreads();
       }
@@ -280,13 +375,16 @@ __device__ int gj_invert_blocked(double2* X0, double2* X1, double2* dst, double2
     __syncthreads();
     // (d) other columns: with R = rows rmap[P] of cur and U the panel,
     //     nxt[P, j] = U[P, :] R[:, j],   nxt[i, j] = cur[rmap[i], j] + U[i, :] R[:, j]
-    gemm_staged<NB>(NB, NB, PW, nxt + (size_t)p0 * NB, NB, false, cur, NB, false, stage,
-                    [&](int i, int j, double2 v) {
-                      if (j >= p0 && j < p0 + PW) return;
-                      const size_t o = i + (size_t)j * NB;
-                      nxt[o] = (i >= p0 && i < p0 + PW) ? v : cadd(cur[(size_t)rmap[i] + (size_t)j * NB], v);
-                    },
-                    rmap + p0);
+    gemm_staged_init<NB>(NB, NB, PW, nxt + (size_t)p0 * NB, NB, false, cur, NB, false, stage,
+                         [&](int i, int j) {
+                           const bool keep = (i < p0 || i >= p0 + PW) && (j < p0 || j >= p0 + PW);
+                           return keep ? cur[(size_t)rmap[i] + (size_t)j * NB] : czero();
+                         },
+                         [&](int i, int j, double2 v) {
+                           if (j >= p0 && j < p0 + PW) return;
+                           nxt[i + (size_t)j * NB] = v;
+                         },
+                         rmap + p0);
     __syncthreads();
     double2* t = cur;
     cur = nxt;
