@@ -174,6 +174,7 @@ __device__ __forceinline__ void cgemm(int n, const double2* A, bool cA, const do
 struct SmemInv {
   int16_t perm[kMaxNb];
   int16_t colsrc[kMaxNb];
+  int16_t coldst[kMaxNb];  // inverse of colsrc (blocked inverse)
   int16_t rmap[kMaxNb];  // row map of the current panel (outside the GEMM staging area)
   double2 pivval;
   double2 akc;  // the pivot column's entry in row k before the interchange

@@ -46,7 +46,7 @@ struct StagedCfg {
   static constexpr int WM = PM / WARPS_M, WN = PN / WARPS_N;   // warp tile
   static constexpr int TM = WM / 8, TN = WN / 8;               // 8x8 subtiles per warp
   static constexpr int STAGE = 2 * KC * LDS;                   // complex values per stage (A + B)
-  static constexpr int NSTAGE = 3;                             // cp.async pipeline depth
+  static constexpr int NSTAGE = 3;                             // cp.async pipeline depth (>= 2)
   static constexpr int PW = NB >= 256 ? 16 : (NB >= 128 ? 48 : 32);  // inverse panel width (max)
   static constexpr bool SMEM_INV = NB <= 64;                   // whole inverse in shared memory
   static constexpr size_t GEMM_SMEM = size_t(NSTAGE) * STAGE * sizeof(double2);
@@ -121,18 +121,23 @@ __device__ __forceinline__ void gemm_staged_init(int M, int N, int K, const doub
             }
       }
       // prologue: chunks 0 .. NSTAGE-2 in flight; one commit group per chunk
-      // (possibly empty), so "all but the newest NSTAGE-1 groups done" means
-      // chunk kc has landed
+      // (possibly empty), so at iteration kc "all but the newest NSTAGE-2
+      // groups done" means chunk kc has landed.  One barrier per chunk: it
+      // makes chunk kc visible and proves every warp done with chunk kc-1,
+      // whose stage the refill after it reuses; the barrier before the
+      // prologue frees the stages of the previous tile (or the caller's use
+      // of the same shared memory).
+      __syncthreads();
 #pragma unroll
       for (int c = 0; c < C::NSTAGE - 1; c++) {
         if (c < nchunks) load_chunk(c, c);
         cp_async_commit();
       }
       for (int kc = 0; kc < nchunks; kc++) {
+        cp_async_wait<C::NSTAGE - 2>();
+        __syncthreads();
         if (kc + C::NSTAGE - 1 < nchunks) load_chunk(kc + C::NSTAGE - 1, (kc + C::NSTAGE - 1) % C::NSTAGE);
         cp_async_commit();
-        cp_async_wait<C::NSTAGE - 1>();
-        __syncthreads();
         const double2* As = stage + (kc % C::NSTAGE) * C::STAGE;
         const double2* Bs = As + C::KC * C::LDS;
 #pragma unroll
@@ -144,7 +149,6 @@ __device__ __forceinline__ void gemm_staged_init(int M, int N, int K, const doub
           for (int b = 0; b < C::TN; b++) bv[b] = Bs[(k4 + t) * C::LDS + wn + 8 * b + g];
           cmma_step<C::TM, C::TN>(cr, ci, av, bv, a_sg, b_sg);
         }
-        __syncthreads();  // the stage is refilled by the next iteration
       }
 #pragma unroll
       for (int a = 0; a < C::TM; a++)
@@ -284,8 +288,9 @@ __device__ __forceinline__ void gj_subblock(double2* panel, int PW, int p0, int 
 // NB, destroyed), result into dst (and dst2).  X1: a second global block.
 // The row interchanges of a panel are never applied in place: the panel's
 // update reads the permuted rows of the current matrix (row gather in the
-// GEMM loader and in the epilogue) and writes the next matrix, the two
-// buffers alternating.  Dynamic shared memory: panel (NB x PW), pivot row
+// GEMM loader and in the accumulators' preload) and writes the next matrix,
+// the two buffers alternating; the last panel writes dst itself, its columns
+// in the inverse's order.  Dynamic shared memory: panel (NB x PW), pivot row
 // (PW), multiplier column (NB) -- none of them is live during the update
 // GEMM, which reuses the same memory as its staging buffers.  The panel's row
 // map is read by that GEMM, so it lives in the static SmemInv.
@@ -370,8 +375,33 @@ __device__ int gj_invert_blocked(double2* X0, double2* X1, double2* dst, double2
       }
     }
     if (s.singular) break;
+    // the last panel writes the inverse itself: its column j is column
+    // colsrc[j] of the eliminated matrix (the interchanges undone), i.e.
+    // column c goes to coldst[c]
+    const bool last = p0 + PW >= NB;
+    if (last) {
+      if (tid == 0) {
+        for (int j = 0; j < NB; j++) s.colsrc[j] = (int16_t)j;
+        for (int k = NB - 1; k >= 0; k--) {
+          const int q = s.perm[k];
+          if (q != k) { const int16_t tmp = s.colsrc[k]; s.colsrc[k] = s.colsrc[q]; s.colsrc[q] = tmp; }
+        }
+      }
+      __syncthreads();
+      for (int j = tid; j < NB; j += kThreads) s.coldst[s.colsrc[j]] = (int16_t)j;
+      __syncthreads();
+    }
     // (c) eliminated panel -> next matrix (its rows are already in the new order)
-    for (int e = tid; e < NB * PW; e += kThreads) nxt[(size_t)p0 * NB + e] = panel[e];
+    for (int e = tid; e < NB * PW; e += kThreads) {
+      const double2 v = panel[e];
+      nxt[(size_t)p0 * NB + e] = v;
+      if (last) {
+        const int jj = e / NB, i = e - jj * NB;
+        const size_t o = i + (size_t)s.coldst[p0 + jj] * NB;
+        dst[o] = v;
+        if (dst2) dst2[o] = v;
+      }
+    }
     __syncthreads();
     // (d) other columns: with R = rows rmap[P] of cur and U the panel,
     //     nxt[P, j] = U[P, :] R[:, j],   nxt[i, j] = cur[rmap[i], j] + U[i, :] R[:, j]
@@ -382,7 +412,13 @@ __device__ int gj_invert_blocked(double2* X0, double2* X1, double2* dst, double2
                          },
                          [&](int i, int j, double2 v) {
                            if (j >= p0 && j < p0 + PW) return;
-                           nxt[i + (size_t)j * NB] = v;
+                           if (last) {
+                             const size_t o = i + (size_t)s.coldst[j] * NB;
+                             dst[o] = v;
+                             if (dst2) dst2[o] = v;
+                           } else {
+                             nxt[i + (size_t)j * NB] = v;
+                           }
                          },
                          rmap + p0);
     __syncthreads();
@@ -399,21 +435,6 @@ __device__ int gj_invert_blocked(double2* X0, double2* X1, double2* dst, double2
     __syncthreads();
     return 1;
   }
-  if (tid == 0) {
-    for (int j = 0; j < NB; j++) s.colsrc[j] = (int16_t)j;
-    for (int k = NB - 1; k >= 0; k--) {
-      const int q = s.perm[k];
-      if (q != k) { const int16_t tmp = s.colsrc[k]; s.colsrc[k] = s.colsrc[q]; s.colsrc[q] = tmp; }
-    }
-  }
-  __syncthreads();
-  for (int e = tid; e < NB * NB; e += kThreads) {
-    const int j = e / NB, i = e - j * NB;
-    const double2 v = cur[i + (size_t)s.colsrc[j] * NB];
-    dst[e] = v;
-    if (dst2) dst2[e] = v;
-  }
-  __syncthreads();
   return 0;
 }
 
