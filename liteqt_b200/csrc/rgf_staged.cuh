@@ -173,21 +173,24 @@ __device__ __forceinline__ void gemm_staged(int M, int N, int K, const double2* 
 // p0+sb0..) with the sub-block held in registers: thread tid owns row tid % NB
 // and CPT consecutive columns of the sub-block.  Per column:
 //   (1) the owners of the pivot column publish it and reduce the pivot key
-//       per warp (partials to shared memory); barrier;
-//   (2) every thread combines the partials (largest |re|+|im|, first index on
-//       ties, as the unblocked elimination); the two owners of row q form
-//       pinv = 1 / x_qc and the scaled pivot row r_j = x_qj pinv, the owners of
-//       row k publish it, the panel's other columns get the interchange;
+//       per warp (redux.sync; partials to shared memory), each lane forming
+//       the reciprocal of its own entry meanwhile so the winner's is ready;
 //       barrier;
+//   (2) every thread combines the partials (largest key, first row on ties);
+//       the two owners of row q form the scaled pivot row r_j = x_qj / x_qc,
+//       the owners of row k publish it, the panel's other columns get the
+//       interchange; barrier;
 //   (3) every thread updates its own elements, x_ij - f_i r_j.
-// The pivot key is the bit pattern of |re|+|im| (monotonic for non-negative
-// doubles) + 2, so the search compares integers: rows above k have key 0 and
-// NaN entries key 1 (never chosen unless the whole column is NaN, then row k,
-// as the scalar search).  The per-element arithmetic is that of the unblocked
-// elimination.  scr: 2 NB + 6 KB + 2 NB/32 complex values of scratch,
-// double-buffered by column parity so one column's readers never race the
-// next column's writers.  Returns with the sub-block written back to the
-// panel and a barrier passed; s.singular is set on a zero pivot.
+// The pivot key is the high word of the bit pattern of |re|+|im| (monotonic
+// for non-negative doubles), so entries within 2^-20 of each other count as
+// equal and the first row among them is taken; rows above k have key 0, NaN
+// entries key 1 (never chosen unless the whole column is NaN, then row k as
+// the scalar search), exact zeros key 2 and every other entry a larger key.
+// The per-element arithmetic is that of the unblocked elimination.  scr:
+// 2 NB + 6 KB + 2 NB/32 complex values of scratch, double-buffered by column
+// parity so one column's readers never race the next column's writers.
+// Returns with the sub-block written back to the panel and a barrier passed;
+// s.singular is set on a zero pivot.
 template <int NB>
 __device__ __forceinline__ void gj_subblock(double2* panel, int PW, int p0, int sb0, double2* scr,
                                             int16_t* rmap, SmemInv& s) {
@@ -195,13 +198,14 @@ __device__ __forceinline__ void gj_subblock(double2* panel, int PW, int p0, int 
   constexpr int CPT = KB * NB / kThreads;  // sub-block columns per thread
   constexpr int WPC = NB / 32;             // warps owning one column
   static_assert(CPT * kThreads == KB * NB && KB % CPT == 0, "sub-block layout");
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5;
   const int i = tid % NB, h = tid / NB;
-  double2* fraw = scr;          // [2][NB] the pivot column before the step
-  double2* rr = scr + 2 * NB;   // [2][KB] the scaled pivot row r
-  double2* rk = rr + 2 * KB;    // [2][KB] row k of the sub-block before the step
-  unsigned long long* pk = reinterpret_cast<unsigned long long*>(rk + 2 * KB);  // [2][WPC] keys
-  int* pi = reinterpret_cast<int*>(pk + 2 * WPC);                              // [2][WPC] rows
+  double2* fraw = scr;           // [2][NB] the pivot column before the step
+  double2* rr = scr + 2 * NB;    // [2][KB] the scaled pivot row r
+  double2* rk = rr + 2 * KB;     // [2][KB] row k of the sub-block before the step
+  double2* pinvw = rk + 2 * KB;  // [2][WPC] per-warp winner's reciprocal
+  unsigned* pk = reinterpret_cast<unsigned*>(pinvw + 2 * WPC);  // [2][WPC] keys
+  int* pi = reinterpret_cast<int*>(pk + 2 * WPC);               // [2][WPC] rows
   double2 x[CPT];
 #pragma unroll
   for (int m = 0; m < CPT; m++) x[m] = panel[i + (size_t)(sb0 + h * CPT + m) * NB];
@@ -213,39 +217,38 @@ __device__ __forceinline__ void gj_subblock(double2* panel, int PW, int p0, int 
       const double2 v = x[mc];
       fraw[par * NB + i] = v;
       const double av = cabs1(v);
-      unsigned long long key = 0;
-      if (i >= k) key = (av == av) ? (unsigned long long)__double_as_longlong(av) + 2ull : 1ull;
-      int bi = i;
-#pragma unroll
-      for (int o = 16; o; o >>= 1) {
-        const unsigned long long ok = __shfl_xor_sync(0xffffffffu, key, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ok > key || (ok == key && oi < bi)) { key = ok; bi = oi; }
+      unsigned key = 0u;
+      if (i >= k) {
+        const unsigned hi = (unsigned)((unsigned long long)__double_as_longlong(av) >> 32);
+        key = !(av == av) ? 1u : (av == 0.0 ? 2u : (hi > 1u ? hi : 1u) + 2u);
       }
-      if (lane == 0) {
-        pk[par * WPC + (warp - hc * WPC)] = key;
-        pi[par * WPC + (warp - hc * WPC)] = bi;
+      const double2 pv = crecip(v);
+      const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
+      const unsigned imin = __reduce_min_sync(0xffffffffu, key == kmax ? (unsigned)i : 0xffffffffu);
+      if ((unsigned)i == imin) {
+        const int w = warp - hc * WPC;
+        pk[par * WPC + w] = kmax;
+        pi[par * WPC + w] = i;
+        pinvw[par * WPC + w] = pv;
       }
     }
     __syncthreads();
-    unsigned long long key = pk[par * WPC];
-    int q = pi[par * WPC];
+    unsigned key = pk[par * WPC];
+    int q = pi[par * WPC], wq = 0;
 #pragma unroll
     for (int w = 1; w < WPC; w++) {
-      const unsigned long long ek = pk[par * WPC + w];
+      const unsigned ek = pk[par * WPC + w];
       const int ei = pi[par * WPC + w];
-      if (ek > key || (ek == key && ei < q)) { key = ek; q = ei; }
+      if (ek > key || (ek == key && ei < q)) { key = ek; q = ei; wq = w; }
     }
-    if (key == 2ull) {  // largest |re|+|im| is zero
-      if (tid == 0) s.singular = 1;
-      break;
-    }
+    // largest |re|+|im| zero: flagged, and the caller discards the block
+    if (key == 2u && tid == 0) s.singular = 1;
     if (tid == 0) {
       s.perm[k] = (int16_t)q;
       if (q != k) { const int16_t t = rmap[k]; rmap[k] = rmap[q]; rmap[q] = t; }
     }
     if (i == q) {
-      const double2 pinv = crecip(fraw[par * NB + q]);
+      const double2 pinv = pinvw[par * WPC + wq];
 #pragma unroll
       for (int m = 0; m < CPT; m++) {
         const int jj = h * CPT + m;
@@ -311,8 +314,10 @@ __device__ int gj_invert_blocked(double2* X0, double2* X1, double2* dst, double2
   for (int p0 = 0; p0 < NB; p0 += PWM) {
     const int PW = (NB - p0) < PWM ? (NB - p0) : PWM;
     // (a) panel columns of the current matrix -> shared memory (ld NB)
-    for (int e = tid; e < NB * PW; e += kThreads) panel[e] = cur[(size_t)p0 * NB + e];
+    for (int e = tid; e < NB * PW; e += kThreads) cp_async16(panel + e, cur + (size_t)p0 * NB + e);
+    cp_async_commit();
     for (int i = tid; i < NB; i += kThreads) rmap[i] = (int16_t)i;
+    cp_async_wait<0>();
     __syncthreads();
     // (b) elimination of the panel in sub-blocks of KB columns: each sub-block
     //     is eliminated unblocked with its columns in registers (gj_subblock;
