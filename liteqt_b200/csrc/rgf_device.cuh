@@ -62,6 +62,16 @@ __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double
       : "d"(a), "d"(b));
 }
 
+// D(16x8) += A(16x4, row) * B(4x8, col); lane (g, t) holds a0 = A[g][t],
+// a1 = A[g+8][t], b = B[t][g], d0, d1 = D[g][2t, 2t+1], d2, d3 = D[g+8][2t,
+// 2t+1]: two m8n8k4 products sharing B in one instruction.
+__device__ __forceinline__ void dmma1684(double& d0, double& d1, double& d2, double& d3, double a0,
+                                         double a1, double b) {
+  asm("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+      : "+d"(d0), "+d"(d1), "+d"(d2), "+d"(d3)
+      : "d"(a0), "d"(a1), "d"(b));
+}
+
 // ---------------------------------------------------------------- reductions
 struct SmemRed {
   double v[2 * kWarps];
@@ -102,22 +112,50 @@ template <int TM, int TN>
 __device__ __forceinline__ void cmma_step(double (&cr)[TM][TN][2], double (&ci)[TM][TN][2],
                                           const double2 (&av)[TM], const double2 (&bv)[TN],
                                           double a_sg, double b_sg) {
+  if constexpr (TM % 2 == 0) {
+    // row subtiles (2p, 2p+1) are rows g and g+8 of one 16-row tile
 #pragma unroll
-  for (int a = 0; a < TM; a++)
+    for (int p = 0; p < TM / 2; p++)
 #pragma unroll
-    for (int b = 0; b < TN; b++) dmma884(cr[a][b][0], cr[a][b][1], av[a].x, bv[b].x);
+      for (int b = 0; b < TN; b++)
+        dmma1684(cr[2 * p][b][0], cr[2 * p][b][1], cr[2 * p + 1][b][0], cr[2 * p + 1][b][1],
+                 av[2 * p].x, av[2 * p + 1].x, bv[b].x);
 #pragma unroll
-  for (int a = 0; a < TM; a++)
+    for (int p = 0; p < TM / 2; p++)
 #pragma unroll
-    for (int b = 0; b < TN; b++) dmma884(ci[a][b][0], ci[a][b][1], av[a].x, bv[b].y * b_sg);
+      for (int b = 0; b < TN; b++)
+        dmma1684(ci[2 * p][b][0], ci[2 * p][b][1], ci[2 * p + 1][b][0], ci[2 * p + 1][b][1],
+                 av[2 * p].x, av[2 * p + 1].x, bv[b].y * b_sg);
 #pragma unroll
-  for (int a = 0; a < TM; a++)
+    for (int p = 0; p < TM / 2; p++)
 #pragma unroll
-    for (int b = 0; b < TN; b++) dmma884(cr[a][b][0], cr[a][b][1], -av[a].y * a_sg, bv[b].y * b_sg);
+      for (int b = 0; b < TN; b++)
+        dmma1684(cr[2 * p][b][0], cr[2 * p][b][1], cr[2 * p + 1][b][0], cr[2 * p + 1][b][1],
+                 -av[2 * p].y * a_sg, -av[2 * p + 1].y * a_sg, bv[b].y * b_sg);
 #pragma unroll
-  for (int a = 0; a < TM; a++)
+    for (int p = 0; p < TM / 2; p++)
 #pragma unroll
-    for (int b = 0; b < TN; b++) dmma884(ci[a][b][0], ci[a][b][1], av[a].y * a_sg, bv[b].x);
+      for (int b = 0; b < TN; b++)
+        dmma1684(ci[2 * p][b][0], ci[2 * p][b][1], ci[2 * p + 1][b][0], ci[2 * p + 1][b][1],
+                 av[2 * p].y * a_sg, av[2 * p + 1].y * a_sg, bv[b].x);
+  } else {
+#pragma unroll
+    for (int a = 0; a < TM; a++)
+#pragma unroll
+      for (int b = 0; b < TN; b++) dmma884(cr[a][b][0], cr[a][b][1], av[a].x, bv[b].x);
+#pragma unroll
+    for (int a = 0; a < TM; a++)
+#pragma unroll
+      for (int b = 0; b < TN; b++) dmma884(ci[a][b][0], ci[a][b][1], av[a].x, bv[b].y * b_sg);
+#pragma unroll
+    for (int a = 0; a < TM; a++)
+#pragma unroll
+      for (int b = 0; b < TN; b++) dmma884(cr[a][b][0], cr[a][b][1], -av[a].y * a_sg, bv[b].y * b_sg);
+#pragma unroll
+    for (int a = 0; a < TM; a++)
+#pragma unroll
+      for (int b = 0; b < TN; b++) dmma884(ci[a][b][0], ci[a][b][1], av[a].y * a_sg, bv[b].x);
+  }
 }
 
 // ---------------------------------------------------------------- GEMM
