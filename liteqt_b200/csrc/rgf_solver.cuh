@@ -101,7 +101,11 @@ struct StagedOps {
     gemm_staged<NB>(NB, NB, NB, A, NB, cA, B, NB, cB, dyn, epi);
   }
   __device__ int invert(int, double2* dst, double2* dst2) {
-    if constexpr (StagedCfg<NB>::SMEM_INV)
+    // nb = 32: matrix in registers (4 elements a thread); nb = 64: in shared
+    // memory (the register form, 16 elements a thread, measured slower)
+    if constexpr (NB == 32)
+      return gj_invert_reg<NB>(X, dst, dst2, inv, dyn + (size_t)NB * NB);
+    else if constexpr (StagedCfg<NB>::SMEM_INV)
       return gj_invert(NB, X, dst, dst2, inv, dyn + (size_t)NB * NB, dyn + (size_t)NB * NB + NB);
     else return gj_invert_blocked<NB>(X, Rt, dst, dst2, dyn, dyn, inv);
   }

@@ -54,8 +54,9 @@ struct StagedCfg {
   static constexpr size_t INV_MAT = SMEM_INV ? size_t(NB) * NB : size_t(NB) * PW;
   // after the panel: pivot row + multiplier column + pivot rows of the other
   // columns, or the register-resident sub-block elimination's scratch
-  static constexpr size_t INV_SCR = (2 * size_t(NB) + 8 * size_t(PW)) > (2 * size_t(NB) + 48 + 2 * size_t(NB) / 32)
-                                        ? (2 * size_t(NB) + 8 * size_t(PW)) : (2 * size_t(NB) + 48 + 2 * size_t(NB) / 32);
+  static constexpr size_t INV_SCR_A = 2 * size_t(NB) + 8 * size_t(PW);
+  static constexpr size_t INV_SCR_B = 6 * size_t(NB) + 4 * size_t(NB) / 32 + 8;  // register inverse
+  static constexpr size_t INV_SCR = INV_SCR_A > INV_SCR_B ? INV_SCR_A : INV_SCR_B;
   static constexpr size_t INV_SMEM = (INV_MAT + INV_SCR) * sizeof(double2);
   static constexpr size_t SMEM = GEMM_SMEM > INV_SMEM ? GEMM_SMEM : INV_SMEM;
   static_assert(TM >= 1 && TN >= 1, "tile");
@@ -150,6 +151,10 @@ __device__ __forceinline__ void gemm_staged_init(int M, int N, int K, const doub
           cmma_step<C::TM, C::TN>(cr, ci, av, bv, a_sg, b_sg);
         }
       }
+      // every warp is done with the stages before any epilogue runs: an
+      // epilogue may write shared memory the stages alias (the nb <= 64
+      // inverse assembles its matrix there)
+      __syncthreads();
 #pragma unroll
       for (int a = 0; a < C::TM; a++)
 #pragma unroll
@@ -167,6 +172,131 @@ __device__ __forceinline__ void gemm_staged(int M, int N, int K, const double2* 
                                             const double2* B, int ldb, bool cB, double2* stage,
                                             Epi&& epi, const int16_t* brow = nullptr) {
   gemm_staged_init<NB>(M, N, K, A, lda, cA, B, ldb, cB, stage, NoInit{}, epi, brow);
+}
+
+// Gauss-Jordan inverse (partial pivoting) of the N x N block X (shared
+// memory; used for N = 32) with the matrix held in registers: thread tid owns row
+// tid % N and the CPT = N^2 / 256 consecutive columns of group tid / N.  Per
+// column k:
+//   (1) the owners of column k publish it and reduce the pivot key per warp
+//       (redux.sync), each forming the reciprocal of its entry meanwhile;
+//       barrier;
+//   (2) every thread combines the partials (largest key, first row on ties);
+//       the owners of row q publish the scaled pivot row r_j = x_qj / x_qk,
+//       the owners of row k publish row k; barrier;
+//   (3) every thread updates its elements, x_ij - f_i r_j (column k: -f_i r_k).
+// Key, tie and zero-pivot rules as gj_subblock.  At the end each thread
+// writes its elements to dst (and dst2) in the inverse's column order
+// (column c of the eliminated matrix is column coldst[c] of the inverse).
+// scr: 6 N + 4 N/32 + 8 complex values of shared scratch, double-buffered by
+// column parity.  Returns 1 (and zeros dst) on a zero pivot.
+template <int N>
+__device__ __noinline__ int gj_invert_reg(const double2* X, double2* dst, double2* dst2, SmemInv& s,
+                                          double2* scr) {
+  constexpr int CPT = N * N / kThreads;  // columns per thread
+  constexpr int WPC = N / 32;            // warps owning one column
+  static_assert(CPT * kThreads == N * N && N % 32 == 0 && CPT >= 1, "register inverse layout");
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int i = tid % N, h = tid / N, j0 = h * CPT;
+  double2* fraw = scr;               // [2][N] column k before the step
+  double2* rr = fraw + 2 * N;        // [2][N] scaled pivot row
+  double2* rk = rr + 2 * N;          // [2][N] row k before the step
+  double2* pinvw = rk + 2 * N;       // [2][WPC] winners' reciprocals
+  unsigned* pk = reinterpret_cast<unsigned*>(pinvw + 2 * WPC);  // [2][WPC]
+  int* pi = reinterpret_cast<int*>(pk + 2 * WPC);               // [2][WPC]
+  double2 x[CPT];
+#pragma unroll
+  for (int m = 0; m < CPT; m++) x[m] = X[i + (j0 + m) * N];
+  if (tid == 0) s.singular = 0;
+  for (int k = 0; k < N; k++) {
+    const int par = k & 1, hc = k / CPT, mc = k - hc * CPT;
+    if (h == hc) {
+      double2 v = x[0];
+#pragma unroll
+      for (int m = 1; m < CPT; m++)
+        if (m == mc) v = x[m];
+      fraw[par * N + i] = v;
+      const double av = cabs1(v);
+      unsigned key = 0u;
+      if (i >= k) {
+        const unsigned hi = (unsigned)((unsigned long long)__double_as_longlong(av) >> 32);
+        key = !(av == av) ? 1u : (av == 0.0 ? 2u : (hi > 1u ? hi : 1u) + 2u);
+      }
+      const double2 pv = crecip(v);
+      const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
+      const unsigned imin = __reduce_min_sync(0xffffffffu, key == kmax ? (unsigned)i : 0xffffffffu);
+      if ((unsigned)i == imin) {
+        const int w = warp - hc * WPC;
+        pk[par * WPC + w] = kmax;
+        pi[par * WPC + w] = i;
+        pinvw[par * WPC + w] = pv;
+      }
+    }
+    __syncthreads();
+    unsigned key = pk[par * WPC];
+    int q = pi[par * WPC], wq = 0;
+#pragma unroll
+    for (int w = 1; w < WPC; w++) {
+      const unsigned ek = pk[par * WPC + w];
+      const int ei = pi[par * WPC + w];
+      if (ek > key || (ek == key && ei < q)) { key = ek; q = ei; wq = w; }
+    }
+    if (tid == 0) {
+      if (key == 2u) s.singular = 1;
+      s.perm[k] = (int16_t)q;
+    }
+    if (i == q) {
+      const double2 pinv = pinvw[par * WPC + wq];
+#pragma unroll
+      for (int m = 0; m < CPT; m++) rr[par * N + j0 + m] = (j0 + m == k) ? pinv : cmul(x[m], pinv);
+    }
+    if (i == k) {
+#pragma unroll
+      for (int m = 0; m < CPT; m++) rk[par * N + j0 + m] = x[m];
+    }
+    __syncthreads();
+    const double2 f = (i == k) ? czero() : (i == q ? rk[par * N + k] : fraw[par * N + i]);
+#pragma unroll
+    for (int m = 0; m < CPT; m++) {
+      const int j = j0 + m;
+      const double2 r = rr[par * N + j];
+      if (i == k) {
+        x[m] = r;
+      } else {
+        const double2 base = (i == q) ? rk[par * N + j] : x[m];
+        const double2 xx = (j == k) ? czero() : base;
+        x[m] = make_double2(xx.x - (f.x * r.x - f.y * r.y), xx.y - (f.x * r.y + f.y * r.x));
+      }
+    }
+  }
+  __syncthreads();
+  if (s.singular) {
+#pragma unroll
+    for (int m = 0; m < CPT; m++) {
+      dst[i + (j0 + m) * N] = czero();
+      if (dst2) dst2[i + (j0 + m) * N] = czero();
+    }
+    __syncthreads();
+    return 1;
+  }
+  if (tid == 0) {
+    for (int j = 0; j < N; j++) s.colsrc[j] = (int16_t)j;
+    for (int k = N - 1; k >= 0; k--) {
+      const int q = s.perm[k];
+      if (q != k) { const int16_t tmp = s.colsrc[k]; s.colsrc[k] = s.colsrc[q]; s.colsrc[q] = tmp; }
+    }
+  }
+  __syncthreads();
+  for (int j = tid; j < N; j += kThreads) s.coldst[s.colsrc[j]] = (int16_t)j;
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < CPT; m++) {
+    const int o = i + s.coldst[j0 + m] * N;
+    dst[o] = x[m];
+    if (dst2) dst2[o] = x[m];
+  }
+  __syncthreads();
+  return 0;
 }
 
 // Gauss-Jordan elimination of the KB = 8 panel columns sb0.. (pivot rows
