@@ -102,11 +102,12 @@ struct StagedOps {
   }
   __device__ int invert(int, double2* dst, double2* dst2) {
     // nb = 32: matrix in registers (4 elements a thread); nb = 64: in shared
-    // memory (the register form, 16 elements a thread, measured slower)
+    // memory as one panel of the blocked form (the register form, 16
+    // elements a thread, measured slower)
     if constexpr (NB == 32)
       return gj_invert_reg<NB>(X, dst, dst2, inv, dyn + (size_t)NB * NB);
     else if constexpr (StagedCfg<NB>::SMEM_INV)
-      return gj_invert(NB, X, dst, dst2, inv, dyn + (size_t)NB * NB, dyn + (size_t)NB * NB + NB);
+      return gj_invert_smem_blocked<NB>(X, dst, dst2, inv, dyn + (size_t)NB * NB);
     else return gj_invert_blocked<NB>(X, Rt, dst, dst2, dyn, dyn, inv);
   }
 };

@@ -52,13 +52,22 @@ struct StagedCfg {
   static constexpr size_t GEMM_SMEM = size_t(NSTAGE) * STAGE * sizeof(double2);
   // inverse: the matrix (nb <= 64) or one panel, then the row / column vectors
   static constexpr size_t INV_MAT = SMEM_INV ? size_t(NB) * NB : size_t(NB) * PW;
-  // after the panel: pivot row + multiplier column + pivot rows of the other
-  // columns, or the register-resident sub-block elimination's scratch
-  static constexpr size_t INV_SCR_A = 2 * size_t(NB) + 8 * size_t(PW);
-  static constexpr size_t INV_SCR_B = 6 * size_t(NB) + 4 * size_t(NB) / 32 + 8;  // register inverse
-  static constexpr size_t INV_SCR = INV_SCR_A > INV_SCR_B ? INV_SCR_A : INV_SCR_B;
+  // inverse scratch after the matrix / panel, per form (complex values):
+  // blocked (nb >= 128): pivot row + multiplier column + 8 pivot rows of the
+  // panel's other columns, which also covers the sub-block elimination's
+  // scratch; register form (nb = 32); one-panel blocked form (nb = 64):
+  // 8 pivot rows of the other columns, or the sub-block scratch
+  static constexpr size_t SCR_SUB = 2 * size_t(NB) + 48 + size_t(NB) / 16;
+  static constexpr size_t SCR_PANEL = 2 * size_t(NB) + 8 * size_t(PW);
+  static constexpr size_t SCR_BLOCKED = SCR_PANEL > SCR_SUB ? SCR_PANEL : SCR_SUB;
+  static constexpr size_t SCR_REG = 6 * size_t(NB) + size_t(NB) / 8 + 8;
+  static constexpr size_t SCR_ONE = 8 * (size_t(NB) - 8) > SCR_SUB ? 8 * (size_t(NB) - 8) : SCR_SUB;
+  static constexpr size_t INV_SCR = !SMEM_INV ? SCR_BLOCKED : (NB == 32 ? SCR_REG : SCR_ONE);
   static constexpr size_t INV_SMEM = (INV_MAT + INV_SCR) * sizeof(double2);
   static constexpr size_t SMEM = GEMM_SMEM > INV_SMEM ? GEMM_SMEM : INV_SMEM;
+  // two CTAs per SM: 2 x (dynamic + static shared memory + 1 KB reserved)
+  // within the SM's 228 KB
+  static_assert(SMEM <= 108 * 1024 + 512, "shared memory for two CTAs per SM");
   static_assert(TM >= 1 && TN >= 1, "tile");
   static_assert(PM % (8 * WARPS_M) == 0 && PN % (8 * WARPS_N) == 0, "tile");
 };
@@ -417,6 +426,105 @@ __device__ __forceinline__ void gj_subblock(double2* panel, int PW, int p0, int 
   __syncthreads();
 }
 
+// Rank-8 update of a panel's other columns after its sub-block sb0.. (pivot
+// rows R = rows p0+sb0.. of those columns, before the update, gathered into
+// rbuf, 8 x (PW - 8)):
+//   X[i, j] = (i in sub-block rows ? 0 : X[i, j]) + sum_t U[i, t] R[t, j]
+// on the FP64 tensor pipe: warp w owns rows 8 TMU w .. (TMU 8-row subtiles)
+// and walks the 8-column subtiles of the other columns; K = 8 is two m8n8k4
+// steps, U's fragments loaded once.  Ends with a barrier.
+template <int NB>
+__device__ __forceinline__ void panel_rank8_update(double2* panel, int PW, int p0, int sb0, double2* rbuf) {
+  constexpr int KB = 8;
+  const int tid = threadIdx.x;
+  const int nrest = PW - KB;
+  if (nrest <= 0) return;
+  for (int e = tid; e < KB * nrest; e += kThreads) {
+    const int t = e % KB, jr = e / KB;
+    const int j = jr < sb0 ? jr : jr + KB;
+    rbuf[t + jr * KB] = panel[(p0 + sb0 + t) + (size_t)j * NB];
+  }
+  __syncthreads();
+  constexpr int TMU = NB / (8 * (kThreads / 32));
+  static_assert(TMU >= 1 && TMU * 8 * (kThreads / 32) == NB, "rows per warp");
+  const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, t4 = lane & 3;
+  const int wm = warp * 8 * TMU;
+  double2 av[2][TMU];
+#pragma unroll
+  for (int ks = 0; ks < 2; ks++)
+#pragma unroll
+    for (int a = 0; a < TMU; a++) av[ks][a] = panel[(wm + 8 * a + g) + (size_t)(sb0 + 4 * ks + t4) * NB];
+  for (int b = 0; b < nrest / 8; b++) {
+    double cr[TMU][1][2], ci[TMU][1][2];
+#pragma unroll
+    for (int a = 0; a < TMU; a++) cr[a][0][0] = cr[a][0][1] = ci[a][0][0] = ci[a][0][1] = 0.0;
+#pragma unroll
+    for (int ks = 0; ks < 2; ks++) {
+      const double2 bv[1] = {rbuf[(4 * ks + t4) + (8 * b + g) * KB]};
+      cmma_step<TMU, 1>(cr, ci, av[ks], bv, 1.0, 1.0);
+    }
+#pragma unroll
+    for (int a = 0; a < TMU; a++)
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const int i = wm + 8 * a + g, jr = 8 * b + 2 * t4 + c;
+        const int j = jr < sb0 ? jr : jr + KB;
+        const bool prow = i >= p0 + sb0 && i < p0 + sb0 + KB;
+        const size_t o = i + (size_t)j * NB;
+        const double2 x = prow ? czero() : panel[o];
+        panel[o] = make_double2(x.x + cr[a][0][c], x.y + ci[a][0][c]);
+      }
+  }
+  __syncthreads();
+}
+
+// Gauss-Jordan inverse (partial pivoting) of the NB x NB block X held whole
+// in shared memory (NB = 64): the blocked form of gj_invert_blocked with one
+// panel, i.e. 8-column sub-blocks eliminated with their elements in
+// registers (gj_subblock) and the other columns updated by rank-8 DMMA
+// products (panel_rank8_update); no trailing matrix.  Then dst[:, j] =
+// X[:, colsrc[j]] undoes the interchanges (and dst2 the same).  scr: shared
+// scratch of max(8 (NB - 8), 2 NB + 48 + NB / 16) complex values.  Returns 1
+// (and zeros dst) on a zero pivot.
+template <int NB>
+__device__ __noinline__ int gj_invert_smem_blocked(double2* X, double2* dst, double2* dst2, SmemInv& s,
+                                                   double2* scr) {
+  constexpr int KB = 8;
+  static_assert(NB % KB == 0, "whole sub-blocks");
+  const int tid = threadIdx.x;
+  if (tid == 0) s.singular = 0;
+  for (int i = tid; i < NB; i += kThreads) s.rmap[i] = (int16_t)i;
+  __syncthreads();
+  for (int sb0 = 0; sb0 < NB; sb0 += KB) {
+    gj_subblock<NB>(X, NB, 0, sb0, scr, s.rmap, s);
+    if (s.singular) break;
+    panel_rank8_update<NB>(X, NB, 0, sb0, scr);
+  }
+  if (s.singular) {
+    for_each_elem(NB, [&](int, int, int idx) {
+      dst[idx] = czero();
+      if (dst2) dst2[idx] = czero();
+    });
+    __syncthreads();
+    return 1;
+  }
+  if (tid == 0) {
+    for (int j = 0; j < NB; j++) s.colsrc[j] = (int16_t)j;
+    for (int k = NB - 1; k >= 0; k--) {
+      const int q = s.perm[k];
+      if (q != k) { const int16_t tmp = s.colsrc[k]; s.colsrc[k] = s.colsrc[q]; s.colsrc[q] = tmp; }
+    }
+  }
+  __syncthreads();
+  for_each_elem(NB, [&](int i, int j, int idx) {
+    const double2 v = X[i + s.colsrc[j] * NB];
+    dst[idx] = v;
+    if (dst2) dst2[idx] = v;
+  });
+  __syncthreads();
+  return 0;
+}
+
 // Blocked Gauss-Jordan inverse of the NB x NB block X0 (global memory, ld
 // NB, destroyed), result into dst (and dst2).  X1: a second global block.
 // The row interchanges of a panel are never applied in place: the panel's
@@ -460,54 +568,9 @@ __device__ int gj_invert_blocked(double2* X0, double2* X1, double2* dst, double2
     static_assert(PWM % KB == 0 && (NB % PWM) % KB == 0, "panels of whole sub-blocks");
     double2* rbuf = fcol + NB;  // KB x PWM pivot rows of the other columns
     for (int sb0 = 0; sb0 < PW && !s.singular; sb0 += KB) {
-      const int kb = KB;
       gj_subblock<NB>(panel, PW, p0, sb0, rowk, rmap, s);
       if (s.singular) break;
-      // rank-KB update of the panel's other columns j (pivot rows R = rows
-      // p0+sb0.. of those columns, before the update):
-      //   X[i, j] = (i in sub-block rows ? 0 : X[i, j]) + sum_t U[i, t] R[t, j]
-      const int nrest = PW - kb;
-      if (nrest > 0) {
-        for (int e = tid; e < kb * nrest; e += kThreads) {
-          const int t = e % kb, jr = e / kb;
-          const int j = jr < sb0 ? jr : jr + kb;
-          rbuf[t + jr * KB] = panel[(p0 + sb0 + t) + (size_t)j * NB];
-        }
-        __syncthreads();
-        // on the FP64 tensor pipe: warp w owns rows 8 TMU w .. (TMU 8-row
-        // subtiles) and walks the 8-column subtiles of the other columns;
-        // K = KB = 8 is two m8n8k4 steps, U's fragments loaded once
-        constexpr int TMU = NB / (8 * (kThreads / 32));
-        const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, t4 = lane & 3;
-        const int wm = warp * 8 * TMU;
-        double2 av[2][TMU];
-#pragma unroll
-        for (int ks = 0; ks < 2; ks++)
-#pragma unroll
-          for (int a = 0; a < TMU; a++) av[ks][a] = panel[(wm + 8 * a + g) + (size_t)(sb0 + 4 * ks + t4) * NB];
-        for (int b = 0; b < nrest / 8; b++) {
-          double cr[TMU][1][2], ci[TMU][1][2];
-#pragma unroll
-          for (int a = 0; a < TMU; a++) cr[a][0][0] = cr[a][0][1] = ci[a][0][0] = ci[a][0][1] = 0.0;
-#pragma unroll
-          for (int ks = 0; ks < 2; ks++) {
-            const double2 bv[1] = {rbuf[(4 * ks + t4) + (8 * b + g) * KB]};
-            cmma_step<TMU, 1>(cr, ci, av[ks], bv, 1.0, 1.0);
-          }
-#pragma unroll
-          for (int a = 0; a < TMU; a++)
-#pragma unroll
-            for (int c = 0; c < 2; c++) {
-              const int i = wm + 8 * a + g, jr = 8 * b + 2 * t4 + c;
-              const int j = jr < sb0 ? jr : jr + KB;
-              const bool prow = i >= p0 + sb0 && i < p0 + sb0 + KB;
-              const size_t o = i + (size_t)j * NB;
-              const double2 x = prow ? czero() : panel[o];
-              panel[o] = make_double2(x.x + cr[a][0][c], x.y + ci[a][0][c]);
-            }
-        }
-        __syncthreads();
-      }
+      panel_rank8_update<NB>(panel, PW, p0, sb0, rbuf);
     }
     if (s.singular) break;
     // the last panel writes the inverse itself: its column j is column
