@@ -215,8 +215,13 @@ def test_c_harness_fortran_calling_convention(rgf, tmp_path):
         compare(g, r, nm, d.H1i)
 
 
-def test_singular_block_reports_status(rgf):
-    nm, nx, E = 8, 3, 0.25
+@pytest.mark.parametrize("nm", [8, 32, 64, 128, 256])
+def test_singular_block_reports_status(rgf, nm):
+    """H = E*I and no coupling: every block to invert is exactly zero, so each
+    inverse form (general nb = 8, registers nb = 32, one shared-memory panel
+    nb = 64, blocked nb = 128 / 256) meets a zero pivot and returns the zero
+    block with the status bit, as the reference's invert fallback."""
+    nx, E = 3, 0.25
     from oracle import oracle as O
     Hii = O.from_blocks(np.broadcast_to(E * np.eye(nm), (nx, nm, nm)).astype(complex))
     H1i = np.zeros_like(Hii)
