@@ -22,8 +22,10 @@
 //     (15 complex products per backward block instead of 22; 9 when
 //     neither `cur` nor GLi1 is requested);
 //   - without scattering Sigma^<, g^<_l = g^L_{l,1} Sigma^<_L g^L_{l,1}^H
-//     from the running column (2 products per forward block instead of 4)
-//     and the last backward G^< term is the conjugate transpose of another;
+//     = i fL V_l V_l^H with V_l = g^L_{l,1} L, Gamma_L = L L^H (pivoted
+//     Cholesky): one product per forward block instead of four, T(E) from
+//     V as well; the last backward G^< term is the conjugate transpose of
+//     another;
 //   - sums, z*I - H - Sigma assembly, Fermi-weighted Sigma^< and the
 //     G^> = G^< + G^R - G^A identity are fused into the product epilogues;
 //   - the traces tr / tre / T form only the diagonal of the final product;
@@ -82,6 +84,8 @@ struct GenericOps {
   __device__ int invert(int n, double2* dst, double2* dst2) {
     return gj_invert(n, X, dst, dst2, inv, rowk, rowk + n);
   }
+  // >= n complex values of shared memory free between block operations
+  __device__ double2* scratch() const { return rowk; }
 };
 
 // nb = 32, 64, 128, 256: shared-memory-staged GEMM; inverse in shared memory
@@ -110,6 +114,8 @@ struct StagedOps {
       return gj_invert_smem_blocked<NB>(X, dst, dst2, inv, dyn + (size_t)NB * NB);
     else return gj_invert_blocked<NB>(X, Rt, dst, dst2, dyn, dyn, inv);
   }
+  // >= NB complex values of shared memory free between block operations
+  __device__ double2* scratch() const { return dyn; }
 };
 
 template <class Ops>
@@ -159,6 +165,70 @@ struct Solver {
                                                      int idx, double2 h) {
     if (S) return csub(cmul(z, S[idx]), h);
     return (i == j) ? make_double2(z.x - h.x, z.y - h.y) : make_double2(-h.x, -h.y);
+  }
+
+  // Cholesky factor of the Hermitian positive semidefinite block G
+  // (destroyed): L with G = L L^H, L in G's own row order (diagonal pivoting
+  // without interchanges: step k takes the largest remaining diagonal entry
+  // as the pivot row, so L is a row permutation of a lower-triangular
+  // factor), columns beyond the rank zero.  The pivoted Cholesky
+  // factorization of LAPACK's xPSTRF, right-looking, with its default stop:
+  // the largest remaining diagonal entry <= n eps times the largest initial
+  // one.  Thread i < n owns row i's diagonal and flags.
+  __device__ void chol_psd(double2* G, double2* L) {
+    const int nn = n, tid = threadIdx.x, warp = tid >> 5;
+    double2* lcol = ops.scratch();
+    const bool own = tid < nn;
+    double d = own ? G[tid + tid * nn].x : 0.0;
+    bool used = !own;
+    double dtol = 0.0;
+    int k = 0;
+    for (; k < nn; k++) {
+      unsigned key = 0u;
+      if (!used) key = d > 0.0 ? (unsigned)((unsigned long long)__double_as_longlong(d) >> 32) + 2u : 1u;
+      const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
+      const unsigned imin = __reduce_min_sync(0xffffffffu, key == kmax ? (unsigned)tid : 0xffffffffu);
+      if ((unsigned)tid == imin) {
+        sm.red.v[warp] = __longlong_as_double((long long)(((unsigned long long)kmax << 32) | imin));
+        sm.red.v[kWarps + warp] = d;
+      }
+      __syncthreads();
+      unsigned long long best = (unsigned long long)__double_as_longlong(sm.red.v[0]);
+      double dp = sm.red.v[kWarps];
+#pragma unroll
+      for (int w = 1; w < kWarps; w++) {
+        const unsigned long long e = (unsigned long long)__double_as_longlong(sm.red.v[w]);
+        const unsigned ek = (unsigned)(e >> 32), bk = (unsigned)(best >> 32);
+        if (ek > bk || (ek == bk && (unsigned)e < (unsigned)best)) { best = e; dp = sm.red.v[kWarps + w]; }
+      }
+      const unsigned bkey = (unsigned)(best >> 32);
+      const int p = (int)(unsigned)best;
+      if (k == 0) dtol = (double)nn * 2.220446049250313e-16 * dp;
+      if (bkey <= 1u || dp <= dtol) break;  // uniform: rank k
+      const double s = sqrt(dp), rs = 1.0 / s;
+      if (own) {
+        double2 l = czero();
+        if (tid == p) {
+          l = make_double2(s, 0.0);
+          used = true;
+        } else if (!used) {
+          const double2 g = G[tid + p * nn];
+          l = make_double2(g.x * rs, g.y * rs);
+          d -= l.x * l.x + l.y * l.y;
+        }
+        L[tid + k * nn] = l;
+        lcol[tid] = tid == p ? czero() : l;  // row and column p are never read again
+      }
+      __syncthreads();
+      for_each_elem(n, [&](int i, int j, int idx) {
+        const double2 a = lcol[i], b = lcol[j];
+        if ((a.x == 0.0 && a.y == 0.0) || (b.x == 0.0 && b.y == 0.0)) return;
+        G[idx] = csub(G[idx], cmul(a, cconj(b)));
+      });
+      __syncthreads();
+    }
+    for (int e = tid; e < (nn - k) * nn; e += kThreads) L[(size_t)k * nn + e] = czero();
+    __syncthreads();
   }
 
   // sancho (green_rgf.f90:4451-4537); S00 = nullptr is the identity (the
@@ -261,26 +331,45 @@ struct Solver {
     double2* sigmal = tmp(T_SIGL);
     gemm_store(H10, false, tmp(T_GS), false, tmp(T_F1));            // A = H10 G00
     gemm_store(tmp(T_F1), false, H10, true, sigmal);                // sigmal = A H10^H
+    const double fl = fermi((E - mul) / (o.boltz * templ));
     {
-      const double fl = fermi((E - mul) / (o.boltz * templ));
       double2* sig = tmp(T_SIG);
+      double2* gam = tmp(T_F3);
       const double2* sl0 = scat(sl, 0, T_SLS);
       const double2* S0 = S_l(0);
       for_each_elem(n, [&](int i, int j, int idx) {
         const double2 s = sigmal[idx], st = cconj(sigmal[j + i * nn]);
-        double2 v = cscale(csub(s, st), -fl);
-        if (sl0) v = cadd(v, sl0[idx]);
-        sig[idx] = v;
+        const double2 w = csub(s, st);
+        if (ballistic) {
+          gam[idx] = make_double2(-w.y, w.x);                         // Gamma_L = i (sL - sL^H)
+        } else {
+          double2 v = cscale(w, -fl);
+          if (sl0) v = cadd(v, sl0[idx]);
+          sig[idx] = v;
+        }
         X[idx] = csub(zs_minus(z, S0, i, j, idx, H00[idx]), s);      // A = z S00 - H00 - sigmal
       });
       __syncthreads();
     }
     invert_X(Gl(0));
-    gemm_store(Gl(0), false, tmp(T_SIG), false, tmp(T_F2));         // B = A sig
-    gemm_store(tmp(T_F2), false, Gl(0), true, Gln(0));              // Gln(1) = B A^H
     const double2* GN1 = Gl(0);
     double2* GN1buf[2] = {tmp(T_GN1A), tmp(T_GN1B)};
     int gsel = 0;
+    if (ballistic) {
+      // sig<_L = -(sL - sL^H) fL = i fL Gamma_L with Gamma_L = L L^H, so every
+      // left-connected g<_l = g^L_{l,1} sig<_L g^L_{l,1}^H is i fL V_l V_l^H
+      // for the running column V_l = g^L_{l,1} L: one product per block
+      chol_psd(tmp(T_F3), tmp(T_SIG));
+      gemm_store(Gl(0), false, tmp(T_SIG), false, GN1buf[gsel]);   // V_1 = g_1 L
+      GN1 = GN1buf[gsel];
+      gsel ^= 1;
+      gemm(GN1, false, GN1, true, [&](int i, int j, double2 v) {      // Gln(1) = i fL V V^H
+        Gln(0)[i + j * nn] = make_double2(-v.y * fl, v.x * fl);
+      });
+    } else {
+      gemm_store(Gl(0), false, tmp(T_SIG), false, tmp(T_F2));       // B = A sig
+      gemm_store(tmp(T_F2), false, Gl(0), true, Gln(0));            // Gln(1) = B A^H
+    }
 
     // ------------------------------------------------ forward sweep
     for (int l = 1; l <= nx - 2; l++) {
@@ -296,7 +385,7 @@ struct Solver {
         X[idx] = csub(zs_minus(z, Sl, i, j, idx, h), v);
       });
       invert_X(Gl(l));
-      if (want_T || ballistic) {                                    // g^L_{l,1} = g_l H_{l,l-1} g^L_{l-1,1}
+      if (want_T || ballistic) {  // g^L_{l,1} = g_l H_{l,l-1} g^L_{l-1,1} (ballistic: times L)
         gemm_store(H, false, GN1, false, tmp(T_F1));
         gemm_store(Gl(l), false, tmp(T_F1), false, GN1buf[gsel]);
         GN1 = GN1buf[gsel];
@@ -304,11 +393,11 @@ struct Solver {
       }
       if (ballistic) {
         // Without scattering the recursion g<_l = g_l H g<_{l-1} H^H g_l^H
-        // unrolls to g<_l = g^L_{l,1} sig<_L (g^L_{l,1})^H: two products on
-        // the running column instead of four (sig<_L stays in T_SIG until
-        // the right contact).
-        gemm_store(GN1, false, tmp(T_SIG), false, tmp(T_F2));        // B = g^L_{l,1} sig<_L
-        gemm_store(tmp(T_F2), false, GN1, true, Gln(l));             // Gln(l) = B g^L_{l,1}^H
+        // unrolls to g<_l = g^L_{l,1} sig<_L (g^L_{l,1})^H = i fL V_l V_l^H:
+        // one product on the running column instead of four.
+        gemm(GN1, false, GN1, true, [&](int i, int j, double2 v) {    // Gln(l) = i fL V V^H
+          Gln(l)[i + j * nn] = make_double2(-v.y * fl, v.x * fl);
+        });
       } else {
         gemm_store(H, false, Gln(l - 1), false, tmp(T_F2));         // B = H10 Gln(l-1)
         gemm(tmp(T_F2), false, H, true, [&](int i, int j, double2 v) { // C = B H10^H + sig<
@@ -393,8 +482,8 @@ struct Solver {
       if (tk.tr && threadIdx.x == 0) *tk.tr = -s;
     }
     if (want_T) {
-      gemm_store(H, false, GN1, false, tmp(T_X1));                  // H_{N,N-1} g^L_{N-1,1}
-      gemm_store(G00, false, tmp(T_X1), false, tmp(T_X2));          // G_{N1}
+      gemm_store(H, false, GN1, false, tmp(T_X1));                  // H_{N,N-1} g^L_{N-1,1} (L)
+      gemm_store(G00, false, tmp(T_X1), false, tmp(T_X2));          // G_{N1} (L)
       for_each_elem(n, [&](int i, int j, int idx) {                 // Gamma = i (Sigma - Sigma^H)
         const double2 dl = csub(sigmal[idx], cconj(sigmal[j + i * nn]));
         const double2 dr = csub(sigmar[idx], cconj(sigmar[j + i * nn]));
@@ -402,10 +491,21 @@ struct Solver {
         tmp(T_GAMR)[idx] = make_double2(-dr.y, dr.x);
       });
       __syncthreads();
-      gemm_store(tmp(T_GAMR), false, tmp(T_X2), false, tmp(T_Y));   // Gamma_R G_N1
-      gemm_store(tmp(T_GAML), false, tmp(T_X2), true, tmp(T_Z));    // Gamma_L G_N1^H
-      const double2 tt = trace_prod(n, tmp(T_Y), tmp(T_Z), sm.red);
-      if (threadIdx.x == 0) *tk.T = tt.x;
+      gemm_store(tmp(T_GAMR), false, tmp(T_X2), false, tmp(T_Y));   // Gamma_R G_N1 (L)
+      if (ballistic) {
+        // X2 = G_N1 L: T = Tr[Gamma_R X2 X2^H] = sum_ij Re (Gamma_R X2)_ij conj(X2_ij)
+        double acc = 0.0;
+        for_each_elem(n, [&](int, int, int idx) {
+          const double2 y = tmp(T_Y)[idx], x = tmp(T_X2)[idx];
+          acc += y.x * x.x + y.y * x.y;
+        });
+        const double tt = block_sum2(make_double2(acc, 0.0), sm.red).x;
+        if (threadIdx.x == 0) *tk.T = tt;
+      } else {
+        gemm_store(tmp(T_GAML), false, tmp(T_X2), true, tmp(T_Z));  // Gamma_L G_N1^H
+        const double2 tt = trace_prod(n, tmp(T_Y), tmp(T_Z), sm.red);
+        if (threadIdx.x == 0) *tk.T = tt.x;
+      }
     }
 
     // ------------------------------------------------ backward sweep
