@@ -39,13 +39,17 @@ int err(int code, const char* msg) {
   return code;
 }
 
-bool on_device(const void* p) {
+// Device memory of GPU `dev` (managed memory is reachable from every GPU);
+// an array on another GPU would be read through a peer address, which
+// faults without peer access.
+bool on_device(const void* p, int dev) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -72,9 +76,13 @@ extern "C" int rgf_solve_energies_noalloc(const rgf_opts* opts, const rgf_device
   const void* arrays[] = {device->Hii, device->H1i, device->Sii, sigma_lesser, sigma_r, ldos, ndens,
                           pdens, GRi1, cur, tr, tre, T};
   if (!device->Hii || !device->H1i) return err(RGF_E_ARG, "Hii / H1i is NULL");
+  int cur_dev = -1;
+  if (cudaGetDevice(&cur_dev) != cudaSuccess) return err(RGF_E_CUDA, "cudaGetDevice failed");
+  if (opts->device != cur_dev) return err(RGF_E_ARG, "opts.device must be the current CUDA device");
   for (const void* a : arrays)
-    if (a && !on_device(a))
-      return err(RGF_E_ARG, "every array must be device memory (host arrays would need staging buffers)");
+    if (a && !on_device(a, cur_dev))
+      return err(RGF_E_ARG, "every array must be device memory of the current device (host arrays would "
+                            "need staging buffers)");
 
   // scratch layout: queue | device | tasks | status | order | per-CTA slots
   const size_t off_dev = 256;

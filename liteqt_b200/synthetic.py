@@ -144,3 +144,44 @@ def energy_grid(nen: int, emin: float = -3.0, emax: float = 3.0) -> np.ndarray:
 
 def temperature_for_kT(kT: float, boltz: float = 8.61734e-05) -> float:
     return kT / boltz
+
+
+def lead_band_edges(Hii: np.ndarray, H1i: np.ndarray, block: int = 0, nk: int = 512) -> np.ndarray:
+    """Subband edges (eV) of the semi-infinite lead that continues block
+    ``block`` of a device (Hii, H1i in the Fortran block layout): the extrema
+    over k of every eigenvalue band of the Bloch Hamiltonian
+    H(k) = H00 + T e^{ik} + T^H e^{-ik}, with H00 the block and T its coupling
+    H1i(:,:,block+1).  Bands are sampled on nk points of [-pi, pi) and each
+    extremum is refined by the parabola through its sample and the two
+    neighbours.  Returns the sorted band minima and maxima."""
+    H00 = np.asarray(Hii[block]).T
+    T = np.asarray(H1i[block]).T
+    k = -np.pi + 2.0 * np.pi * np.arange(nk) / nk
+    ev = np.empty((nk, H00.shape[0]))
+    for i, kk in enumerate(k):
+        Hk = H00 + T * np.exp(1j * kk) + T.conj().T * np.exp(-1j * kk)
+        ev[i] = np.linalg.eigvalsh(0.5 * (Hk + Hk.conj().T))
+    edges = []
+    for n in range(ev.shape[1]):
+        band = ev[:, n]
+        for i0 in (int(np.argmin(band)), int(np.argmax(band))):
+            y0, y1, y2 = band[(i0 - 1) % nk], band[i0], band[(i0 + 1) % nk]
+            den = y0 - 2.0 * y1 + y2
+            edges.append(y1 - 0.125 * (y2 - y0) ** 2 / den if den != 0.0 else y1)
+    return np.sort(np.array(edges))
+
+
+def band_edge_energy_grid(nen: int, edges: np.ndarray, emin: float = -3.0, emax: float = 3.0,
+                          frac: float = 0.1, width: float = 1e-3, seed: int = 5) -> np.ndarray:
+    """Energies for the band-edge workload: round(frac*nen) points placed
+    within `width` eV of band edges in [emin, emax] (edges drawn uniformly
+    with replacement, offsets uniform in [-width, width]), the rest on the
+    uniform liteQT grid of [emin, emax]; sorted."""
+    rng = np.random.default_rng(seed)
+    n_edge = int(round(frac * nen))
+    inside = edges[(edges > emin + width) & (edges < emax - width)]
+    grid = energy_grid(nen - n_edge, emin, emax)
+    if n_edge == 0 or inside.size == 0:
+        return energy_grid(nen, emin, emax)
+    near = rng.choice(inside, n_edge) + rng.uniform(-width, width, n_edge)
+    return np.sort(np.concatenate([grid, near]))

@@ -59,15 +59,21 @@ def rel_err(a, b, scale=None):
 # GPU-vs-oracle parity rule (the FP64 tolerance and the noise-floor fallback
 # are explained in test_gpu_parity.py's module docstring).
 def errors(g, r, nm, H1i, skip_last_gri1=True):
+    """Per-output relative errors of g against r; outputs absent from g
+    (not requested from the GPU) are skipped."""
     errs = {}
     errs["ldos"] = rel_err(g["ldos"], r["ldos"])
     errs["ndens"] = rel_err(g["ndens"], r["ndens"])
-    errs["pdens"] = rel_err(g["pdens"], r["pdens"], scale=max(np.max(np.abs(r["ldos"])),
-                                                                np.max(np.abs(r["ndens"]))))
+    if g.get("pdens") is not None:
+        errs["pdens"] = rel_err(g["pdens"], r["pdens"], scale=max(np.max(np.abs(r["ldos"])),
+                                                                    np.max(np.abs(r["ndens"]))))
     sl = slice(0, -1) if skip_last_gri1 else slice(None)
-    errs["GRi1"] = rel_err(g["GRi1"][:, sl], r["GRi1"][:, sl])
-    cur_scale = nm * np.max(np.abs(H1i)) * np.max(np.abs(r["ndens"]))
-    errs["cur"] = rel_err(g["cur"], r["cur"], scale=cur_scale)
+    for k in ("GRi1", "GLi1", "GGi1"):
+        if g.get(k) is not None:
+            errs[k] = rel_err(g[k][:, sl], r[k][:, sl])
+    if g.get("cur") is not None:
+        cur_scale = nm * np.max(np.abs(H1i)) * np.max(np.abs(r["ndens"]))
+        errs["cur"] = rel_err(g["cur"], r["cur"], scale=cur_scale)
     trs = max(np.max(np.abs(r["tr"])), np.max(np.abs(r["tre"])), np.max(np.abs(r["T"])), 1e-300)
     errs["tr"] = float(np.max(np.abs(g["tr"] - r["tr"])) / trs)
     errs["tre"] = float(np.max(np.abs(g["tre"] - r["tre"])) / trs)
@@ -92,6 +98,27 @@ def compare(g, r, nm, H1i, tol=1e-10, truth=None, skip_last_gri1=True, floor=())
            if not (e_go[k] <= tol or e_gt[k] <= 8.0 * e_rt[k] + 1e-12) or not e_gt[k] < 1e-6}
     assert not bad, f"(gpu-oracle, gpu-exact, oracle-exact) failing: {bad}"
     return e_go
+
+
+def compare_spread(g, r, floors, nm, H1i, tol=1e-10, factor=8.0, skip_last_gri1=True):
+    """Parity rule for the full-size configurations, where the 80-bit
+    evaluation takes minutes: every output within `tol` of the FP64 oracle r,
+    or within `factor` times the FP64 spread of the problem -- the largest
+    distance between r and the FP64 oracle run on inputs perturbed by one
+    rounding (floors).  The spread is the problem's own conditioning: a
+    200-block disordered chain near a resonance moves its G^R by 1e-4
+    (relative) under one rounding of the input, so no absolute cap applies.
+    Returns the errors and the spread."""
+    e_go = errors(g, r, nm, H1i, skip_last_gri1)
+    spread = {k: 0.0 for k in e_go}
+    for f in floors:
+        e_f = errors({k: f[k] for k in f if k in g or k in ("tr", "tre", "T")}, r, nm, H1i,
+                     skip_last_gri1)
+        spread = {k: max(spread[k], e_f.get(k, 0.0)) for k in spread}
+    bad = {k: (e_go[k], spread[k]) for k in e_go
+           if not (e_go[k] <= tol or e_go[k] <= factor * spread[k] + 1e-12)}
+    assert not bad, f"(gpu-oracle, fp64 spread) failing: {bad}"
+    return e_go, spread
 
 
 

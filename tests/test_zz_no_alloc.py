@@ -124,3 +124,27 @@ def test_no_alloc_rejects_oversized_problem_and_host_arrays(lib):
                                         *([None] * 12))
     assert rc == rgf.RGF_E_ARG
     assert "device memory" in lib.rgf_noalloc_last_error().decode()
+
+
+def test_no_alloc_nb128_matches_allocating_entry_point(lib):
+    """nb = 128 with a chain of 24 blocks: one solver slot is 15 MB, so the
+    256 MiB scratch holds 16 slots and the launch runs 16 CTAs; the results
+    must still equal the allocating entry point's."""
+    import torch
+    from liteqt_b200 import rgf
+    nm, nx, nen = 128, 24, 20
+    opts = rgf.Options(eta_dev=1e-5, eta_lead=1e-5)
+    d, Hii, H1i, E = _device_problem(nm, nx, nen, 21, -2.5, 2.5)
+    ref = _outputs(nen, nx, nm)
+    with rgf.Context(opts) as ctx:
+        ctx.solve_energies(Hii, H1i, E, MU, (S.temperature_for_kT(0.025),) * 2, ldos=ref["ldos"],
+                           ndens=ref["ndens"], tr=ref["tr"], T=ref["T"])
+    got = _outputs(nen, nx, nm)
+    rc, info = _call_noalloc(lib, opts, nm, nx, Hii, H1i, E, got)
+    assert rc == 0, lib.rgf_noalloc_last_error().decode()
+    assert np.all(info["status"] == 0)
+    torch.cuda.synchronize()
+    for k in ("ldos", "ndens", "T", "tr"):
+        a = got[k].cpu().numpy()
+        b = ref[k].cpu().numpy()
+        assert _rel(a, b) <= TOL, (k, _rel(a, b))
