@@ -51,7 +51,11 @@ def parse():
     p.add_argument("--nb", type=int, default=128)
     p.add_argument("--nx", type=int, default=100)
     p.add_argument("--nen", type=int, default=296, help="energies per GPU per step")
-    p.add_argument("--precision", choices=["fp64"], default="fp64")
+    p.add_argument("--precision", choices=["fp64", "mixed"], default="mixed",
+                   help="mixed (default): the chosen form, split-integer block products on the int8 "
+                        "tensor cores with refined FP32 inverses (nb = 128); fp64: the plain drop-in form")
+    p.add_argument("--no-plain", action="store_true",
+                   help="with --precision mixed: skip timing the plain FP64 form beside it")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-threads", type=int, default=0)
@@ -160,6 +164,16 @@ def zgemm_peak_tflops(torch, dev):
     return 8.0 * 4096 ** 3 / (best * 1e-3) / 1e12
 
 
+def int8_peak_tops():
+    """Dense int8 tensor peak: twice the measured dense bf16 burst (the
+    B200's int8 MMA rate is twice its bf16 rate per clock)."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    bf16 = 1590.0   # the recipe's fallback when the measured file is absent
+    if os.path.exists(path):
+        bf16 = float(json.load(open(path)).get("bf16_tflops", bf16))
+    return 2.0 * bf16
+
+
 def traffic_from_profiles(args):
     """Per-task DRAM bytes of the solver kernel from the committed ncu summary,
     scaled to a launch of --nen tasks (None if no summary exists)."""
@@ -254,7 +268,9 @@ def run_ours(args):
     d, E_all, temp = workload(args, world)
     E = np.ascontiguousarray(E_all[rank * args.nen:(rank + 1) * args.nen])
     nen, nx, nb = args.nen, args.nx, args.nb
-    opts = rgf.Options(device=local, eta_dev=ETA, eta_lead=ETA)
+    mixed = args.precision == "mixed"
+    opts = rgf.Options(device=local, eta_dev=ETA, eta_lead=ETA,
+                       precision=rgf.RGF_PREC_MIXED if mixed else rgf.RGF_PREC_FP64)
     ctx = rgf.Context(opts)
     stream = torch.cuda.Stream(device=dev)
     sh = stream.cuda_stream
@@ -289,6 +305,7 @@ def run_ours(args):
     step_ms = []
     kern_ms = []
     flops = []
+    int8_ops = []
     with torch.cuda.stream(stream):
         for _ in range(args.steps):
             flush.fill_(1.0)
@@ -302,9 +319,12 @@ def run_ours(args):
             st = ctx.stats()
             kern_ms.append(st["last_kernel_ms"])
             flops.append(st["last_flops"])
+            int8_ops.append(st["last_int8_ops"])
     barrier()
     clk = clocks.stop()
     launches = ctx.stats()["launches"] - launches0
+
+
     t_dev = sum(step_ms) / 1e3
     if world > 1:
         tt = torch.tensor([t_dev], dtype=torch.float64, device=dev)
@@ -324,14 +344,35 @@ def run_ours(args):
     alg_flops = float(np.sum(8.0 * nb ** 3 * ((28 * nx - 18 + 6 * nsum) + (nx + 4 + nsum))))
     kern_s = float(np.mean(kern_ms)) * 1e-3
     achieved = alg_flops / kern_s / 1e12
-    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": traffic_from_profiles(args),
-                "peak_source": "cuBLAS ZGEMM 4096^3 measured live on this GPU (FP64 tensor pipe; "
-                               "MEASURED_PEAKS.json holds no FP64 figure)",
-                "algorithmic_flops_per_launch": alg_flops, "kernel_ms": 1e3 * kern_s,
-                "executed_flops_per_launch": float(np.mean(flops)),
-                "executed_tflops": float(np.mean(flops)) / kern_s / 1e12,
-                "executed_frac": float(np.mean(flops)) / kern_s / 1e12 / peak}
+    fp64_exec = float(np.mean(flops))
+    if not mixed:
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak, "traffic": traffic_from_profiles(args),
+                    "peak_source": "cuBLAS ZGEMM 4096^3 measured live on this GPU (FP64 tensor pipe; "
+                                   "MEASURED_PEAKS.json holds no FP64 figure)",
+                    "algorithmic_flops_per_launch": alg_flops, "kernel_ms": 1e3 * kern_s,
+                    "executed_flops_per_launch": fp64_exec,
+                    "executed_tflops": fp64_exec / kern_s / 1e12,
+                    "executed_frac": fp64_exec / kern_s / 1e12 / peak}
+    else:
+        # The mixed form's kernel runs two tensor pipes: int8 for the split-
+        # integer products, FP64 DMMA for the lead decimation and the FP64
+        # fallbacks.  Its roofline time is the sum of the two executed works
+        # at their peaks; `peak` is the algorithmic rate the kernel would
+        # reach in that time, so frac = (t_int8 + t_fp64) at peak / t_kernel.
+        i8 = float(np.mean(int8_ops))
+        i8_peak = int8_peak_tops()
+        t_min = i8 / (i8_peak * 1e12) + fp64_exec / (peak * 1e12)
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": alg_flops / t_min / 1e12,
+                    "unit": "TFLOP/s", "frac": t_min / kern_s, "traffic": traffic_from_profiles(args),
+                    "peak_source": "int8 tensor: 2 x the measured dense bf16 burst of MEASURED_PEAKS.json "
+                                   "(the B200 int8 rate is twice bf16 per clock); FP64 tensor: cuBLAS ZGEMM "
+                                   "4096^3 measured live",
+                    "algorithmic_flops_per_launch": alg_flops, "kernel_ms": 1e3 * kern_s,
+                    "int8_ops_per_launch": i8, "int8_tops": i8 / kern_s / 1e12, "int8_peak_tops": i8_peak,
+                    "int8_frac": i8 / kern_s / 1e12 / i8_peak,
+                    "fp64_flops_per_launch": fp64_exec, "fp64_tflops": fp64_exec / kern_s / 1e12,
+                    "fp64_peak_tflops": peak, "fp64_frac": fp64_exec / kern_s / 1e12 / peak}
 
     # ---- end to end through the C ABI with pinned host buffers
     e2e = None
@@ -371,6 +412,37 @@ def run_ours(args):
         # parity spot check of the e2e outputs against the device-resident run
         assert np.array_equal(arrs["T"], T.cpu().numpy())
 
+    # the plain FP64 form on the same workload and timing, for the ratio the
+    # metric names (mixed vs plain)
+    plain = None
+    if mixed and not args.no_plain:
+        ctx64 = rgf.Context(rgf.Options(device=local, eta_dev=ETA, eta_lead=ETA))
+        with torch.cuda.stream(stream):
+            for _ in range(max(1, args.warmup)):
+                ctx64.solve_energies(Hii, H1i, E, MU, temp, ldos=ldos, ndens=ndens, tr=tr, tre=tre, T=T,
+                                     stream=sh)
+            torch.cuda.synchronize(dev)
+            pms = []
+            for _ in range(args.steps):
+                flush.fill_(1.0)
+                s = torch.cuda.Event(enable_timing=True)
+                e = torch.cuda.Event(enable_timing=True)
+                s.record(stream)
+                ctx64.solve_energies(Hii, H1i, E, MU, temp, ldos=ldos, ndens=ndens, tr=tr, tre=tre, T=T,
+                                     stream=sh)
+                e.record(stream)
+                e.synchronize()
+                pms.append(s.elapsed_time(e))
+        ctx64.close()
+        t_plain = sum(pms) / 1e3
+        if world > 1:
+            tt = torch.tensor([t_plain], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t_plain = float(tt.item())
+        plain = {"value": nen * world * args.steps / t_plain, "unit": UNIT,
+                 "ms_per_step": 1e3 * t_plain / args.steps,
+                 "form": "plain FP64 (RGF_PREC_FP64), same workload, timing and outputs"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args, d, E, temp, host_threads(args))
@@ -378,9 +450,13 @@ def run_ours(args):
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 * t_dev / args.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "int8 tensor products + f64" if mixed else "f64",
                 "data": "synthetic", "config": config(args, world), "roofline": roofline,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk}
+        if plain is not None:
+            line["plain_fp64"] = plain
+            line["mixed_vs_plain"] = value / plain["value"]
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

@@ -60,11 +60,17 @@ typedef struct rgf_c16 { double re, im; } rgf_c16;
 #define RGF_ST_SINGULAR    1   /* a block inverse hit a zero pivot; block set to 0 (compat) */
 #define RGF_ST_SANCHO_NC   2   /* Sancho-Rubio hit nmax; lead self-energy dropped (compat) */
 #define RGF_ST_BAD_TASK    4   /* task descriptor rejected on the device */
-#define RGF_ST_REFINE_NC   8   /* mixed precision: refinement did not converge */
+#define RGF_ST_REFINE_NC   8   /* mixed precision, informational: a refined inverse did not converge
+                                  and that block was inverted in FP64 instead (results unaffected;
+                                  not an error: RGF_E_STATUS ignores this bit) */
+#define RGF_ST_TIMEOUT    16   /* mixed precision: a bounded tensor-core wait gave up; the task's
+                                  outputs are invalid and its CTA stopped */
 
 /* precision modes */
 #define RGF_PREC_FP64  0       /* complex FP64 throughout: the drop-in */
-#define RGF_PREC_MIXED 1       /* split-precision GEMMs on tcgen05 with FP64 refinement */
+#define RGF_PREC_MIXED 1       /* nb = 128: split-integer block products on the int8 tensor cores
+                                  (tcgen05), FP32 inverses refined against FP64 residuals;
+                                  Sancho-Rubio and the lead self-energies in FP64 */
 
 typedef struct rgf_opts {
   int32_t struct_size;     /* sizeof(rgf_opts); filled by rgf_opts_default */
@@ -133,18 +139,22 @@ typedef struct rgf_task_info {
   int32_t status;          /* RGF_ST_* bits */
   int32_t sancho_iters_left;
   int32_t sancho_iters_right;
-  int32_t n_gemm;          /* nb^3 complex products executed */
-  int32_t n_inv;           /* nb x nb inversions executed */
-  int32_t reserved;
+  int32_t n_gemm;          /* nb^3 complex products executed in FP64 */
+  int32_t n_inv;           /* nb x nb inversions executed in FP64 */
+  int32_t mixed_pairs;     /* RGF_PREC_MIXED: digit-pair products of the split-integer form
+                              (products and refinement steps; each is 4 real nb^3 int8
+                              products on the tensor cores) */
 } rgf_task_info;
 
 /* Measurements of the last rgf_solve_batch on a context. */
 typedef struct rgf_stats {
   double last_kernel_ms;   /* device time of its solver launches (CUDA events on its stream) */
-  double last_flops;       /* executed real flops: 8 nb^3 (n_gemm + n_inv) summed over tasks */
+  double last_flops;       /* executed FP64 real flops: 8 nb^3 (n_gemm + n_inv) summed over tasks */
   int64_t last_tasks;      /* tasks in it */
   int64_t launches;        /* solver kernel launches since the context was created */
-  int64_t reserved[4];
+  double last_int8_ops;    /* RGF_PREC_MIXED: int8 tensor-core operations (2 per multiply-add) of
+                              the split-integer products: 8 nb^3 per digit pair */
+  int64_t reserved[3];
 } rgf_stats;
 
 /* Options with the reference's behaviour (compat mode). */
@@ -374,10 +384,17 @@ RGF_API int rgf_calc_n_electron(rgf_ctx* ctx, const rgf_c16* G_lesser, const rgf
  *     memory; there is no context: options come per call, `stream` is a
  *     cudaStream_t (NULL = the default stream), and the call returns when the
  *     results are written;
+ *   - every array must be on the current device, which must be opts->device;
  *   - its workspace is a fixed 256 MiB array inside the library, reserved on
  *     every GPU that loads the library until the process exits; problems
  *     whose one solver slot plus task tables exceed it ((2 nx + 32) nm^2 * 16
  *     bytes + about 200 bytes per energy) are rejected with RGF_E_ARG;
+ *   - the array holds as many solver slots as fit, and one CTA runs per slot:
+ *     floor((256 MiB - tables) / ((2 nx + 32) nm^2 * 16 B)) of them, at most
+ *     2 per SM.  Small problems run on most of the GPU (nm = 32, nx = 50:
+ *     2.2 MB a slot, 124 CTAs); large ones on few SMs (nm = 128, nx = 100:
+ *     61 MB a slot, 4 CTAs, about 1/70 of rgf_solve_energies' throughput on
+ *     a 148-SM B200);
  *   - the first call on a device looks up the array's device address
  *     (cudaGetSymbolAddress) with that device current, so make that first
  *     call before any stream capture;
@@ -458,6 +475,28 @@ RGF_API int rgf_read_ham_dat(const char* path, const int32_t* axis, rgf_ham_info
 
 /* Last error message of the calling thread ("" if none). */
 RGF_API const char* rgf_last_error(void);
+
+/* Batched block operations of either precision form on device arrays of
+ * `count` nb x nb complex(8) column-major blocks (no counterpart in the
+ * reference; the building blocks of the solver, exposed for callers that
+ * assemble their own recursions and for accuracy checks of the mixed form).
+ * rgf_block_product: C_b = op(A_b) op(B_b), op = conjugate transpose when
+ *   conj_a / conj_b is non-zero; nb = 128.  RGF_PREC_MIXED: the split-integer
+ *   product on the int8 tensor cores (absolute error below about
+ *   2^-44 nb max_k |op(A)_ik| max_k |op(B)_kj|: operands are scaled per row of
+ *   op(A) and per column of op(B)); RGF_PREC_FP64: the FP64 DMMA product.
+ * rgf_block_inverse: Xinv_b = X_b^-1.  RGF_PREC_FP64 (nb = 32, 64, 128): the
+ *   Gauss-Jordan inverse of the plain form (partial pivoting; a zero pivot
+ *   gives the zero block and RGF_ST_SINGULAR); RGF_PREC_MIXED (nb = 128): the
+ *   FP32 inverse refined by Newton-Schulz steps against FP64 residuals
+ *   (RGF_ST_REFINE_NC when a block fell back to the FP64 inverse).
+ *   status (host, count entries) may be NULL.
+ * Both return after the results are written (on `stream`, NULL = the
+ * context's). */
+RGF_API int rgf_block_product(rgf_ctx* ctx, int32_t precision, int64_t nb, int64_t count, const rgf_c16* A,
+                            int32_t conj_a, const rgf_c16* B, int32_t conj_b, rgf_c16* C, void* stream);
+RGF_API int rgf_block_inverse(rgf_ctx* ctx, int32_t precision, int64_t nb, int64_t count, const rgf_c16* X,
+                           rgf_c16* Xinv, int32_t* status, void* stream);
 
 /* Library version string. */
 RGF_API const char* rgf_version(void);

@@ -32,6 +32,12 @@ NVCC_FLAGS = [
 ]
 
 
+# Units whose kernels run one CTA per SM (their __launch_bounds__ give them up
+# to 255 registers a thread): the mixed-precision form holds a 128 x 128 FP32
+# matrix in registers during its inverse.
+ONE_CTA_PER_SM = {"rgf_mixed.cu"}
+
+
 def nvcc() -> str:
     for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
         if c and os.path.exists(c):
@@ -64,7 +70,10 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         obj = os.path.join(BUILD_DIR, os.path.basename(src) + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + hdrs):
-            cmd = [nvcc(), *NVCC_FLAGS, "-c", src, "-o", obj]
+            flags = list(NVCC_FLAGS)
+            if os.path.basename(src) in ONE_CTA_PER_SM:
+                flags.remove("-maxrregcount=128")
+            cmd = [nvcc(), *flags, "-c", src, "-o", obj]
             if ptxas_info:
                 cmd.insert(1, "-Xptxas=-v")
             jobs.append(cmd)

@@ -349,8 +349,7 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
     return fail(RGF_E_ARG, "invalid task list");
   if (n_tasks == 0) return RGF_OK;
   if (n_tasks > (int64_t)INT32_MAX) return fail(RGF_E_ARG, "too many tasks in one batch");
-  if (c->opts.precision != RGF_PREC_FP64)
-    return fail(RGF_E_UNSUPPORTED, "precision mode %d is not available in this build", c->opts.precision);
+  const bool mixed = c->opts.precision == RGF_PREC_MIXED;
   RGF_CUDA(cudaSetDevice(c->device));
   cudaStream_t st = stream_ ? (cudaStream_t)stream_ : c->stream;
   const bool want_T = c->opts.want_T != 0;
@@ -358,6 +357,15 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
   // ---- validate
   int rc = validate_batch(devices, n_devices, tasks, n_tasks);
   if (rc) return rc;
+  if (mixed)
+    for (int32_t d = 0; d < n_devices; d++) {
+      if (devices[d].nm != 128)
+        return fail(RGF_E_UNSUPPORTED, "RGF_PREC_MIXED: device %d has nm=%lld; the mixed form is built for nm=128",
+                    d, (long long)devices[d].nm);
+      if (devices[d].Sii)
+        return fail(RGF_E_UNSUPPORTED, "RGF_PREC_MIXED: device %d has overlap blocks (green_RGF_CMS runs in FP64 "
+                    "only)", d);
+    }
 
   // ---- staging of host arrays
   Stage sg;
@@ -433,9 +441,15 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
   // tasks first, so the launch ends on its shortest tasks
   const LaunchShape shape = launch_shape(c, devices, tasks, n_tasks);
   const std::vector<int32_t>& order = shape.order;
-  const int64_t slot = shape.slot;
+  int64_t slot = shape.slot;
   const size_t smem = shape.smem;
   int grid = c->sm_count * launch_ctas_per_sm(c, smem, shape.nb_mask);
+  if (mixed) {
+    int64_t nx_max = 2;
+    for (int32_t d = 0; d < n_devices; d++) nx_max = std::max<int64_t>(nx_max, devices[d].nx);
+    slot = mixed_slot_elems(nx_max);
+    grid = c->sm_count;   // one CTA per SM
+  }
   if ((int64_t)grid > n_tasks) grid = (int)n_tasks;
   if ((rc = c->work.reserve(sizeof(double2) * (size_t)slot * grid))) return rc;
   if ((rc = c->devs.reserve(sizeof(DDev) * n_devices))) return rc;
@@ -459,7 +473,7 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
   p.slot_elems = slot;
   p.info = (DInfo*)c->info.p;
   RGF_CUDA(cudaEventRecord(c->ev0, st));
-  cudaError_t e = launch_solver(p, grid, smem, st);
+  cudaError_t e = mixed ? launch_mixed(p, grid, st) : launch_solver(p, grid, smem, st);
   if (e != cudaSuccess) return fail(RGF_E_CUDA, "solver launch failed: %s", cudaGetErrorString(e));
   c->stats.launches++;
   RGF_CUDA(cudaEventRecord(c->ev1, st));
@@ -472,16 +486,18 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
   RGF_CUDA(cudaMemcpyAsync(hinfo.data(), c->info.p, sizeof(DInfo) * n_tasks, cudaMemcpyDeviceToHost, st));
   RGF_CUDA(cudaStreamSynchronize(st));
   int worst = 0;
-  double flops = 0.0;
+  double flops = 0.0, int8_ops = 0.0;
   for (int64_t t = 0; t < n_tasks; t++) {
     worst |= hinfo[t].status;
     const double nb = (double)devices[tasks[t].device].nm;
     flops += 8.0 * nb * nb * nb * (double)(hinfo[t].n_gemm + hinfo[t].n_inv);
+    int8_ops += 8.0 * nb * nb * nb * (double)hinfo[t].pad;   // 4 real nb^3 products per digit pair
   }
   float kms = 0.0f;
   RGF_CUDA(cudaEventElapsedTime(&kms, c->ev0, c->ev1));
   c->stats.last_kernel_ms = kms;
   c->stats.last_flops = flops;
+  c->stats.last_int8_ops = int8_ops;
   c->stats.last_tasks = n_tasks;
   if (info) std::memcpy(info, hinfo.data(), sizeof(DInfo) * n_tasks);
   if (c->opts.verbose && worst) {
@@ -493,7 +509,72 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
     }
   }
   if (worst & RGF_ST_BAD_TASK) return fail(RGF_E_ARG, "a task was rejected on the device");
-  return worst ? RGF_E_STATUS : RGF_OK;
+  if (worst & RGF_ST_TIMEOUT) return fail(RGF_E_CUDA, "a tensor-core wait of the mixed form gave up");
+  return (worst & ~RGF_ST_REFINE_NC) ? RGF_E_STATUS : RGF_OK;
+}
+
+// ------------------------------------------------------------------ blocks
+// Batched block products and inverses in either form (device arrays).
+static int block_args(rgf_ctx* c, int32_t precision, int64_t nb, int64_t count, std::initializer_list<const void*> ptrs) {
+  if (!c) return fail(RGF_E_ARG, "ctx is NULL");
+  if (precision != RGF_PREC_FP64 && precision != RGF_PREC_MIXED) return fail(RGF_E_ARG, "unknown precision %d", precision);
+  if (count < 0) return fail(RGF_E_ARG, "count < 0");
+  for (const void* p : ptrs)
+    if (count > 0 && !is_device_ptr(p)) return fail(RGF_E_ARG, "block arrays must be device memory");
+  return RGF_OK;
+}
+
+extern "C" int rgf_block_product(rgf_ctx* c, int32_t precision, int64_t nb, int64_t count, const rgf_c16* A,
+                               int32_t conj_a, const rgf_c16* B, int32_t conj_b, rgf_c16* C, void* stream_) {
+  int rc = block_args(c, precision, nb, count, {A, B, C});
+  if (rc) return rc;
+  if (nb != 128) return fail(RGF_E_UNSUPPORTED, "rgf_block_product: nb=%lld (built for 128)", (long long)nb);
+  if (count == 0) return RGF_OK;
+  RGF_CUDA(cudaSetDevice(c->device));
+  cudaStream_t st = stream_ ? (cudaStream_t)stream_ : c->stream;
+  const int grid = (int)std::min<int64_t>(count, c->sm_count);
+  if ((rc = c->work.reserve(sizeof(double2) * 4 * 128 * 128 * (size_t)grid))) return rc;
+  if ((rc = c->info.reserve(sizeof(int32_t) * (size_t)count))) return rc;
+  RGF_CUDA(cudaMemsetAsync(c->info.p, 0, sizeof(int32_t) * (size_t)count, st));
+  const int mode = precision == RGF_PREC_MIXED ? 0 : 1;
+  cudaError_t e = launch_block_mixed(mode, 0, (const double2*)A, conj_a, (const double2*)B, conj_b, (double2*)C,
+                                     count, (double2*)c->work.p, grid, (int32_t*)c->info.p, st);
+  if (e != cudaSuccess) return fail(RGF_E_CUDA, "block product launch failed: %s", cudaGetErrorString(e));
+  std::vector<int32_t> h((size_t)count);
+  RGF_CUDA(cudaMemcpyAsync(h.data(), c->info.p, sizeof(int32_t) * (size_t)count, cudaMemcpyDeviceToHost, st));
+  RGF_CUDA(cudaStreamSynchronize(st));
+  for (int32_t v : h)
+    if (v & RGF_ST_TIMEOUT) return fail(RGF_E_CUDA, "a tensor-core wait gave up");
+  return RGF_OK;
+}
+
+extern "C" int rgf_block_inverse(rgf_ctx* c, int32_t precision, int64_t nb, int64_t count, const rgf_c16* X,
+                              rgf_c16* Xinv, int32_t* status, void* stream_) {
+  int rc = block_args(c, precision, nb, count, {X, Xinv});
+  if (rc) return rc;
+  const bool mixed = precision == RGF_PREC_MIXED;
+  if (mixed ? nb != 128 : (nb != 32 && nb != 64 && nb != 128))
+    return fail(RGF_E_UNSUPPORTED, "rgf_block_inverse: nb=%lld not built for this precision", (long long)nb);
+  if (count == 0) return RGF_OK;
+  RGF_CUDA(cudaSetDevice(c->device));
+  cudaStream_t st = stream_ ? (cudaStream_t)stream_ : c->stream;
+  const int grid = (int)std::min<int64_t>(count, c->sm_count);
+  if ((rc = c->work.reserve(sizeof(double2) * 4 * 128 * 128 * (size_t)grid))) return rc;
+  if ((rc = c->info.reserve(sizeof(int32_t) * (size_t)count))) return rc;
+  RGF_CUDA(cudaMemsetAsync(c->info.p, 0, sizeof(int32_t) * (size_t)count, st));
+  cudaError_t e = mixed ? launch_block_mixed(2, 0, (const double2*)X, 0, nullptr, 0, (double2*)Xinv, count,
+                                             (double2*)c->work.p, grid, (int32_t*)c->info.p, st)
+                        : launch_block_fp64_inv((int)nb, (const double2*)X, (double2*)Xinv, count,
+                                                (double2*)c->work.p, grid, (int32_t*)c->info.p, st);
+  if (e != cudaSuccess) return fail(RGF_E_CUDA, "block inverse launch failed: %s", cudaGetErrorString(e));
+  std::vector<int32_t> h((size_t)count);
+  RGF_CUDA(cudaMemcpyAsync(h.data(), c->info.p, sizeof(int32_t) * (size_t)count, cudaMemcpyDeviceToHost, st));
+  RGF_CUDA(cudaStreamSynchronize(st));
+  int worst = 0;
+  for (int32_t v : h) worst |= v;
+  if (status) std::memcpy(status, h.data(), sizeof(int32_t) * (size_t)count);
+  if (worst & RGF_ST_TIMEOUT) return fail(RGF_E_CUDA, "a tensor-core wait gave up");
+  return (worst & ~RGF_ST_REFINE_NC) ? RGF_E_STATUS : RGF_OK;
 }
 
 // ------------------------------------------------------------------ adjoint
@@ -1139,16 +1220,18 @@ extern "C" int rgf_w_solve_batch(rgf_ctx* c, const rgf_w_device* devices, int32_
   RGF_CUDA(cudaMemcpyAsync(hinfo.data(), c->info.p, sizeof(DInfo) * n_tasks, cudaMemcpyDeviceToHost, st));
   RGF_CUDA(cudaStreamSynchronize(st));
   int worst = 0;
-  double flops = 0.0;
+  double flops = 0.0, int8_ops = 0.0;
   for (int64_t t = 0; t < n_tasks; t++) {
     worst |= hinfo[t].status;
     const double nb = (double)devices[tasks[t].device].nm;
     flops += 8.0 * nb * nb * nb * (double)(hinfo[t].n_gemm + hinfo[t].n_inv);
+    int8_ops += 8.0 * nb * nb * nb * (double)hinfo[t].pad;   // 4 real nb^3 products per digit pair
   }
   float kms = 0.0f;
   RGF_CUDA(cudaEventElapsedTime(&kms, c->ev0, c->ev1));
   c->stats.last_kernel_ms = kms;
   c->stats.last_flops = flops;
+  c->stats.last_int8_ops = int8_ops;
   c->stats.last_tasks = n_tasks;
   if (info) std::memcpy(info, hinfo.data(), sizeof(DInfo) * n_tasks);
   if (worst & RGF_ST_BAD_TASK) return fail(RGF_E_ARG, "a task was rejected on the device");

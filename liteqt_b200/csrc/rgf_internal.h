@@ -136,4 +136,18 @@ cudaError_t launch_solver(const KParams& p, int grid, size_t smem, cudaStream_t 
                           bool set_attr = true);
 int solver_threads();
 
+// Mixed-precision form (rgf_mixed.cu): nb = 128, one CTA per SM.
+size_t mixed_smem();                          // dynamic shared memory of a CTA
+int64_t mixed_slot_elems(int64_t nx);         // complex elements of one CTA's slot
+cudaError_t launch_mixed(const KParams& p, int grid, cudaStream_t stream, bool set_attr = true);
+// Batched block operations on nb = 128 blocks, one CTA per block (grid-stride):
+// mode 0 split-integer product with ns slices, 1 FP64 product, 2 refined
+// inverse, 3 FP64 inverse; ws = 4 blocks per CTA; status per block or NULL.
+cudaError_t launch_block_mixed(int mode, int ns, const double2* A, int cA, const double2* B, int cB,
+                               double2* C, int64_t count, double2* ws, int grid, int32_t* status,
+                               cudaStream_t stream);
+// FP64 inverse of nb = 32, 64 or 128 blocks (the plain form's kernels).
+cudaError_t launch_block_fp64_inv(int nb, const double2* X, double2* Xi, int64_t count, double2* ws, int grid,
+                                  int32_t* status, cudaStream_t stream);
+
 }  // namespace rgf

@@ -67,6 +67,7 @@ constexpr int kSmemXMaxNb = 64;  // generic path: inverse workspace in shared me
 // TM x TN 8x8 subtiles), unblocked Gauss-Jordan.
 template <int TM, int TN>
 struct GenericOps {
+  static constexpr bool kMixed = false;
   static constexpr int kMinBlocks = 2;
   static size_t smem_bytes(int nb) {
     return ((nb <= kSmemXMaxNb ? (size_t)nb * nb : 0) + 2 * (size_t)nb) * sizeof(double2);
@@ -92,6 +93,7 @@ struct GenericOps {
 // (nb <= 64) or blocked with shared-memory panels.
 template <int NB>
 struct StagedOps {
+  static constexpr bool kMixed = false;
   static constexpr int kMinBlocks = 2;
   static size_t smem_bytes(int) { return StagedCfg<NB>::SMEM; }
   SmemInv& inv;
@@ -139,10 +141,22 @@ struct Solver {
   __device__ double2* Gl(int l) const { return slot + (size_t)l * n2; }
   __device__ double2* Gln(int l) const { return slot + (nx_max + l) * n2; }
 
+  // Mixed form only: the block operations of the device chain run in the
+  // split-integer / refined form, Sancho-Rubio and its self-energies in FP64.
+  __device__ void set_mixed(bool on) {
+    if constexpr (Ops::kMixed) ops.mixed_on = on;
+  }
+  __device__ bool fp64_now() const {
+    if constexpr (Ops::kMixed) return !ops.mixed_on;
+    return true;
+  }
+
+  // n_gemm / n_inv count the products and inverses run in FP64; the mixed
+  // form's own operations are counted by its policy.
   template <class Epi>
   __device__ void gemm(const double2* A, bool cA, const double2* B, bool cB, Epi&& epi) {
+    if (fp64_now()) n_gemm++;
     ops.gemm(n, A, cA, B, cB, epi);
-    n_gemm++;
     __syncthreads();
   }
   // C = op(A) op(B)
@@ -156,7 +170,7 @@ struct Solver {
   }
   // X holds the matrix; dst (and dst2) receive its inverse.
   __device__ void invert_X(double2* dst, double2* dst2 = nullptr) {
-    n_inv++;
+    if (fp64_now()) n_inv++;
     if (ops.invert(n, dst, dst2)) status |= RGF_ST_SINGULAR;
   }
 
@@ -175,13 +189,28 @@ struct Solver {
   // factorization of LAPACK's xPSTRF, right-looking, with its default stop:
   // the largest remaining diagonal entry <= n eps times the largest initial
   // one.  Thread i < n owns row i's diagonal and flags.
-  __device__ void chol_psd(double2* G, double2* L) {
-    const int nn = n, tid = threadIdx.x, warp = tid >> 5;
+  // Returns false when G is not positive semidefinite to rounding: a row
+  // left out of the factor keeps a remaining diagonal entry below
+  // -n eps max_i |G_ii| (an indefinite Gamma, e.g. from a non-retarded
+  // sigma or an unconverged lead); L is then unusable and the caller takes
+  // the general form.
+  __device__ bool chol_psd(double2* G, double2* L) {
+    const int nn = n, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     double2* lcol = ops.scratch();
     const bool own = tid < nn;
     double d = own ? G[tid + tid * nn].x : 0.0;
     bool used = !own;
     double dtol = 0.0;
+    double amax = fabs(d);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    if (lane == 0) sm.red.v[warp] = amax;
+    __syncthreads();
+    amax = 0.0;
+#pragma unroll
+    for (int w = 0; w < kWarps; w++) amax = fmax(amax, sm.red.v[w]);
+    __syncthreads();
+    const double neg_tol = (double)nn * 2.220446049250313e-16 * amax;
     int k = 0;
     for (; k < nn; k++) {
       unsigned key = 0u;
@@ -228,7 +257,16 @@ struct Solver {
       __syncthreads();
     }
     for (int e = tid; e < (nn - k) * nn; e += kThreads) L[(size_t)k * nn + e] = czero();
+    double dmin = (own && !used) ? d : 0.0;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) dmin = fmin(dmin, __shfl_xor_sync(0xffffffffu, dmin, o));
+    if (lane == 0) sm.red.v[warp] = dmin;
     __syncthreads();
+    dmin = 0.0;
+#pragma unroll
+    for (int w = 0; w < kWarps; w++) dmin = fmin(dmin, sm.red.v[w]);
+    __syncthreads();
+    return !(dmin < -neg_tol);
   }
 
   // sancho (green_rgf.f90:4451-4537); S00 = nullptr is the identity (the
@@ -351,15 +389,24 @@ struct Solver {
       });
       __syncthreads();
     }
+    set_mixed(true);   // the device chain (mixed form)
     invert_X(Gl(0));
     const double2* GN1 = Gl(0);
     double2* GN1buf[2] = {tmp(T_GN1A), tmp(T_GN1B)};
     int gsel = 0;
-    if (ballistic) {
-      // sig<_L = -(sL - sL^H) fL = i fL Gamma_L with Gamma_L = L L^H, so every
-      // left-connected g<_l = g^L_{l,1} sig<_L g^L_{l,1}^H is i fL V_l V_l^H
-      // for the running column V_l = g^L_{l,1} L: one product per block
-      chol_psd(tmp(T_F3), tmp(T_SIG));
+    // sig<_L = -(sL - sL^H) fL = i fL Gamma_L with Gamma_L = L L^H, so every
+    // left-connected g<_l = g^L_{l,1} sig<_L g^L_{l,1}^H is i fL V_l V_l^H
+    // for the running column V_l = g^L_{l,1} L: one product per block.  An
+    // indefinite Gamma_L has no such factor: sig<_L is formed and the
+    // general recursion runs.
+    const bool lowrank = ballistic && chol_psd(tmp(T_F3), tmp(T_SIG));
+    if (ballistic && !lowrank) {
+      for_each_elem(n, [&](int i, int j, int idx) {
+        tmp(T_SIG)[idx] = cscale(csub(sigmal[idx], cconj(sigmal[j + i * nn])), -fl);
+      });
+      __syncthreads();
+    }
+    if (lowrank) {
       gemm_store(Gl(0), false, tmp(T_SIG), false, GN1buf[gsel]);   // V_1 = g_1 L
       GN1 = GN1buf[gsel];
       gsel ^= 1;
@@ -385,13 +432,13 @@ struct Solver {
         X[idx] = csub(zs_minus(z, Sl, i, j, idx, h), v);
       });
       invert_X(Gl(l));
-      if (want_T || ballistic) {  // g^L_{l,1} = g_l H_{l,l-1} g^L_{l-1,1} (ballistic: times L)
+      if (want_T || lowrank) {  // g^L_{l,1} = g_l H_{l,l-1} g^L_{l-1,1} (low rank: times L)
         gemm_store(H, false, GN1, false, tmp(T_F1));
         gemm_store(Gl(l), false, tmp(T_F1), false, GN1buf[gsel]);
         GN1 = GN1buf[gsel];
         gsel ^= 1;
       }
-      if (ballistic) {
+      if (lowrank) {
         // Without scattering the recursion g<_l = g_l H g<_{l-1} H^H g_l^H
         // unrolls to g<_l = g^L_{l,1} sig<_L (g^L_{l,1})^H = i fL V_l V_l^H:
         // one product on the running column instead of four.
@@ -420,10 +467,12 @@ struct Solver {
       __syncthreads();
     }
     const double2* H = blk(H1i, nx - 1);
+    set_mixed(false);  // the right lead in FP64
     const int itR = sancho(E, H00, H, false, tmp(T_GS), S_l(nx - 1));
     double2* sigmar = tmp(T_SIGR);
     gemm_store(H, true, tmp(T_GS), false, tmp(T_F1));               // A = H10^H G00
     gemm_store(tmp(T_F1), false, H, false, sigmar);                 // sigmar = A H10
+    set_mixed(true);
     gemm_store(H, false, Gl(nx - 2), false, tmp(T_F2));             // B = H10 Gl(nx-1)
     {
       const double2* SN = S_l(nx - 1);
@@ -492,7 +541,7 @@ struct Solver {
       });
       __syncthreads();
       gemm_store(tmp(T_GAMR), false, tmp(T_X2), false, tmp(T_Y));   // Gamma_R G_N1 (L)
-      if (ballistic) {
+      if (lowrank) {
         // X2 = G_N1 L: T = Tr[Gamma_R X2 X2^H] = sum_ij Re (Gamma_R X2)_ij conj(X2_ij)
         double acc = 0.0;
         for_each_elem(n, [&](int, int, int idx) {

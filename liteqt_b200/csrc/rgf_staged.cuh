@@ -27,6 +27,10 @@
 #include "rgf_device.cuh"
 
 namespace rgf {
+// Internal linkage: every translation unit compiles its own copies, under its
+// own register budget (the FP64 kernel's units cap at 128 registers, the
+// mixed form's unit does not), so no out-of-line instance is shared.
+namespace {
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -635,5 +639,7 @@ __device__ int gj_invert_blocked(double2* X0, double2* X1, double2* dst, double2
   }
   return 0;
 }
+
+}  // namespace
 
 }  // namespace rgf

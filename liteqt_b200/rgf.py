@@ -117,12 +117,12 @@ class c_ham_info(ctypes.Structure):
 class c_stats(ctypes.Structure):
     _fields_ = [("last_kernel_ms", ctypes.c_double), ("last_flops", ctypes.c_double),
                 ("last_tasks", ctypes.c_int64), ("launches", ctypes.c_int64),
-                ("reserved", ctypes.c_int64 * 4)]
+                ("last_int8_ops", ctypes.c_double), ("reserved", ctypes.c_int64 * 3)]
 
 
 INFO_DTYPE = np.dtype([("status", "<i4"), ("sancho_iters_left", "<i4"),
                        ("sancho_iters_right", "<i4"), ("n_gemm", "<i4"), ("n_inv", "<i4"),
-                       ("reserved", "<i4")])
+                       ("mixed_pairs", "<i4")])
 
 
 
@@ -204,6 +204,11 @@ def load(path: str = LIB_PATH):
     L.rgf_variant_name.restype = ctypes.c_char_p
     for name in ("rgf_plan_create", "rgf_plan_execute", "rgf_plan_destroy", "rgf_autotune"):
         getattr(L, name).restype = ctypes.c_int
+    L.rgf_block_product.argtypes = [P, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, P, ctypes.c_int32, P,
+                                  ctypes.c_int32, P, P]
+    L.rgf_block_inverse.argtypes = [P, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, P, P, P, P]
+    L.rgf_block_product.restype = ctypes.c_int
+    L.rgf_block_inverse.restype = ctypes.c_int
     L.rgf_last_error.restype = ctypes.c_char_p
     L.rgf_version.restype = ctypes.c_char_p
     for name in ("rgf_ctx_create", "rgf_ctx_destroy", "rgf_ctx_set_opts", "rgf_solve_batch",
@@ -308,7 +313,24 @@ class Context:
         s = c_stats()
         _check(load().rgf_ctx_get_stats(self.h, ctypes.byref(s)))
         return dict(last_kernel_ms=s.last_kernel_ms, last_flops=s.last_flops,
-                    last_tasks=s.last_tasks, launches=s.launches)
+                    last_tasks=s.last_tasks, launches=s.launches, last_int8_ops=s.last_int8_ops)
+
+    # ------------------------------------------------------------------ blocks
+    def block_product(self, A, B, C, conj_a=False, conj_b=False, precision=None, stream=None):
+        """rgf_block_product on device tensors of shape (count, nb, nb) (Fortran
+        block layout: the last two axes are (column, row))."""
+        prec = self.opts.precision if precision is None else precision
+        count, nb = int(A.shape[0]), int(A.shape[-1])
+        _check(load().rgf_block_product(self.h, int(prec), nb, count, _ptr(A), int(bool(conj_a)), _ptr(B),
+                                      int(bool(conj_b)), _ptr(C), stream))
+
+    def block_inverse(self, X, Xinv, status=None, precision=None, stream=None, allow_status=True):
+        """rgf_block_inverse on device tensors of shape (count, nb, nb); status:
+        host int32 array (count,) or None."""
+        prec = self.opts.precision if precision is None else precision
+        count, nb = int(X.shape[0]), int(X.shape[-1])
+        return _check(load().rgf_block_inverse(self.h, int(prec), nb, count, _ptr(X), _ptr(Xinv), _ptr(status),
+                                            stream), allow_status)
 
     def set_opts(self, opts: Options):
         o = opts.c()
