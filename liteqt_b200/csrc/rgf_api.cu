@@ -533,7 +533,7 @@ extern "C" int rgf_block_product(rgf_ctx* c, int32_t precision, int64_t nb, int6
   RGF_CUDA(cudaSetDevice(c->device));
   cudaStream_t st = stream_ ? (cudaStream_t)stream_ : c->stream;
   const int grid = (int)std::min<int64_t>(count, c->sm_count);
-  if ((rc = c->work.reserve(sizeof(double2) * 4 * 128 * 128 * (size_t)grid))) return rc;
+  if ((rc = c->work.reserve(sizeof(double2) * 5 * 128 * 128 * (size_t)grid))) return rc;
   if ((rc = c->info.reserve(sizeof(int32_t) * (size_t)count))) return rc;
   RGF_CUDA(cudaMemsetAsync(c->info.p, 0, sizeof(int32_t) * (size_t)count, st));
   const int mode = precision == RGF_PREC_MIXED ? 0 : 1;
@@ -559,7 +559,7 @@ extern "C" int rgf_block_inverse(rgf_ctx* c, int32_t precision, int64_t nb, int6
   RGF_CUDA(cudaSetDevice(c->device));
   cudaStream_t st = stream_ ? (cudaStream_t)stream_ : c->stream;
   const int grid = (int)std::min<int64_t>(count, c->sm_count);
-  if ((rc = c->work.reserve(sizeof(double2) * 4 * 128 * 128 * (size_t)grid))) return rc;
+  if ((rc = c->work.reserve(sizeof(double2) * 5 * 128 * 128 * (size_t)grid))) return rc;
   if ((rc = c->info.reserve(sizeof(int32_t) * (size_t)count))) return rc;
   RGF_CUDA(cudaMemsetAsync(c->info.p, 0, sizeof(int32_t) * (size_t)count, st));
   cudaError_t e = mixed ? launch_block_mixed(2, 0, (const double2*)X, 0, nullptr, 0, (double2*)Xinv, count,

@@ -141,8 +141,9 @@ size_t mixed_smem();                          // dynamic shared memory of a CTA
 int64_t mixed_slot_elems(int64_t nx);         // complex elements of one CTA's slot
 cudaError_t launch_mixed(const KParams& p, int grid, cudaStream_t stream, bool set_attr = true);
 // Batched block operations on nb = 128 blocks, one CTA per block (grid-stride):
-// mode 0 split-integer product with ns slices, 1 FP64 product, 2 refined
-// inverse, 3 FP64 inverse; ws = 4 blocks per CTA; status per block or NULL.
+// mode 0 split-integer product with ns slices (0 = all), 1 FP64 product,
+// 2 refined inverse, 3 FP64 inverse; ws = 5 blocks per CTA; status per block
+// or NULL.
 cudaError_t launch_block_mixed(int mode, int ns, const double2* A, int cA, const double2* B, int cB,
                                double2* C, int64_t count, double2* ws, int grid, int32_t* status,
                                cudaStream_t stream);

@@ -22,8 +22,8 @@ namespace rgf {
 namespace {
 
 // Extra scratch blocks of a mixed-form slot beyond slot_elems_for(): the
-// refined inverse Y and the residual R.
-constexpr int kMixedExtraBlocks = 2;
+// refined inverse Y, the residual R and the product staging block.
+constexpr int kMixedExtraBlocks = 3;
 
 struct MixedCta {
   uint32_t tmem;
@@ -86,11 +86,12 @@ __device__ __noinline__ void task_mixed128(const KParams& p, int64_t t, double2*
   const size_t n2 = 128 * 128;
   double2* temps = slot + 2 * (size_t)dv.nx * n2;
   MixedOps ops(sm.inv, sm.red, dyn, temps + (size_t)T_INV * n2, temps + (size_t)T_RT * n2,
-               temps + (size_t)kNumTemps * n2, temps + (size_t)(kNumTemps + 1) * n2, c.tmem, c.st);
+               temps + (size_t)kNumTemps * n2, temps + (size_t)(kNumTemps + 1) * n2,
+               temps + (size_t)(kNumTemps + 2) * n2, c.tmem, c.st);
   Solver<MixedOps> s(p.o, dv.nx, sm, ops, slot, 128, (int)dv.nx);
   s.run(p.tasks[t], dv, info);
   if (info && threadIdx.x == 0) {
-    info->n_inv += ops.n_fallback;
+    info->n_inv += ops.n_fallback + ops.n_fp64_inv;
     info->pad = ops.n_pairs;
     if (ops.n_fallback) info->status |= RGF_ST_REFINE_NC;
     if (!c.st.ok) info->status |= RGF_ST_TIMEOUT;
@@ -128,7 +129,7 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_mixed_kernel(KParams p) {
 // ------------------------------------------------------------------ blocks
 // One CTA per block (grid-stride): mode 0 product op(A) op(B) split-integer
 // with ns slices, 1 product FP64 (nb = 128), 2 inverse refined, 3 inverse
-// FP64.  ws: 4 global blocks per CTA (X, X1, Y, R).
+// FP64.  ws: 5 global blocks per CTA (X, X1, Y, R, product staging).
 template <int NB>
 __device__ void block_fp64_inverse(const double2* A, double2* C, double2* ws, Smem& sm, unsigned char* dyn,
                                    int32_t* status, int b) {
@@ -162,8 +163,8 @@ __global__ void __launch_bounds__(kThreads, 1) rgf_block_mixed_kernel(int mode, 
   MixedCta c;
   mixed_cta_begin(dyn_smem, &tmem_slot, c);
   constexpr size_t n2 = 128 * 128;
-  double2* w = ws + (size_t)blockIdx.x * 4 * n2;
-  MixedOps ops(sm.inv, sm.red, dyn_smem, w, w + n2, w + 2 * n2, w + 3 * n2, c.tmem, c.st);
+  double2* w = ws + (size_t)blockIdx.x * 5 * n2;
+  MixedOps ops(sm.inv, sm.red, dyn_smem, w, w + n2, w + 2 * n2, w + 3 * n2, w + 4 * n2, c.tmem, c.st);
   for (int64_t b = blockIdx.x; b < count && c.st.ok; b += gridDim.x) {
     const double2* a = A + (size_t)b * n2;
     double2* o = C + (size_t)b * n2;

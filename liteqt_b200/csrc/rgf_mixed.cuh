@@ -11,13 +11,14 @@
 //     0x80 * sum_b 256^b to the integer makes its bytes the digits plus 128;
 //   * the digit products sum_k a_p[r][k] b_q[k][j] are exact in int32 (at
 //     most S K 2^14 in magnitude), accumulated in tensor memory (TMEM) by the
-//     MMA; the pairs with p + q = L share one accumulator ("level" L), the
-//     pairs with p + q >= S are dropped (weights 2^-8S and below of the
-//     leading pair);
+//     MMA; the pairs with p + q = L share one accumulator ("level" L) --
+//     one MMA multiplies slice p with all B slices q at once, into columns
+//     offset so that (p, q) lands on level p + q -- and the pairs with
+//     p + q >= S are dropped (weights 2^-8S and below of the leading pair);
 //   * the levels are combined in FP64 registers and scaled back:
 //     C[r][j] = 2^(E_r + F_j - 12) sum_L T_L 2^(-8 L).
-// The complex product runs as two real MMAs per digit pair and K step,
-// a_re x [b_re | b_im] and a_im x [b_re | b_im] (N = 2 NT columns each), into
+// The complex product runs as two real MMAs per A slice and K step,
+// a_re x [b_re | b_im]_q and a_im x [b_re | b_im]_q over the B slices q, into
 // two accumulators, combined on the way out: Re = ArBr - AiBi,
 // Im = ArBi + AiBr.  Error per element: below about
 // 2^-(8S-4) n max_k |op(A)[r][k]| max_k |op(B)[k][j]| (rounding of both
@@ -33,11 +34,12 @@
 // (k / 16) 16 R + 16 r + k % 16.  A K group of all rows is one contiguous
 // run, so the tensor cores' operand reads and the digit stores (consecutive
 // rows from consecutive threads) do not collide in the shared-memory banks,
-// which they do when 8-row groups sit 1 KB apart.  Operand bases are
-// 1024-byte aligned.  TMEM (512 columns) holds every level of a tile, 4 NT
-// columns each; the levels are issued in two groups with a commit each, so
-// the CTA reads the first group back (tcgen05.ld) and accumulates it in FP64
-// while the tensor cores run the second.
+// which they do when 8-row groups sit 1 KB apart.  The B slices of a tile
+// are consecutive row groups of one operand.  Operand bases are 1024-byte
+// aligned.  TMEM holds every level of a tile (2 S x 2 NT columns); the MMAs
+// are issued in two groups with a commit each, so the CTA reads the first
+// levels back (tcgen05.ld) and accumulates them in FP64 while the tensor
+// cores run the second group.
 //
 // Inverse: Gauss-Jordan with partial pivoting in FP32, the matrix in
 // registers (64 complex values per thread), then Newton-Schulz steps
@@ -68,25 +70,26 @@ constexpr int NTILE = NB / NT;
 constexpr int KSTEPS = NB / 32;       // MMA K steps (32 int8 each)
 constexpr uint32_t A_BLK = NB * NB;                 // bytes of one (slice, component) of op(A)
 constexpr uint32_t A_BYTES = S * 2 * A_BLK;         // all digits of op(A)
-constexpr uint32_t B_ROWS = 2 * NT;                 // B tile rows: real parts, then imaginary
-constexpr uint32_t B_BLK = B_ROWS * NB;             // bytes of one slice of the B tile
-constexpr uint32_t B_BYTES = S * B_BLK;
+constexpr uint32_t B_SL = 2 * NT;                   // B tile rows of one slice: real parts, imaginary
+constexpr uint32_t B_ROWS = S * B_SL;               // all slices, as one operand (slice q at rows q B_SL ..)
+constexpr uint32_t B_BYTES = B_ROWS * NB;
 constexpr uint32_t EXP_OFF = A_BYTES + B_BYTES;     // int rowexp[NB], colexp[NB]
 constexpr uint32_t BAR_OFF = EXP_OFF + 2 * NB * 4;  // 3 mbarriers
 constexpr uint32_t SMEM_BYTES = BAR_OFF + 64;
-constexpr uint32_t BUF_COLS = 4 * NT;               // one level: ArBr | ArBi | AiBr | AiBi
-constexpr int H1_LEVELS = (S + 1) / 2;              // levels drained first (the leading ones)
-constexpr uint32_t TMEM_COLS = 512;                 // S levels of a tile (S x 4 NT <= 512)
-static_assert(S * BUF_COLS <= TMEM_COLS, "every level of a tile in TMEM");
+constexpr uint32_t D_I = S * B_SL;                  // TMEM: levels x [ArBr | ArBi], then levels x [AiBr | AiBi]
+constexpr int H1_SLICES = (S + 1) / 2;              // A slices of the first MMA group (levels 0 .. H1-1 final)
+constexpr uint32_t TMEM_COLS = 512;
+static_assert(2 * D_I <= TMEM_COLS, "every level of a tile in TMEM");
+static_assert(B_ROWS <= 256, "one MMA spans every B slice (N <= 256)");
 static_assert(TMEM_COLS == 32 || TMEM_COLS == 64 || TMEM_COLS == 128 || TMEM_COLS == 256 ||
               TMEM_COLS == 512, "TMEM allocation is a power of two >= 32 columns");
 static_assert(SMEM_BYTES + 1024 <= 227 * 1024, "one CTA per SM, with 1 KB of alignment slack");
 static_assert(StagedCfg<NB>::SMEM <= A_BYTES, "the FP64 operations alias the digit area");
 static_assert(NT == 16, "the drain reads 8 columns per thread of each 16-column block");
 // instruction descriptor: D s32 (bits 4-5 = 2), A and B s8 (bits 7-9, 10-12
-// = 1), both K-major, N = 2 NT (bits 17-22: N >> 3), M = 128 (bits 24-28: M >> 4)
-constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | (((uint32_t)B_ROWS >> 3) << 17) |
-                           (((uint32_t)NB >> 4) << 24);
+// = 1), both K-major, M = 128 (bits 24-28: M >> 4); N in bits 17-22 (N >> 3)
+constexpr uint32_t IDESC_BASE = (2u << 4) | (1u << 7) | (1u << 10) | (((uint32_t)NB >> 4) << 24);
+__host__ __device__ constexpr uint32_t idesc_n(uint32_t n) { return IDESC_BASE | ((n >> 3) << 17); }
 constexpr long long kWaitCycles = 2000000000ll;     // ~1 s at the B200 boost clock
 
 // ------------------------------------------------------------------ PTX
@@ -101,11 +104,12 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t
   return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
-__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t acc) {
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t acc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
-      "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 // One lane of a converged warp (elect.sync): the lane that issues the MMAs
 // and commits while its whole warp computes the (warp-uniform) descriptors.
@@ -307,16 +311,18 @@ struct MixedOps {
   double2* X;           // the matrix to invert (global)
   double2* Y;           // refined inverse (global scratch block)
   double2* R;           // residual I - X Y (global scratch block)
+  double2* Cs;          // product staging: the tiles' results, then one epilogue pass
   uint32_t tmem;        // TMEM base address of this CTA
   MixState& st;         // mbarrier parities, failure flag (the CTA's, across tasks)
   bool mixed_on = false;
   int n_pairs = 0;      // digit-pair products (4 real 128^3 int8 products each)
-  int n_fallback = 0;   // inverses that fell back to FP64
+  int n_fallback = 0;   // refined inverses that fell back to FP64
+  int n_fp64_inv = 0;   // inverses of the device chain run in FP64
 
   __device__ MixedOps(SmemInv& i, SmemRed& r, unsigned char* dyn, double2* slot_inv, double2* slot_rt,
-                      double2* y, double2* res, uint32_t tm, MixState& s)
+                      double2* y, double2* res, double2* cs, uint32_t tm, MixState& s)
       : f64(i, (double2*)dyn, slot_inv, slot_rt, 128), inv(i), red(r), sm(dyn), X(slot_inv), Y(y), R(res),
-        tmem(tm), st(s) {}
+        Cs(cs), tmem(tm), st(s) {}
   __device__ bool ok() const { return st.ok != 0; }
 
   __device__ double2* scratch() const { return (double2*)sm; }
@@ -344,7 +350,7 @@ struct MixedOps {
     if (tid < mx::NB) { rx[tid] = 0; cx[tid] = 0; }
     __syncthreads();
     constexpr int PER = (mx::NB * mx::NB) / kThreads;   // 64 elements a thread
-    constexpr int BATCH = 16;
+    constexpr int BATCH = 32;
 #pragma unroll 1
     for (int which = 0; which < 2; which++) {
       const double2* M = which ? B : A;
@@ -352,7 +358,8 @@ struct MixedOps {
       const bool mod_key = which ? cB : !cA;
       int* dst = which ? cx : rx;
       unsigned local = 0;
-#pragma unroll 1
+      unsigned wmax[PER / 32] = {};
+#pragma unroll
       for (int m0 = 0; m0 < PER; m0 += BATCH) {
         unsigned e[BATCH];
 #pragma unroll
@@ -361,14 +368,22 @@ struct MixedOps {
 #pragma unroll
           for (int b = 0; b < BATCH; b++) local = e[b] > local ? e[b] : local;
         } else {
+          // key (tid + m kThreads) >> 7 = tid / 128 + 2 m is warp-uniform: the
+          // warp's maximum for element m is kept by lane m % 32 (two per lane)
 #pragma unroll
           for (int b = 0; b < BATCH; b++) {
             const unsigned w = __reduce_max_sync(0xffffffffu, e[b]);
-            if ((tid & 31) == 0) atomicMax(dst + ((tid + (m0 + b) * kThreads) >> 7), (int)w);
+            if (((m0 + b) & 31) == (tid & 31)) wmax[(m0 + b) >> 5] = w;
           }
         }
       }
-      if (mod_key) atomicMax(dst + (tid & (mx::NB - 1)), (int)local);
+      if (mod_key) {
+        atomicMax(dst + (tid & (mx::NB - 1)), (int)local);
+      } else {
+#pragma unroll
+        for (int u = 0; u < PER / 32; u++)
+          atomicMax(dst + ((tid >> 7) + 2 * ((tid & 31) + 32 * u)), (int)wmax[u]);
+      }
     }
     __syncthreads();
   }
@@ -414,44 +429,47 @@ struct MixedOps {
     unsigned long long y[8];
 #pragma unroll
     for (int kk = 0; kk < 8; kk++) y[kk] = mx::digits_of(v[kk].x, sc);
-    mx::store_digits8(y, base + mx::kmaj_off(j, g, mx::B_ROWS), mx::B_BLK);
+    mx::store_digits8(y, base + mx::kmaj_off(j, g, mx::B_ROWS), 16 * mx::B_SL);
 #pragma unroll
     for (int kk = 0; kk < 8; kk++) y[kk] = mx::digits_of(v[kk].y, sc);
-    mx::store_digits8(y, base + mx::kmaj_off(mx::NT + j, g, mx::B_ROWS), mx::B_BLK);
+    mx::store_digits8(y, base + mx::kmaj_off(mx::NT + j, g, mx::B_ROWS), 16 * mx::B_SL);
   }
   static_assert(2 * mx::NT * (mx::NB / 16) == kThreads, "one B half-group per thread");
 
-  // MMAs of levels L0 .. L1-1 (digit pairs p + q = L, both < ns), level L
-  // into TMEM columns L x 4 NT, then a commit to mbarrier b.  Called by every
-  // lane of one warp: the descriptors are warp-uniform values, and one
-  // elected lane issues the MMAs (issuing them from a single diverged thread
-  // cost ~100 cycles an MMA).  A descriptor's start address sits in its low
-  // bits (addresses < 256 KB, no carry), so an operand offset is added to the
-  // base descriptor as offset >> 4.
-  __device__ void issue_levels(int L0, int L1, int ns, int b) {
+  // The MMAs of A slices p0 .. p1-1, then a commit to mbarrier b.  One MMA
+  // multiplies slice p of op(A) (real or imaginary digits) with every B slice
+  // q < ns - p at once (N = (ns - p) x 2 NT: the slices are consecutive row
+  // groups of the B operand) into TMEM columns starting p x 2 NT further
+  // along, so the product of slices p and q lands on level p + q's columns:
+  // the levels accumulate without a separate pass per digit pair, in S MMAs
+  // per component and K step instead of S (S + 1) / 2.  Slice 0, K step 0
+  // writes every level (accumulate off); all others accumulate, so the MMAs
+  // of a tile are issued by one thread, in order.  Called by every lane of
+  // one warp: the descriptors are warp-uniform values and one elected lane
+  // issues (a single diverged thread issued each MMA in ~100 cycles).  A
+  // descriptor's start address sits in its low bits (addresses < 256 KB, no
+  // carry), so an operand offset is added to the base descriptor as
+  // offset >> 4.
+  __device__ void issue_slices(int p0, int p1, int ns, int b) {
     const uint32_t sa = mx::smem_u32(sm), sb = sa + mx::A_BYTES;
     constexpr uint32_t la = 16 * mx::NB, lb = 16 * mx::B_ROWS;        // K-group strides
     const uint64_t dA0 = mx::sdesc(sa, la, 128);
     const uint64_t dB0 = mx::sdesc(sb, lb, 128);
     const bool leader = mx::elect_one();
     mx::fence_after_sync();
-    for (int L = L0; L < L1; L++) {
-      const uint32_t d_r = tmem + (uint32_t)L * mx::BUF_COLS;          // [ArBr | ArBi]
-      const uint32_t d_i = d_r + mx::B_ROWS;                           // [AiBr | AiBi]
-      const int p0 = L - ns + 1 > 0 ? L - ns + 1 : 0;
-      const int p1 = L < ns - 1 ? L : ns - 1;
-      for (int p = p0; p <= p1; p++) {
-        const uint64_t ar = dA0 + ((uint64_t)(2 * p) * mx::A_BLK >> 4);
-        const uint64_t ai = ar + (mx::A_BLK >> 4);
-        const uint64_t bq = dB0 + ((uint64_t)(L - p) * mx::B_BLK >> 4);
+    for (int p = p0; p < p1; p++) {
+      const uint32_t idesc = mx::idesc_n((uint32_t)(ns - p) * mx::B_SL);
+      const uint32_t d_r = tmem + (uint32_t)p * mx::B_SL;              // levels x [ArBr | ArBi]
+      const uint32_t d_i = d_r + mx::D_I;                              // levels x [AiBr | AiBi]
+      const uint64_t ar = dA0 + ((uint64_t)(2 * p) * mx::A_BLK >> 4);
+      const uint64_t ai = ar + (mx::A_BLK >> 4);
 #pragma unroll
-        for (int ks = 0; ks < mx::KSTEPS; ks++) {
-          // an MMA's K = 32 is K groups 2 ks and 2 ks + 1
-          const uint32_t acc = (p > p0 || ks > 0) ? 1u : 0u;
-          if (leader) {
-            mx::mma_i8(d_r, ar + (2 * ks * la >> 4), bq + (2 * ks * lb >> 4), acc);
-            mx::mma_i8(d_i, ai + (2 * ks * la >> 4), bq + (2 * ks * lb >> 4), acc);
-          }
+      for (int ks = 0; ks < mx::KSTEPS; ks++) {
+        // an MMA's K = 32 is K groups 2 ks and 2 ks + 1
+        const uint32_t acc = (p > 0 || ks > 0) ? 1u : 0u;
+        if (leader) {
+          mx::mma_i8(d_r, ar + (2 * ks * la >> 4), dB0 + (2 * ks * lb >> 4), idesc, acc);
+          mx::mma_i8(d_i, ai + (2 * ks * la >> 4), dB0 + (2 * ks * lb >> 4), idesc, acc);
         }
       }
     }
@@ -466,12 +484,12 @@ struct MixedOps {
     mx::fence_after_sync();
     __syncwarp();   // tcgen05.ld is warp-collective (.sync.aligned)
     for (int L = L0; L < L1; L++) {
-      const uint32_t cb = tl + (uint32_t)L * mx::BUF_COLS + 8 * h;
+      const uint32_t cb = tl + (uint32_t)L * mx::B_SL + 8 * h;
       int32_t rbr[8], rbi[8], ibr[8], ibi[8];
-      mx::tmem_ld8(cb, rbr);                       // ArBr
-      mx::tmem_ld8(cb + mx::NT, rbi);              // ArBi
-      mx::tmem_ld8(cb + 2 * mx::NT, ibr);          // AiBr
-      mx::tmem_ld8(cb + 3 * mx::NT, ibi);          // AiBi
+      mx::tmem_ld8(cb, rbr);                           // ArBr
+      mx::tmem_ld8(cb + mx::NT, rbi);                  // ArBi
+      mx::tmem_ld8(cb + mx::D_I, ibr);                 // AiBr
+      mx::tmem_ld8(cb + mx::D_I + mx::NT, ibi);        // AiBi
       mx::tmem_wait_ld(rbr, rbi, ibr, ibi);
       const double w = __longlong_as_double((long long)(1023 - 8 * L) << 52);   // 2^-8L
 #pragma unroll
@@ -488,17 +506,17 @@ struct MixedOps {
   // written by epi (op(A) is read once, before the first epilogue); B is
   // read tile by tile.
   //
-  // Per tile of 16 output columns every level accumulates in its own TMEM
-  // columns, issued in two groups (the leading levels, then the rest), each
-  // with a commit: the CTA reads the first group back while the tensor
-  // cores run the second, and the next tile's first group (whose TMEM was
-  // just read) runs while the CTA reads the second.  The B tile is rewritten
-  // once the tile's last MMA has completed.
+  // Per tile of 16 output columns the MMAs go out in two groups with a
+  // commit each: A slices 0 .. h1-1, after which levels 0 .. h1-1 are final
+  // and the CTA reads them back while the tensor cores run the second group;
+  // then the remaining levels.  The next tile's B digits are written once
+  // every MMA of the tile has completed, its MMAs issued, and the finished
+  // tile's outputs scaled and stored while they run.
   template <class Epi>
   __device__ void gemm_mixed(const double2* A, bool cA, const double2* B, bool cB, Epi&& epi, int ns = mx::S) {
     if (!ok()) return;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int h1 = ns < mx::H1_LEVELS ? ns : mx::H1_LEVELS;   // levels 0 .. h1-1, then h1 .. ns-1
+    const int h1 = ns < mx::H1_SLICES ? ns : mx::H1_SLICES;
     const bool two = h1 < ns;
     exponents(A, cA, B, cB);
     double2 bv[8];
@@ -508,38 +526,37 @@ struct MixedOps {
     mx::fence_async_smem();
     __syncthreads();
     if (mx::NTILE > 1) load_b(B, cB, mx::NT, bv);          // tile 1's values, in flight
-    if (warp == 0) issue_levels(0, h1, ns, 0);
-    if (two && warp == 1) issue_levels(h1, ns, ns, 1);
+    if (warp == 0) {
+      issue_slices(0, h1, ns, 0);
+      if (two) issue_slices(h1, ns, ns, 1);
+    }
     const int r = 32 * (warp & 3) + lane;                  // output row (TMEM lane)
     const int h = warp >> 2;                               // which 8 of the tile's 16 columns
     const uint32_t tl = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
     const int xr = rowexp()[r];
     for (int tile = 0; tile < mx::NTILE; tile++) {
       const int j0 = tile * mx::NT;
-      const bool next = tile + 1 < mx::NTILE;
       double re[8], im[8];
 #pragma unroll
       for (int c = 0; c < 8; c++) re[c] = im[c] = 0.0;
-      wait_buf(0);                                         // first group done
+      wait_buf(0);                                         // levels 0 .. h1-1 final
       if (!ok()) return;
       drain_levels(0, h1, tl, h, re, im);
       if (two) {
-        wait_buf(1);                                       // the tile's last MMA done: B tile free
+        wait_buf(1);                                       // every MMA of the tile done
         if (!ok()) return;
-      } else {
-        __syncthreads();
+        drain_levels(h1, ns, tl, h, re, im);
       }
-      if (next) {
+      __syncthreads();                                     // TMEM read by all; B tile free
+      if (tile + 1 < mx::NTILE) {
         store_b(j0 + mx::NT, bv);
         mx::fence_async_smem();
-      }
-      __syncthreads();                                     // B tile written, first group's TMEM read
-      if (next && warp == 0) issue_levels(0, h1, ns, 0);
-      if (next && tile + 2 < mx::NTILE) load_b(B, cB, j0 + 2 * mx::NT, bv);
-      if (two) {
-        drain_levels(h1, ns, tl, h, re, im);
-        __syncthreads();                                   // second group's TMEM read
-        if (next && warp == 1) issue_levels(h1, ns, ns, 1);
+        __syncthreads();
+        if (warp == 0) {
+          issue_slices(0, h1, ns, 0);
+          if (two) issue_slices(h1, ns, ns, 1);
+        }
+        if (tile + 2 < mx::NTILE) load_b(B, cB, j0 + 2 * mx::NT, bv);
       }
 #pragma unroll
       for (int c = 0; c < 8; c++) {
@@ -552,7 +569,21 @@ struct MixedOps {
           const int e = xr + yc - 2056;        // 2^(E_r + F_j - 12), E = X - 1022
           v = make_double2(mx::scale2(re[c], e), mx::scale2(im[c], e));
         }
-        epi(r, j, v);
+        Cs[r + (size_t)j * mx::NB] = v;
+      }
+    }
+    __syncthreads();
+    // One elementwise pass of the epilogue over the staged product, eight
+    // elements a thread at a time: the epilogues' own global loads (H, Gl,
+    // ...) go out together instead of eight per tile behind each drain.
+    for (int base = tid; base < mx::NB * mx::NB; base += 8 * kThreads) {
+      double2 v[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) v[u] = Cs[base + u * kThreads];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int idx = base + u * kThreads;
+        epi(idx & (mx::NB - 1), idx >> 7, v[u]);
       }
     }
     n_pairs += ns * (ns + 1) / 2;
@@ -734,8 +765,13 @@ struct MixedOps {
     return f64.invert(N, dst, dst2);
   }
 
+  // The chain's inverses: the FP64 Gauss-Jordan of the plain form.  The
+  // refined FP32 inverse (invert_mixed) is correct but, with one CTA per SM,
+  // slower than it (1.55 M cycles against 0.60 M at nb = 128: the FP32
+  // elimination's column loop is latency-bound like the FP64 one, and the
+  // residual products come on top), so it serves rgf_block_inverse only.
   __device__ int invert(int n, double2* dst, double2* dst2) {
-    if (mixed_on) return invert_mixed(dst, dst2);
+    if (mixed_on) n_fp64_inv++;
     return f64.invert(n, dst, dst2);
   }
 };
