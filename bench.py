@@ -68,6 +68,10 @@ def parse():
     p.add_argument("--gw", action="store_true",
                    help="time the GW-loop convolutions (polarization, self-energy) on a 2x2 k-grid, "
                         "nen=512, nx=10, nm=16, ndiag=3")
+    p.add_argument("--dropin", action="store_true",
+                   help="time the per-energy drop-in green_RGF_RS called from every host thread at once, "
+                        "each on its own energies (the reference's `!$omp do` loop), against the batched "
+                        "entry point on the same energies and outputs")
     p.add_argument("--single", action="store_true",
                    help="one device-resident solve and exit (for profiler captures; prints no JSON)")
     return p.parse_args()
@@ -701,9 +705,81 @@ def run_gw(args):
     print(json.dumps(line), flush=True)
 
 
+def run_dropin(args):
+    """Per-energy drop-in throughput: host threads (all of them, as the
+    reference's `!$omp do ie` loop over green_RGF_RS at green_rgf.f90:
+    2916-2925) each call rgf_green_rgf_rs for two energies of the
+    rgf_nb128_nx100 workload with the reference's output set (ndens, pdens,
+    ldos, cur, GRi1, tr, tre) in pageable host memory; no context is passed,
+    so concurrent calls are coalesced into shared batches.  Timed by wall
+    clock from the first call to the last return, next to
+    rgf_solve_energies on the same energies and outputs."""
+    import threading
+    import torch
+    from liteqt_b200 import rgf
+    rgf.load()
+    d, E_all, temp = workload(args)
+    nthr = host_threads(args)
+    per = 2
+    nen = nthr * per
+    E = np.ascontiguousarray(E_all[np.linspace(0, len(E_all) - 1, nen).astype(int)])
+    nm, nx = args.nb, args.nx
+    mk = lambda: np.zeros((nx, nm, nm), complex)
+    outs = [dict(nd=mk(), pd=mk(), ld=mk(), gr=mk(), cur=np.zeros((nx, nm, nm)), tr=np.zeros(1), tre=np.zeros(1))
+            for _ in range(nthr)]
+    # the drop-in takes no options: both arms run the reference's own
+    # settings (device eta 0, lead eta 1e-3)
+    start = threading.Barrier(nthr + 1)
+
+    def work(k):
+        o = outs[k]
+        start.wait()
+        for i in range(per):
+            e = float(E[k * per + i])
+            rgf.green_RGF_RS(temp, nm, nx, e, MU, d.Hii, d.H1i, None, None, None, o["nd"], o["pd"], o["ld"],
+                             o["tr"], o["tre"], o["cur"], GRi1=o["gr"])
+    # warm-up: one call per thread (contexts, workspace, staging buffers)
+    warm = [threading.Thread(target=lambda k=k: rgf.green_RGF_RS(
+        temp, nm, nx, float(E[k]), MU, d.Hii, d.H1i, None, None, None, outs[k]["nd"], outs[k]["pd"],
+        outs[k]["ld"], outs[k]["tr"], outs[k]["tre"], outs[k]["cur"], GRi1=outs[k]["gr"])) for k in range(nthr)]
+    for t in warm:
+        t.start()
+    for t in warm:
+        t.join()
+    threads = [threading.Thread(target=work, args=(k,)) for k in range(nthr)]
+    for t in threads:
+        t.start()
+    start.wait()
+    t0 = time.perf_counter()
+    for t in threads:
+        t.join()
+    t_drop = time.perf_counter() - t0
+    # the batched entry point on the same energies, options and output set
+    shape = (nen, nx, nm, nm)
+    B = dict(ldos=np.zeros(shape, complex), ndens=np.zeros(shape, complex), pdens=np.zeros(shape, complex),
+             GRi1=np.zeros(shape, complex), cur=np.zeros(shape), tr=np.zeros(nen), tre=np.zeros(nen))
+    with rgf.Context(rgf.Options(want_T=False)) as ctx:
+        ctx.solve_energies(d.Hii, d.H1i, E, MU, temp, **B)
+        t1 = time.perf_counter()
+        ctx.solve_energies(d.Hii, d.H1i, E, MU, temp, **B)
+        t_batch = time.perf_counter() - t1
+    line = {"metric": "per-energy drop-in energy-pts/s (green_RGF_RS from every host thread)",
+            "value": nen / t_drop, "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+            "config": {"workload": f"rgf_nb{nm}_nx{nx}", "host_threads": nthr, "energies": nen,
+                       "options": "the reference's (device eta 0, lead eta 1e-3)",
+                       "outputs": ["ndens", "pdens", "ldos", "cur", "GRi1", "tr", "tre"],
+                       "memory": "pageable host arrays, as Fortran passes them"},
+            "batched_same_energies": {"value": nen / t_batch, "unit": UNIT,
+                                      "api": "rgf_solve_energies, host arrays"},
+            "dropin_vs_batched": t_batch / t_drop}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
-    if args.gw:
+    if args.dropin:
+        run_dropin(args)
+    elif args.gw:
         run_gw(args)
     elif args.w:
         run_w(args)

@@ -6,7 +6,10 @@
 // happens on the host, and there is no CPU fallback: if the CUDA path cannot
 // run, the call fails with RGF_E_CUDA / RGF_E_UNSUPPORTED.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <condition_variable>
+#include <cstdlib>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -723,6 +726,131 @@ struct TlsCtx {
 };
 thread_local TlsCtx g_tls;
 
+// ---- coalescing of concurrent per-energy calls
+// The reference calls green_RGF_RS once per energy from `!$omp do` threads
+// (green_rgf.f90:2916-2925).  Calls made without a context are queued
+// process-wide; the first caller that finds no batch being formed becomes
+// the leader: it keeps the queue open while new calls keep arriving (at most
+// a few milliseconds), then runs every queued call with its BOLTZ as one
+// rgf_solve_batch on a shared context -- one persistent launch, the shared
+// Hamiltonian staged once -- and wakes the callers, each of which returns
+// once its own outputs are written.  Calls that arrive meanwhile form the
+// next batch.  RGF_DROPIN_COALESCE=0 in the environment switches this off
+// (each thread then runs its call alone on a context of its own).
+struct Pending {
+  rgf_device dev;
+  rgf_task task;
+  double boltz;
+  int rc;
+  bool done;
+};
+struct Coalescer {
+  std::mutex mu;
+  std::condition_variable cv;
+  std::vector<Pending*> queue;
+  bool forming = false;
+  rgf_ctx* ctx[2] = {nullptr, nullptr};   // by BOLTZ: green_RGF_RS / RGF_G
+  double ctx_boltz[2] = {0.0, 0.0};
+  std::string last_error;
+};
+Coalescer& coalescer() {
+  static Coalescer* c = new Coalescer();   // never destroyed: process-lifetime contexts
+  return *c;
+}
+bool coalescing_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("RGF_DROPIN_COALESCE");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+bool same_device(const rgf_device& a, const rgf_device& b) {
+  return a.nm == b.nm && a.nx == b.nx && a.Hii == b.Hii && a.H1i == b.H1i && a.Sii == b.Sii &&
+         a.mu[0] == b.mu[0] && a.mu[1] == b.mu[1] && a.temp[0] == b.temp[0] && a.temp[1] == b.temp[1];
+}
+
+// Runs one batch (leader, without the lock): every call of `batch` shares
+// `boltz`.
+void run_batch(Coalescer& co, std::vector<Pending*>& batch, double boltz) {
+  int slot = 0;
+  {
+    std::lock_guard<std::mutex> g(co.mu);
+    for (slot = 0; slot < 2; slot++)
+      if (!co.ctx[slot] || co.ctx_boltz[slot] == boltz) break;
+  }
+  int rc = RGF_OK;
+  if (slot == 2) slot = 1;
+  if (!co.ctx[slot] || co.ctx_boltz[slot] != boltz) {
+    if (co.ctx[slot]) rgf_ctx_destroy(co.ctx[slot]);
+    co.ctx[slot] = nullptr;
+    rgf_opts o;
+    rgf_opts_default(&o);
+    o.boltz = boltz;
+    o.want_T = 0;
+    rc = rgf_ctx_create(&o, &co.ctx[slot]);
+    co.ctx_boltz[slot] = boltz;
+  }
+  if (rc == RGF_OK) {
+    std::vector<rgf_device> devs;
+    std::vector<rgf_task> tasks;
+    tasks.reserve(batch.size());
+    for (Pending* p : batch) {
+      int d = 0;
+      while (d < (int)devs.size() && !same_device(devs[d], p->dev)) d++;
+      if (d == (int)devs.size()) devs.push_back(p->dev);
+      rgf_task t = p->task;
+      t.device = d;
+      tasks.push_back(t);
+    }
+    rc = rgf_solve_batch(co.ctx[slot], devs.data(), (int32_t)devs.size(), tasks.data(), (int64_t)tasks.size(),
+                         nullptr, nullptr);
+    if (rc == RGF_E_STATUS) rc = RGF_OK;   // status bits only mean "SEVERE warning"
+  }
+  const std::string err = rc ? rgf_last_error() : std::string();
+  std::lock_guard<std::mutex> g(co.mu);
+  if (rc) co.last_error = err;
+  for (Pending* p : batch) {
+    p->rc = rc;
+    p->done = true;
+  }
+}
+
+int solve_coalesced(const rgf_device& dev, const rgf_task& task, double boltz) {
+  Coalescer& co = coalescer();
+  Pending me{dev, task, boltz, RGF_OK, false};
+  std::unique_lock<std::mutex> lk(co.mu);
+  co.queue.push_back(&me);
+  co.cv.notify_all();
+  while (!me.done) {
+    if (co.forming) {
+      co.cv.wait(lk);
+      continue;
+    }
+    co.forming = true;
+    // collection window: while calls keep arriving (each within 200 us of
+    // the previous), for at most 5 ms
+    const auto t0 = std::chrono::steady_clock::now();
+    size_t seen = co.queue.size();
+    for (;;) {
+      co.cv.wait_for(lk, std::chrono::microseconds(200));
+      const auto dt = std::chrono::steady_clock::now() - t0;
+      if (co.queue.size() == seen || dt > std::chrono::milliseconds(5)) break;
+      seen = co.queue.size();
+    }
+    std::vector<Pending*> batch, rest;
+    const double b = co.queue.front()->boltz;
+    for (Pending* p : co.queue) (p->boltz == b ? batch : rest).push_back(p);
+    co.queue.swap(rest);
+    lk.unlock();
+    run_batch(co, batch, b);
+    lk.lock();
+    co.forming = false;
+    co.cv.notify_all();
+  }
+  if (me.rc) g_last_error = co.last_error;
+  return me.rc;
+}
+
 rgf_ctx* default_ctx(double boltz, int* rc) {
   if (!g_tls.ctx) {
     rgf_opts o;
@@ -743,6 +871,34 @@ int solve_one(rgf_ctx* ctx, double boltz, const double* temp, const int64_t* nm,
   if (!temp || !nm || !nx || !E || !mu) return fail(RGF_E_ARG, "NULL scalar argument");
   int rc = RGF_OK;
   double saved_boltz = 0.0;
+  if (!ctx && coalescing_enabled()) {
+    rgf_device d;
+    std::memset(&d, 0, sizeof(d));
+    d.nm = *nm;
+    d.nx = *nx;
+    d.Sii = Sii;
+    d.Hii = Hii;
+    d.H1i = H1i;
+    d.mu[0] = mu[0];
+    d.mu[1] = mu[1];
+    d.temp[0] = temp[0];
+    d.temp[1] = temp[1];
+    rgf_task t;
+    std::memset(&t, 0, sizeof(t));
+    t.E = *E;
+    t.sigma_lesser = sl;
+    t.sigma_r = sr;
+    t.ldos = ldos;
+    t.ndens = ndens;
+    t.pdens = pdens;
+    t.GRi1 = GRi1;
+    t.GLi1 = GLi1;
+    t.GGi1 = GGi1;
+    t.cur = cur;
+    t.tr = tr;
+    t.tre = tre;
+    return solve_coalesced(d, t, boltz);
+  }
   if (!ctx) {
     ctx = default_ctx(boltz, &rc);
     if (!ctx) return rc;

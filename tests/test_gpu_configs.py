@@ -269,3 +269,44 @@ def test_indefinite_lead_broadening_takes_general_form(rgf):
     r = _oracle(d.Hii, d.H1i, E, O.Opts(), None, sr)
     x = O.rgf_batch(d.Hii, d.H1i, E, MU, _temp(), O.Opts(), sig_r=sr, extended=True)
     compare(g, r, nm, d.H1i, truth=x)
+
+
+def test_concurrent_drop_in_calls_are_coalesced(rgf):
+    """green_RGF_RS called per energy from 12 host threads at once, as the
+    reference's `!$omp do` loop does (green_rgf.f90:2916-2925), without a
+    context: the calls are queued and solved in shared batches.  Each
+    thread's outputs must equal the oracle's for its own energy, and the
+    solver must have run fewer launches than calls."""
+    import threading
+    from oracle import oracle as O
+    nm, nx, nthr = 16, 6, 12
+    d = S.make_device(nm, nx, seed=61)
+    E = np.linspace(-2.2, 2.1, nthr)
+    outs = []
+    for _ in range(nthr):
+        outs.append(dict(nd=np.zeros((nx, nm, nm), complex), pd=np.zeros((nx, nm, nm), complex),
+                         ld=np.zeros((nx, nm, nm), complex), gr=np.zeros((nx, nm, nm), complex),
+                         cur=np.zeros((nx, nm, nm)), tr=np.zeros(1), tre=np.zeros(1)))
+    errors = []
+    start = threading.Barrier(nthr)
+
+    def work(k):
+        try:
+            o = outs[k]
+            start.wait()
+            rgf.green_RGF_RS(_temp(), nm, nx, E[k], MU, d.Hii, d.H1i, None, None, None, o["nd"], o["pd"],
+                             o["ld"], o["tr"], o["tre"], o["cur"], GRi1=o["gr"])
+        except Exception as exc:  # noqa: BLE001 - reported below
+            errors.append(exc)
+    threads = [threading.Thread(target=work, args=(k,)) for k in range(nthr)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    r = _oracle(d.Hii, d.H1i, E, O.Opts())
+    g = dict(ldos=np.stack([o["ld"] for o in outs]), ndens=np.stack([o["nd"] for o in outs]),
+             pdens=np.stack([o["pd"] for o in outs]), GRi1=np.stack([o["gr"] for o in outs]),
+             cur=np.stack([o["cur"] for o in outs]), tr=np.array([o["tr"][0] for o in outs]),
+             tre=np.array([o["tre"][0] for o in outs]), T=r["T"])
+    compare(g, r, nm, d.H1i)
