@@ -56,6 +56,9 @@ def parse():
                         "split-integer block products on the int8 tensor cores (nb = 128).  The other form "
                         "is timed beside it on the same workload (mixed_vs_plain)")
     p.add_argument("--no-other", action="store_true", help="skip timing the other precision form")
+    p.add_argument("--full-outputs", action="store_true",
+                   help="request the reference's full output set per energy (G^R_ll, G^<_ll, G^>_ll, the bond "
+                        "current cur, G^R_{l,l+1}, tr, tre, T) instead of G^R_ll, G^<_ll, T, tr, tre")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-threads", type=int, default=0)
@@ -68,10 +71,22 @@ def parse():
     p.add_argument("--gw", action="store_true",
                    help="time the GW-loop convolutions (polarization, self-energy) on a 2x2 k-grid, "
                         "nen=512, nx=10, nm=16, ndiag=3")
+    p.add_argument("--gw-fft", action="store_true",
+                   help="time the FFT form of the GW convolutions (rgf_gw_polarization_fft / "
+                        "rgf_gw_self_energy_fft) at nk=16, nen=4096, nx=40, nm=64 on one rank's (i,j) slice")
     p.add_argument("--dropin", action="store_true",
                    help="time the per-energy drop-in green_RGF_RS called from every host thread at once, "
                         "each on its own energies (the reference's `!$omp do` loop), against the batched "
                         "entry point on the same energies and outputs")
+    p.add_argument("--uneven", action="store_true",
+                   help="uneven batch: 64 devices, Nx in {20..200}, nb in {32,64,128}, one graph-replayed "
+                        "persistent launch (--nen energies per device per step; default 32)")
+    p.add_argument("--band-edge", action="store_true",
+                   help="band-edge workload: nb=256, Nx=64, eta=1e-6, 10%% of a 4096-point grid within 1e-3 eV "
+                        "of lead subband edges (--nen sampled energies per step)")
+    p.add_argument("--aux", action="store_true",
+                   help="time the routines around the solve (redistribution transpose, calc_n_electron, "
+                        "calc_block_current, the writers' GPU sums) on arrays of the output size")
     p.add_argument("--single", action="store_true",
                    help="one device-resident solve and exit (for profiler captures; prints no JSON)")
     return p.parse_args()
@@ -88,7 +103,9 @@ def workload(args, world=1):
 def config(args, world):
     return {"workload": f"rgf_nb{args.nb}_nx{args.nx}", "nb": args.nb, "nx": args.nx,
             "energies_per_gpu_per_step": args.nen, "energy_range_eV": [-3.0, 3.0], "eta_eV": ETA,
-            "mu_eV": list(MU), "kT_eV": KT, "outputs": ["G^R_ll", "G^<_ll", "T", "tr", "tre"],
+            "mu_eV": list(MU), "kT_eV": KT,
+            "outputs": (["G^R_ll", "G^<_ll", "G^>_ll", "cur", "G^R_l,l+1", "T", "tr", "tre"]
+                        if args.full_outputs else ["G^R_ll", "G^<_ll", "T", "tr", "tre"]),
             "precision": args.precision, "parallelism": f"energy-sharded x{world}",
             "l2": "flushed between timed steps (256 MiB write)", "seed": 1}
 
@@ -179,9 +196,12 @@ def int8_peak_tops():
 
 
 def traffic_from_profiles(args):
-    """Per-task DRAM bytes of the solver kernel from the committed ncu summary,
-    scaled to a launch of --nen tasks (None if no summary exists)."""
-    path = os.path.join(ROOT, "profiles", f"rgf_fp64_nb{args.nb}_nx{args.nx}.md")
+    """Per-task DRAM bytes of the solver kernel (the form --precision names)
+    from the committed ncu summary, scaled to a launch of --nen tasks (None if
+    no summary exists or the output set is not the summary's)."""
+    if args.full_outputs:
+        return None
+    path = os.path.join(ROOT, "profiles", f"rgf_{args.precision}_nb{args.nb}_nx{args.nx}.md")
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -288,12 +308,16 @@ def run_ours(args):
     T = torch.empty(nen, dtype=torch.float64, device=dev)
     tr = torch.empty_like(T)
     tre = torch.empty_like(T)
+    extra = {}
+    if args.full_outputs:
+        extra = dict(pdens=torch.empty_like(ldos), GRi1=torch.empty_like(ldos),
+                     cur=torch.empty(shape, dtype=torch.float64, device=dev))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     peak = zgemm_peak_tflops(torch, dev)
 
     def step_dev():
         ctx.solve_energies(Hii, H1i, E, MU, temp, ldos=ldos, ndens=ndens, tr=tr, tre=tre, T=T,
-                           stream=sh)
+                           stream=sh, **extra)
 
     def barrier():
         torch.cuda.synchronize(dev)
@@ -342,7 +366,7 @@ def run_ours(args):
     # task, identical to the reference's), summed over the launch's energies.
     info = np.zeros(nen, rgf.INFO_DTYPE)
     ctx.solve_energies(Hii, H1i, E, MU, temp, ldos=ldos, ndens=ndens, tr=tr, tre=tre, T=T,
-                       info=info, stream=sh)
+                       info=info, stream=sh, **extra)
     torch.cuda.synchronize(dev)
     nsum = info["sancho_iters_left"].astype(np.float64) + info["sancho_iters_right"]
     alg_flops = float(np.sum(8.0 * nb ** 3 * ((28 * nx - 18 + 6 * nsum) + (nx + 4 + nsum))))
@@ -390,6 +414,8 @@ def run_ours(args):
         tre_h = torch.empty_like(T_h).pin_memory()
         arrs = dict(ldos=ldos_h.numpy(), ndens=ndens_h.numpy(), T=T_h.numpy(), tr=tr_h.numpy(),
                     tre=tre_h.numpy())
+        extra_h = {k: torch.empty(v.shape, dtype=v.dtype).pin_memory() for k, v in extra.items()}
+        arrs.update({k: v.numpy() for k, v in extra_h.items()})
 
         def step_host():
             ctx.solve_energies(Hii_h.numpy(), H1i_h.numpy(), E, MU, temp, stream=sh, **arrs)
@@ -409,7 +435,8 @@ def run_ours(args):
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             t_e2e = float(tt.item())
         bi = Hii_h.numel() * 16 + H1i_h.numel() * 16
-        bo = (ldos_h.numel() + ndens_h.numel()) * 16 + 3 * nen * 8
+        bo = (ldos_h.numel() + ndens_h.numel()) * 16 + 3 * nen * 8 + \
+            sum(v.numel() * v.element_size() for v in extra_h.values())
         e2e = {"value": nen * world * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": bi,
                "d2h_bytes_per_step": bo, "ms_per_step": 1e3 * t_e2e / args.steps,
                "api": "rgf_solve_energies (C ABI) with pinned host arrays"}
@@ -419,7 +446,7 @@ def run_ours(args):
     # the other precision form on the same workload and timing, for the ratio
     # the metric names (mixed vs plain FP64)
     other = None
-    if not args.no_other and nb == 128:
+    if not args.no_other and nb == 128 and not args.full_outputs:
         oprec = rgf.RGF_PREC_FP64 if mixed else rgf.RGF_PREC_MIXED
         ctx2 = rgf.Context(rgf.Options(device=local, eta_dev=ETA, eta_lead=ETA, precision=oprec))
         with torch.cuda.stream(stream):
@@ -488,11 +515,14 @@ def run_single(args):
     ldos = torch.empty(shape, dtype=torch.complex128, device=dev)
     ndens = torch.empty_like(ldos)
     T = torch.empty(args.nen, dtype=torch.float64, device=dev)
-    with rgf.Context(rgf.Options(eta_dev=ETA, eta_lead=ETA)) as ctx:
+    mixed = args.precision == "mixed"
+    opts = rgf.Options(eta_dev=ETA, eta_lead=ETA, precision=rgf.RGF_PREC_MIXED if mixed else rgf.RGF_PREC_FP64)
+    with rgf.Context(opts) as ctx:
         ctx.solve_energies(Hii, H1i, E, MU, temp, ldos=ldos, ndens=ndens, T=T)
         st = ctx.stats()
-    print(f"single solve nb={args.nb} nx={args.nx} nen={args.nen}: kernel {st['last_kernel_ms']:.1f} ms, "
-          f"{st['last_flops'] / st['last_kernel_ms'] / 1e9:.2f} TFLOP/s executed")
+    print(f"single {args.precision} solve nb={args.nb} nx={args.nx} nen={args.nen}: kernel "
+          f"{st['last_kernel_ms']:.1f} ms, {st['last_flops'] / st['last_kernel_ms'] / 1e9:.2f} TFLOP/s executed "
+          f"in FP64, {st['last_int8_ops'] / st['last_kernel_ms'] / 1e9:.1f} int8 TOP/s")
 
 
 def run_adjoint(args):
@@ -705,6 +735,84 @@ def run_gw(args):
     print(json.dumps(line), flush=True)
 
 
+def run_gw_fft(args):
+    """FFT form of the GW convolutions at the GW workload's sizes: 4 x 4
+    k-grid, nen = 4096, nx = 40, nm = 64, ndiag = 3, on one rank's slice of
+    128 (i,j) elements (columns 30-31 of the 64 x 64 block: 14 banded
+    elements, 560 (i,j, block) lines) in the *_by_blocks layout.  One step =
+    rgf_gw_polarization_fft + rgf_gw_self_energy_fft on seeded inputs.
+    Reported: lines per second and the time of a whole iteration's
+    convolutions (all 436 banded elements x 40 blocks = 17 440 lines) at
+    that rate.  Roofline: HBM, algorithmic bytes = the banded lines' inputs
+    read once (5 + 6 series) plus every output element written once (the
+    zeros outside the band included)."""
+    import torch
+    from liteqt_b200 import rgf
+    nky, nkz, nen, nx, nm, ndiag = 4, 4, 4096, 40, 64, 3
+    nk = nky * nkz
+    nij, first_ij = 128, 29 * nm + 1
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    g = torch.Generator(device=dev).manual_seed(11)
+    shape = (nij, nx, nk, nen)
+
+    def rnd():
+        return torch.complex(torch.randn(shape, generator=g, device=dev, dtype=torch.float64),
+                             torch.randn(shape, generator=g, device=dev, dtype=torch.float64))
+    GL, GG, GR, GLt, GGt, WL, WG, WR = (rnd() for _ in range(8))
+    out = [torch.empty_like(GL) for _ in range(3)]
+    band = sum(1 for i in range(nij) if max((i + first_ij - 1) % nm + 1 - ndiag, 1) <= (i + first_ij - 1) // nm + 1
+               <= min(nm, (i + first_ij - 1) % nm + 1 + ndiag))
+    lines = band * nx
+    full_lines = (nm * (2 * ndiag + 1) - ndiag * (ndiag + 1)) * nx
+    stream = torch.cuda.Stream(device=dev)
+    ctx = rgf.Context(rgf.Options())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    tp, ts = [], []
+    with torch.cuda.stream(stream):
+        for it in range(args.warmup + args.steps):
+            flush.fill_(1.0)
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e[0].record(stream)
+            ctx.gw_polarization_fft(GL, GG, GR, GLt, GGt, PL=out[0], PG=out[1], PR=out[2], nky=nky, nkz=nkz, nm=nm,
+                                    ndiag=ndiag, first_ij=first_ij, dEn=8.0 / (nen - 1), spindeg=2.0,
+                                    stream=stream.cuda_stream)
+            e[1].record(stream)
+            ctx.gw_self_energy_fft(GL, GG, GR, WL, WG, WR, SL=out[0], SG=out[1], SR=out[2], nky=nky, nkz=nkz,
+                                   nm=nm, ndiag=ndiag, first_ij=first_ij, dEn=8.0 / (nen - 1),
+                                   stream=stream.cuda_stream)
+            e[2].record(stream)
+            e[2].synchronize()
+            if it >= args.warmup:
+                tp.append(e[0].elapsed_time(e[1]))
+                ts.append(e[1].elapsed_time(e[2]))
+    ctx.close()
+    mp, ms_ = float(np.mean(tp)), float(np.mean(ts))
+    series = nk * nen * 16
+    alg = lines * series * (5 + 6) + 2 * 3 * nij * nx * series
+    peak = None
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        peak = float(json.load(open(path)).get("hbm_gbs"))
+    peak_src = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    gbs = alg / ((mp + ms_) * 1e-3) / 1e9
+    line = {"metric": "GW FFT convolutions: (i,j,block) lines per second (P + Sigma)",
+            "value": lines / ((mp + ms_) * 1e-3), "unit": "lines/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mp + ms_, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c16", "data": "synthetic",
+            "config": {"workload": "gw_fft_nk16_nen4096_nx40_nm64_nd3", "nky": nky, "nkz": nkz, "nen": nen,
+                       "nx": nx, "nm": nm, "ndiag": ndiag, "nij_slice": nij, "first_ij": first_ij,
+                       "banded_in_slice": band, "lines_per_step": lines, "fft_length": 8192,
+                       "l2": "flushed before each step (256 MiB write)"},
+            "polarization_ms": mp, "self_energy_ms": ms_,
+            "full_iteration": {"lines": full_lines, "s": full_lines / (lines / ((mp + ms_) * 1e-3)),
+                               "note": "every banded (i,j) element of the 64 x 64 block, 40 blocks"},
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                         "traffic": None, "peak_source": peak_src, "algorithmic_bytes_per_step": alg}}
+    print(json.dumps(line), flush=True)
+
+
 def run_dropin(args):
     """Per-energy drop-in throughput: host threads (all of them, as the
     reference's `!$omp do ie` loop over green_RGF_RS at green_rgf.f90:
@@ -775,9 +883,264 @@ def run_dropin(args):
     print(json.dumps(line), flush=True)
 
 
+def _timed_steps(torch, fn, steps, warmup, flush, stream):
+    """Device time (ms) of each of `steps` calls of fn after `warmup` calls,
+    CUDA events on `stream`, L2 flushed before each timed call."""
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(steps):
+            flush.fill_(1.0)
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            fn()
+            e.record(stream)
+            e.synchronize()
+            ms.append(s.elapsed_time(e))
+    return ms
+
+
+def run_uneven(args):
+    """Uneven batch in one persistent launch: 64 seeded devices with Nx
+    uniform in {20..200} and nb uniform in {32, 64, 128} (the H construction
+    of the main workload), --nen energies per device per step on the uniform
+    grid of [-3, 3] eV (the configuration's 2048 per device are 32 such
+    steps), eta = 1e-5, outputs G^R_ll, G^<_ll, T, tr, tre in HBM.  The
+    context is autotuned for the three block sizes first; one step replays
+    a CUDA-graph plan of the whole launch."""
+    import torch
+    from liteqt_b200 import rgf, synthetic as S
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    rng = np.random.default_rng(2)
+    ndev = 64
+    nxs = rng.integers(20, 201, ndev)
+    nbs = rng.choice([32, 64, 128], ndev)
+    nen = args.nen if args.nen != 296 else 32
+    temp = (S.temperature_for_kT(KT),) * 2
+    ctx = rgf.Context(rgf.Options(eta_dev=ETA, eta_lead=ETA))
+    keep, cdevs, ctasks, tuned = [], [], [], {}
+    for i in range(ndev):
+        d = S.make_device(int(nbs[i]), int(nxs[i]), seed=1000 + i)
+        if d.nm not in tuned:
+            tuned[d.nm] = ctx.autotune(d.Hii, d.H1i, MU, temp)
+        Hii, H1i = torch.from_numpy(d.Hii).to(dev), torch.from_numpy(d.H1i).to(dev)
+        cd = rgf.c_device()
+        cd.nm, cd.nx = d.nm, d.nx
+        cd.Hii, cd.H1i = Hii.data_ptr(), H1i.data_ptr()
+        cd.mu[0], cd.mu[1] = MU
+        cd.temp[0], cd.temp[1] = temp
+        cdevs.append(cd)
+        o = {k: torch.empty((nen, d.nx, d.nm, d.nm), dtype=torch.complex128, device=dev)
+             for k in ("ldos", "ndens")}
+        for k in ("tr", "tre", "T"):
+            o[k] = torch.empty(nen, dtype=torch.float64, device=dev)
+        keep += [Hii, H1i, o]
+        E = S.energy_grid(nen, -3.0, 3.0)
+        for ie in range(nen):
+            t = rgf.c_task()
+            t.device, t.E = i, float(E[ie])
+            t.ldos, t.ndens = o["ldos"][ie].data_ptr(), o["ndens"][ie].data_ptr()
+            t.tr, t.tre, t.T = o["tr"][ie:].data_ptr(), o["tre"][ie:].data_ptr(), o["T"][ie:].data_ptr()
+            ctasks.append(t)
+    plan = ctx.plan(cdevs, ctasks)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms = _timed_steps(torch, lambda: plan.execute(stream=stream.cuda_stream), args.steps, max(3, args.warmup),
+                      flush, stream)
+    clk = clocks.stop()
+    info = np.zeros(len(ctasks), rgf.INFO_DTYPE)
+    plan.execute(info=info, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    plan.close()
+    ntask = len(ctasks)
+    nb_t = np.repeat(nbs, nen).astype(np.float64)
+    nx_t = np.repeat(nxs, nen).astype(np.float64)
+    nsum = info["sancho_iters_left"].astype(np.float64) + info["sancho_iters_right"]
+    alg = float(np.sum(8.0 * nb_t ** 3 * ((28 * nx_t - 18 + 6 * nsum) + (nx_t + 4 + nsum))))
+    peak = zgemm_peak_tflops(torch, dev)
+    ctx.close()
+    m = float(np.mean(ms))
+    line = {"metric": "uneven batched RGF energy-pts/s (one persistent launch, graph replay)",
+            "value": ntask / (m * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": m, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "rgf_uneven_64dev", "devices": ndev, "nx": [int(v) for v in nxs],
+                       "nb": [int(v) for v in nbs], "energies_per_device_per_step": nen, "eta_eV": ETA,
+                       "outputs": ["G^R_ll", "G^<_ll", "T", "tr", "tre"], "tasks_per_step": ntask,
+                       "full_configuration_s": 2048 * ndev / (ntask / (m * 1e-3)),
+                       "autotuned": {str(k): [v["variant"], v["ctas_per_sm"]] for k, v in tuned.items()},
+                       "l2": "flushed between timed steps (256 MiB write)", "seed": 2},
+            "status_nonzero": int(np.count_nonzero(info["status"])),
+            "roofline": {"bound": "tensor", "achieved": alg / (m * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                         "frac": alg / (m * 1e-3) / 1e12 / peak, "traffic": None,
+                         "peak_source": "cuBLAS ZGEMM 4096^3 measured live",
+                         "algorithmic_flops_per_launch": alg},
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
+def run_band_edge(args):
+    """Band-edge workload: nb = 256, Nx = 64, eta = 1e-6 in device and
+    leads, energies from a 4096-point grid of [-3, 3] eV with 10 % of them
+    within 1e-3 eV of a lead subband edge; one step solves --nen of them (a
+    seeded sample that keeps the 10 %), outputs G^R_ll, G^<_ll, T, tr, tre.
+    Plain FP64 (the split-integer form is built for nb = 128)."""
+    import torch
+    from liteqt_b200 import rgf, synthetic as S
+    nb, nx, eta = 256, 64, 1e-6
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    d = S.make_device(nb, nx, seed=3)
+    edges = S.lead_band_edges(d.Hii, d.H1i, 0, 128)
+    grid = S.band_edge_energy_grid(4096, edges, -3.0, 3.0, 0.1, 1e-3, seed=5)
+    near = np.min(np.abs(grid[:, None] - edges[None, :]), axis=1) <= 1e-3
+    nen = args.nen
+    pick = np.sort(np.random.default_rng(7).choice(len(grid), nen, replace=False))
+    E = np.ascontiguousarray(grid[pick])
+    temp = (S.temperature_for_kT(KT),) * 2
+    ctx = rgf.Context(rgf.Options(eta_dev=eta, eta_lead=eta))
+    Hii, H1i = torch.from_numpy(d.Hii).to(dev), torch.from_numpy(d.H1i).to(dev)
+    o = {k: torch.empty((nen, nx, nb, nb), dtype=torch.complex128, device=dev) for k in ("ldos", "ndens")}
+    for k in ("tr", "tre", "T"):
+        o[k] = torch.empty(nen, dtype=torch.float64, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms = _timed_steps(torch, lambda: ctx.solve_energies(Hii, H1i, E, MU, temp, stream=stream.cuda_stream, **o),
+                      args.steps, max(3, args.warmup), flush, stream)
+    clk = clocks.stop()
+    info = np.zeros(nen, rgf.INFO_DTYPE)
+    ctx.solve_energies(Hii, H1i, E, MU, temp, info=info, stream=stream.cuda_stream, **o)
+    torch.cuda.synchronize()
+    peak = zgemm_peak_tflops(torch, dev)
+    ctx.close()
+    nsum = info["sancho_iters_left"].astype(np.float64) + info["sancho_iters_right"]
+    alg = float(np.sum(8.0 * nb ** 3 * ((28 * nx - 18 + 6 * nsum) + (nx + 4 + nsum))))
+    m = float(np.mean(ms))
+    line = {"metric": "band-edge RGF energy-pts/s (nb 256, eta 1e-6)", "value": nen / (m * 1e-3), "unit": UNIT,
+            "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": m,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "rgf_band_edge_nb256_nx64", "nb": nb, "nx": nx, "eta_eV": eta,
+                       "grid_points": len(grid), "near_edge_in_grid": int(near.sum()),
+                       "energies_per_step": nen, "near_edge_in_step": int(near[pick].sum()),
+                       "outputs": ["G^R_ll", "G^<_ll", "T", "tr", "tre"],
+                       "full_grid_s": len(grid) / (nen / (m * 1e-3)),
+                       "l2": "flushed between timed steps (256 MiB write)", "seed": 3},
+            "sancho_iters": {"mean": float(np.mean(nsum) / 2), "max": int(max(info["sancho_iters_left"].max(),
+                                                                             info["sancho_iters_right"].max()))},
+            "status_nonzero": int(np.count_nonzero(info["status"])),
+            "roofline": {"bound": "tensor", "achieved": alg / (m * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                         "frac": alg / (m * 1e-3) / 1e12 / peak, "traffic": None,
+                         "peak_source": "cuBLAS ZGEMM 4096^3 measured live",
+                         "algorithmic_flops_per_launch": alg},
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
+def run_aux(args):
+    """The HBM-bound routines around the solve on arrays of the benchmark's
+    output size (G (nen, nx, nb, nb) complex(8), seeded): the GW loop's
+    energy -> (i,j) transpose (rgf_permute_c16, energies_to_ijs_2's second
+    RESHAPE as an 8-rank run has it), calc_n_electron, calc_block_current
+    (4 sub-blocks of nb/4) and the writers' GPU sums (write_spectrum's
+    diagonal traces, write_dos_summed_over_k).  Each routine is timed with
+    CUDA events through its public entry point (host outputs included), the
+    L2 flushed before each call.  Algorithmic bytes: the transpose reads and
+    writes the array once; the integrals and traces read the elements they
+    sum (16 B each; the diagonal gathers touch one 32-byte sector per
+    element)."""
+    import torch
+    from liteqt_b200 import rgf, writers as Wr
+    nen, nx, nm = args.nen, args.nx, args.nb
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    g = torch.Generator(device=dev).manual_seed(5)
+    shape = (1, nen, nx, nm, nm)
+
+    def rnd():
+        return torch.complex(torch.randn(shape, generator=g, device=dev, dtype=torch.float64),
+                             torch.randn(shape, generator=g, device=dev, dtype=torch.float64))
+    Gl, Gg = rnd(), rnd()
+    H = torch.complex(torch.randn((nx, nm, nm), generator=g, device=dev, dtype=torch.float64),
+                      torch.randn((nx, nm, nm), generator=g, device=dev, dtype=torch.float64))
+    dst = torch.empty_like(Gl)
+    E = np.linspace(-3.0, 3.0, nen)
+    midgap = np.zeros(nx)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    ranks = 8
+    nij = nm * nm // ranks
+    src_shape, order = (nij, nx, nen, 1, ranks), (5, 4, 1, 3, 2)
+    ns = 4
+    sub = nm // ns
+    tmp = tempfile.mkdtemp()
+    ctx = rgf.Context(rgf.Options())
+    arr = 16 * Gl.numel()
+    calls = {
+        "permute_c16": (lambda: ctx.permute(Gl, dst, src_shape, order), 2.0 * arr),
+        "calc_n_electron": (lambda: ctx.calc_n_electron(Gl, Gg, E, midgap), 16.0 * nen * nx * nm),
+        "calc_block_current": (lambda: ctx.calc_block_current(H, Gl[0], E, 2.0, sub, ns),
+                               2 * 16.0 * nen * nx * (ns - 1) * sub * sub),
+        "write_spectrum": (lambda: Wr.write_spectrum(ctx, os.path.join(tmp, "ldos"), 1, Gl, E, nx, sub, ns,
+                                                     1.0, (1.0, 1.0)), 16.0 * nen * nx * nm),
+        "write_dos": (lambda: Wr.write_dos_summed_over_k(ctx, os.path.join(tmp, "dos"), 1, Gl, E, 1, nx, sub,
+                                                          ns, 1.0), 16.0 * nen * nx * nm),
+    }
+    peak = None
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        peak = float(json.load(open(path)).get("hbm_gbs"))
+    peak_src = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    out = {}
+    for name, (fn, nbytes) in calls.items():
+        ms = []
+        for it in range(args.warmup + args.steps):
+            flush.fill_(1.0)
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record()
+            fn()
+            e.record()
+            e.synchronize()
+            if it >= args.warmup:
+                ms.append(s.elapsed_time(e))
+        m = float(np.mean(ms))
+        out[name] = {"ms": m, "alg_bytes": nbytes, "GB/s": nbytes / (m * 1e-3) / 1e9,
+                     "frac": nbytes / (m * 1e-3) / 1e9 / peak}
+    ctx.close()
+    for f in os.listdir(tmp):
+        os.unlink(os.path.join(tmp, f))
+    os.rmdir(tmp)
+    top = out["permute_c16"]
+    line = {"metric": "redistribution transpose GB/s (energies_to_ijs_2)", "value": top["GB/s"], "unit": "GB/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": top["ms"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c16", "data": "synthetic",
+            "config": {"workload": f"aux_nb{nm}_nx{nx}_nen{nen}", "array_bytes": arr, "ranks_in_layout": ranks,
+                       "sub_blocks": ns, "l2": "flushed before each call (256 MiB write)"},
+            "routines": out,
+            "roofline": {"bound": "hbm", "achieved": top["GB/s"], "peak": peak, "unit": "GB/s",
+                         "frac": top["frac"], "traffic": None, "peak_source": peak_src}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
-    if args.dropin:
+    if args.aux:
+        run_aux(args)
+    elif args.uneven:
+        run_uneven(args)
+    elif args.band_edge:
+        run_band_edge(args)
+    elif args.gw_fft:
+        run_gw_fft(args)
+    elif args.dropin:
         run_dropin(args)
     elif args.gw:
         run_gw(args)

@@ -352,6 +352,39 @@ RGF_API int rgf_gw_self_energy(rgf_ctx* ctx, int64_t nm, int64_t nx, int64_t nen
                                rgf_c16* Sigma_greater_gw, rgf_c16* Sigma_r_gw, void* stream);
 RGF_API const char* rgf_gw_last_error(void);
 
+/* FFT form of the GW convolutions as the production loop with energy <-> (i,j)
+ * redistribution computes them (green_rgf_solve_gw_ephoton_3d_ijs,
+ * src/green_rgf.f90:1397-1473 and :1598-1678; corr1d2 / conv1d2 with method
+ * 'fft', src/fft_mod.f90:56-89, :175-212): the rank's slice of nij (i,j)
+ * elements, global indices first_ij .. first_ij+nij-1 (1-based, column-major
+ * (i,j) of an nm x nm block), after energies_to_ijs_2.  Arrays are device
+ * memory in the *_by_blocks layout (nen, nk, nx, nij) complex(8), nk = nky*nkz,
+ * ik = ikz + nkz*(iky-1); nen even.  Elements outside the band |i-j| <= ndiag
+ * are written as zeros.  dEn = En(2) - En(1).
+ *   rgf_gw_polarization_fft: P^< = sum_k corr(G^<_k, G^>_t,kd), P^> likewise,
+ *     P^R = sum_k corr(G^<_k, conj(G^R_kd)) + corr(G^R_k, G^<_t,kd), times
+ *     -i dEn/(2 pi) spindeg/nk; G^<_t, G^>_t are the transposed G^<, G^>
+ *     (element (j,i)) in the same layout;
+ *   rgf_gw_self_energy_fft: Sigma^< = sum_q conv(G^<_kd, W^<_q), Sigma^>
+ *     likewise, Sigma^R = conv(G^<, W^R) + conv(G^R, W^<) + conv(G^R, W^R),
+ *     times i dEn/(2 pi)/nk, then Sigma^R = Re + i Im(Sigma^> - Sigma^<)/2.
+ * The transforms are cuFFT's, in chunks of (i,j, ix) lines within a few GB of
+ * stream-ordered scratch (RGF_GW_FFT_CHUNK sets the lines per chunk).
+ * Stream-ordered on `stream`; returns when the results are written.  Error
+ * text: rgf_gw_fft_last_error(). */
+RGF_API int rgf_gw_polarization_fft(rgf_ctx* ctx, int64_t nm, int64_t nx, int64_t nen, int64_t nky,
+                                    int64_t nkz, int64_t ndiag, int64_t nij, int64_t first_ij, double dEn,
+                                    double spindeg, const rgf_c16* G_lesser, const rgf_c16* G_greater,
+                                    const rgf_c16* G_r, const rgf_c16* G_lesser_t, const rgf_c16* G_greater_t,
+                                    rgf_c16* P_lesser, rgf_c16* P_greater, rgf_c16* P_retarded, void* stream);
+RGF_API int rgf_gw_self_energy_fft(rgf_ctx* ctx, int64_t nm, int64_t nx, int64_t nen, int64_t nky,
+                                   int64_t nkz, int64_t ndiag, int64_t nij, int64_t first_ij, double dEn,
+                                   const rgf_c16* G_lesser, const rgf_c16* G_greater, const rgf_c16* G_r,
+                                   const rgf_c16* W_lesser, const rgf_c16* W_greater, const rgf_c16* W_retarded,
+                                   rgf_c16* Sigma_lesser_new, rgf_c16* Sigma_greater_new, rgf_c16* Sigma_r_new,
+                                   void* stream);
+RGF_API const char* rgf_gw_fft_last_error(void);
+
 /* Local transpose of the GW loop's energy <-> (i,j) redistribution
  * (energies_to_ijs_2 / ijs_to_energies_2, src/green_rgf.f90:243-329):
  * dst = RESHAPE(src, dst_shape, ORDER=order) with Fortran's meaning, for pure

@@ -97,8 +97,12 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     if force or _stale(LIB, objs):
         # device link of the relocatable objects + host link; exported symbols:
         # the extern "C" rgf_* entry points (visibility default via the map)
+        # cuFFT (the GW convolutions' FFT form) from the CUDA toolkit, found at
+        # run time through the toolkit's library directory
+        cudalib = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(nvcc()))), "lib64")
         cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-rdc=true", "-shared", "-o", LIB, *objs,
-               "-Xlinker", "--version-script=" + os.path.join(CSRC, "exports.map")]
+               "-Xlinker", "--version-script=" + os.path.join(CSRC, "exports.map"),
+               "-L" + cudalib, "-lcufft", "-Xlinker", "-rpath=" + cudalib]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)

@@ -5,9 +5,11 @@
 //   calc_n_electron   electron / hole density per block from Im G^<_jj and
 //                     Im G^>_jj, split at midgap (src/green_rgf.f90:3920-3945)
 //
-// Both are HBM-bound reductions.  Each output value is summed by one CTA with
-// a fixed thread-to-element mapping and a fixed reduction tree, so results are
-// bit-reproducible run to run.
+// All are HBM-bound reductions with a fixed thread-to-element mapping and a
+// fixed reduction order, so results are bit-reproducible run to run.  They
+// run on the legacy default stream (ordered after the caller's work there);
+// temporaries are stream-ordered allocations, which neither synchronise the
+// device nor return memory to the driver between calls.
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -30,41 +32,57 @@ __global__ void sum_kernel(const double* x, int64_t n, double* out) {
   if (threadIdx.x == 0) *out = s;
 }
 
-// One CTA per block ix.  G arrays (nm,nm,nx,nen,nk) column-major.
-__global__ void n_electron_kernel(const double2* Gl, const double2* Gg, int64_t nen, const double* E,
-                                  int64_t nm, int64_t nk, int64_t nx, const double* midgap,
-                                  double* nelec, double* pelec) {
+// calc_n_electron in two passes.  Pass 1: CTA (ix, c) sums chunk c of block
+// ix's (energy, k) pairs -- pairs c*per .. (c+1)*per-1 in the order
+// i + nen*ik, every diagonal element j of each -- into partial[ix][c]
+// (fixed thread mapping and reduction tree).  Pass 2: one thread per block
+// adds its chunks in order and applies dE dK.  G arrays (nm,nm,nx,nen,nk)
+// column-major.
+__global__ void n_electron_partial_kernel(const double2* Gl, const double2* Gg, int64_t nen, const double* E,
+                                          int64_t nm, int64_t nk, int64_t nx, int64_t per, const double* midgap,
+                                          double2* partial) {
   __shared__ rgf::SmemRed red;
-  const int64_t ix = blockIdx.x;
+  const int64_t ix = blockIdx.x, c = blockIdx.y, nch = gridDim.y;
   const size_t n2 = (size_t)nm * nm;
   const double mg = midgap[ix];
+  const int64_t p0 = c * per, p1 = (p0 + per < nen * nk) ? p0 + per : nen * nk;
   double ne = 0.0, pe = 0.0;
-  const int64_t total = nen * nk * nm;
+  const int64_t total = (p1 - p0) * nm;
   for (int64_t q = threadIdx.x; q < total; q += rgf::kThreads) {
     const int64_t j = q % nm;
-    const int64_t r = q / nm;
-    const int64_t ik = r % nk;
-    const int64_t i = r / nk;
+    const int64_t pr = p0 + q / nm;            // pair index i + nen * ik
+    const int64_t i = pr % nen, ik = pr / nen;
     const size_t off = (size_t)j * (nm + 1) + ix * n2 + (size_t)nx * n2 * (i + (size_t)nen * ik);
     if (E[i] > mg) ne += Gl[off].y;
     else pe -= Gg[off].y;
   }
   const double2 s = rgf::block_sum2(make_double2(ne, pe), red);
-  if (threadIdx.x == 0) {
-    const double dE = (E[1] - E[0]) / (2.0 * kPi);
-    const double dK = 2.0 * kPi / (double)nk;
-    nelec[ix] = s.x * dE * dK;
-    pelec[ix] = s.y * dE * dK;
+  if (threadIdx.x == 0) partial[ix * nch + c] = s;
+}
+
+__global__ void n_electron_combine_kernel(const double2* partial, int64_t nch, int64_t nx, const double* E,
+                                          int64_t nk, double* nelec, double* pelec) {
+  const int64_t ix = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ix >= nx) return;
+  double ne = 0.0, pe = 0.0;
+  for (int64_t c = 0; c < nch; c++) {
+    ne += partial[ix * nch + c].x;
+    pe += partial[ix * nch + c].y;
   }
+  const double dE = (E[1] - E[0]) / (2.0 * kPi);
+  const double dK = 2.0 * kPi / (double)nk;
+  nelec[ix] = ne * dE * dK;
+  pelec[ix] = pe * dE * dK;
 }
 
 // calc_block_current (src/green_rgf.f90:4602-4640): one thread per output
 // element (io, jo, l); energies summed in the reference's order.  The last
 // sub-block of a block repeats the previous one (ib = ns - 1), as the
 // reference's stale matrix does; ns = 1 gives zeros.
-__global__ void block_current_kernel(const double2* H, const double2* G, int64_t nen, const double* en,
-                                     double scale, int64_t nb, int64_t ns, int64_t nm, int64_t nx,
-                                     double* tot_cur, double* tot_ecur, double* jdens) {
+__global__ void block_current_kernel(const double2* __restrict__ H, const double2* __restrict__ G, int64_t nen,
+                                     const double* __restrict__ en, double scale, int64_t nb, int64_t ns,
+                                     int64_t nm, int64_t nx, double* __restrict__ tot_cur,
+                                     double* __restrict__ tot_ecur, double* __restrict__ jdens) {
   const int64_t b2 = nb * nb, nl = nx * ns;
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= b2 * nl) return;
@@ -74,6 +92,7 @@ __global__ void block_current_kernel(const double2* H, const double2* G, int64_t
   const int64_t ib = (ibm == ns - 1) ? ns - 2 : ibm;   // last sub-block repeats the previous one
   const size_t n2 = (size_t)nm * nm;
   double tc = 0.0, te = 0.0;
+#pragma unroll 4
   for (int64_t ie = 0; ie < nen; ie++) {
     double v = 0.0;
     if (ib >= 0) {
@@ -100,18 +119,27 @@ bool is_dev(const void* p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
-// device copy of a (host or device) input array; frees on destruction
+// Device copy of a (host or device) input array on the legacy default
+// stream (stream-ordered allocation); freed, stream-ordered, on destruction.
 struct In {
   const void* d = nullptr;
   void* own = nullptr;
   cudaError_t err = cudaSuccess;
   In(const void* p, size_t bytes) {
     if (is_dev(p)) { d = p; return; }
-    err = cudaMalloc(&own, bytes);
-    if (err == cudaSuccess) err = cudaMemcpy(own, p, bytes, cudaMemcpyHostToDevice);
+    err = cudaMallocAsync(&own, bytes, 0);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(own, p, bytes, cudaMemcpyHostToDevice, 0);
     d = own;
   }
-  ~In() { if (own) cudaFree(own); }
+  ~In() { if (own) cudaFreeAsync(own, 0); }
+};
+
+// Stream-ordered device scratch of `bytes` (legacy default stream).
+struct Tmp {
+  void* p = nullptr;
+  cudaError_t err;
+  explicit Tmp(size_t bytes) { err = cudaMallocAsync(&p, bytes, 0); }
+  ~Tmp() { if (p) cudaFreeAsync(p, 0); }
 };
 
 }  // namespace
@@ -121,12 +149,11 @@ extern "C" int rgf_terminal_current(rgf_ctx* ctx, const double* tr, int64_t nen,
   if (!ctx || !tr || !current || nen < 1 || nk < 1) return RGF_E_ARG;
   In x(tr, sizeof(double) * nen);
   if (x.err != cudaSuccess) return RGF_E_CUDA;
-  double* d_out = nullptr;
-  if (cudaMalloc(&d_out, sizeof(double)) != cudaSuccess) return RGF_E_NOMEM;
-  sum_kernel<<<1, rgf::kThreads>>>((const double*)x.d, nen, d_out);
+  Tmp out(sizeof(double));
+  if (out.err != cudaSuccess) return RGF_E_NOMEM;
+  sum_kernel<<<1, rgf::kThreads>>>((const double*)x.d, nen, (double*)out.p);
   double s = 0.0;
-  cudaError_t e = cudaMemcpy(&s, d_out, sizeof(double), cudaMemcpyDeviceToHost);
-  cudaFree(d_out);
+  const cudaError_t e = cudaMemcpy(&s, out.p, sizeof(double), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return RGF_E_CUDA;
   *current = s * dE * kE0 / kTpi / kHbar * kE0 * spindeg / (double)nk;
   return RGF_OK;
@@ -142,9 +169,10 @@ extern "C" int rgf_calc_block_current(rgf_ctx* ctx, const rgf_c16* H, const rgf_
   In h(H, sizeof(rgf_c16) * n2 * nx), g(G_lesser, sizeof(rgf_c16) * n2 * nx * nen), e(E, sizeof(double) * nen);
   if (h.err || g.err || e.err) return RGF_E_CUDA;
   const size_t nout = (size_t)nb * nb * nx * ns;
-  double* d_out = nullptr;
   const size_t jbytes = jdens ? sizeof(double) * nout * nen : 0;
-  if (cudaMalloc(&d_out, sizeof(double) * 2 * nout + jbytes) != cudaSuccess) return RGF_E_NOMEM;
+  Tmp out(sizeof(double) * 2 * nout + jbytes);
+  if (out.err != cudaSuccess) return RGF_E_NOMEM;
+  double* d_out = (double*)out.p;
   const double kTpiLocal = 6.28318530718;  // calc_block_current's own tpi (green_rgf.f90:4614)
   const double scale = (E[1] - E[0]) * kE0 / kTpiLocal / kHbar * kE0 * spindeg;
   const int thr = 256;
@@ -155,7 +183,6 @@ extern "C" int rgf_calc_block_current(rgf_ctx* ctx, const rgf_c16* H, const rgf_
   cudaError_t err = cudaMemcpy(tot_cur, d_out, sizeof(double) * nout, cudaMemcpyDeviceToHost);
   if (err == cudaSuccess && tot_ecur) err = cudaMemcpy(tot_ecur, d_out + nout, sizeof(double) * nout, cudaMemcpyDeviceToHost);
   if (err == cudaSuccess && jdens) err = cudaMemcpy(jdens, d_out + 2 * nout, jbytes, cudaMemcpyDeviceToHost);
-  cudaFree(d_out);
   return err == cudaSuccess ? RGF_OK : RGF_E_CUDA;
 }
 
@@ -167,13 +194,25 @@ extern "C" int rgf_calc_n_electron(rgf_ctx* ctx, const rgf_c16* G_lesser, const 
   const size_t gb = sizeof(rgf_c16) * (size_t)nm * nm * nx * nen * nk;
   In gl(G_lesser, gb), gg(G_greater, gb), e(E, sizeof(double) * nen), mg(midgap, sizeof(double) * nx);
   if (gl.err || gg.err || e.err || mg.err) return RGF_E_CUDA;
-  double* d_out = nullptr;
-  if (cudaMalloc(&d_out, 2 * sizeof(double) * nx) != cudaSuccess) return RGF_E_NOMEM;
-  n_electron_kernel<<<(unsigned)nx, rgf::kThreads>>>((const double2*)gl.d, (const double2*)gg.d, nen,
-                                                     (const double*)e.d, nm, nk, nx,
-                                                     (const double*)mg.d, d_out, d_out + nx);
+  // chunks per block: about four CTAs per SM over the whole grid
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t pairs = nen * nk;
+  int64_t nch = (4 * (int64_t)sms + nx - 1) / nx;
+  if (nch > pairs) nch = pairs;
+  if (nch > 65535) nch = 65535;
+  const int64_t per = (pairs + nch - 1) / nch;
+  nch = (pairs + per - 1) / per;
+  Tmp part(sizeof(double2) * nx * nch), out(2 * sizeof(double) * nx);
+  if (part.err != cudaSuccess || out.err != cudaSuccess) return RGF_E_NOMEM;
+  n_electron_partial_kernel<<<dim3((unsigned)nx, (unsigned)nch), rgf::kThreads>>>(
+      (const double2*)gl.d, (const double2*)gg.d, nen, (const double*)e.d, nm, nk, nx, per,
+      (const double*)mg.d, (double2*)part.p);
+  double* d_out = (double*)out.p;
+  n_electron_combine_kernel<<<(unsigned)((nx + 127) / 128), 128>>>((const double2*)part.p, nch, nx,
+                                                                   (const double*)e.d, nk, d_out, d_out + nx);
   cudaError_t err = cudaMemcpy(nelec, d_out, sizeof(double) * nx, cudaMemcpyDeviceToHost);
   if (err == cudaSuccess) err = cudaMemcpy(pelec, d_out + nx, sizeof(double) * nx, cudaMemcpyDeviceToHost);
-  cudaFree(d_out);
   return err == cudaSuccess ? RGF_OK : RGF_E_CUDA;
 }

@@ -39,18 +39,54 @@ bool is_dev(const void* p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+// Device view of a host or device input array.  Copies and temporaries are
+// stream-ordered on the legacy default stream (where the sums run, after the
+// caller's work there), so a call neither synchronises the device for an
+// allocation nor returns memory to the driver.
 struct DevIn {
   const void* d = nullptr;
   void* own = nullptr;
   cudaError_t err = cudaSuccess;
   DevIn(const void* p, size_t bytes) {
     if (is_dev(p)) { d = p; return; }
-    err = cudaMalloc(&own, bytes);
-    if (err == cudaSuccess) err = cudaMemcpy(own, p, bytes, cudaMemcpyHostToDevice);
+    err = cudaMallocAsync(&own, bytes, 0);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(own, p, bytes, cudaMemcpyHostToDevice, 0);
     d = own;
   }
-  ~DevIn() { if (own) cudaFree(own); }
+  ~DevIn() { if (own) cudaFreeAsync(own, 0); }
 };
+
+struct DevTmp {
+  void* p = nullptr;
+  cudaError_t err;
+  explicit DevTmp(size_t bytes) { err = cudaMallocAsync(&p, bytes, 0); }
+  ~DevTmp() { if (p) cudaFreeAsync(p, 0); }
+};
+
+// Sum, in index order e = 0 .. count-1, of the values at(e), by one warp:
+// the lanes load 32 consecutive terms at a time (the next 32 in flight while
+// these are added) and every lane adds them in order, so the result is the
+// sequential loop's, bit for bit.
+__device__ __forceinline__ double add_lane(double acc, double v, int l) {
+  return acc + __shfl_sync(0xffffffffu, v, l);
+}
+__device__ __forceinline__ double2 add_lane(double2 acc, double2 v, int l) {
+  return make_double2(acc.x + __shfl_sync(0xffffffffu, v.x, l), acc.y + __shfl_sync(0xffffffffu, v.y, l));
+}
+template <class T, class At>
+__device__ __forceinline__ T warp_ordered_sum(int64_t count, At at) {
+  const int lane = threadIdx.x & 31;
+  T acc{};
+  T nxt{};
+  if (lane < count) nxt = at(lane);
+  for (int64_t base = 0; base < count; base += 32) {
+    const T cur = nxt;
+    if (base + 32 + lane < count) nxt = at(base + 32 + lane);
+    const int n = (count - base) < 32 ? (int)(count - base) : 32;
+    for (int l = 0; l < n; l++) acc = add_lane(acc, cur, l);
+  }
+  return acc;
+}
 
 // out[k + NS*(j + length*ie)] = sum_ik sum_ib G(ib+k*NB, ib+k*NB, j, ie, ik); one thread each
 __global__ void diag_trace_kernel(const double2* G, int64_t NB, int64_t NS, int64_t length, int64_t nen,
@@ -74,69 +110,97 @@ __global__ void diag_trace_kernel(const double2* G, int64_t NB, int64_t NS, int6
 // (write_current_summed_over_k, :4757-4763).  cur(NB, NB, length, nen, nk).
 __global__ void cur_sum_kernel(const double* cur, int64_t NB, int64_t length, int64_t nen, int64_t nk,
                                int mode, double* out) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;   // one warp per output
   if (t >= length * nen) return;
   const int64_t j = t % length, ie = t / length;
   auto at = [&](int64_t ib, int64_t jb, int64_t ik) {
     return cur[ib + NB * (jb + NB * (j + length * (ie + nen * ik)))];
   };
-  double acc = 0.0;
-  if (mode == 2) {
-    for (int64_t ib = 0; ib < NB; ib++)
-      for (int64_t jb = 0; jb < NB; jb++)
-        for (int64_t ik = 0; ik < nk; ik++) acc += at(ib, jb, ik);
-  } else {
-    for (int64_t ik = 0; ik < nk; ik++)
-      for (int64_t ib = 0; ib < NB; ib++)
-        for (int64_t jb = 0; jb < NB; jb++) acc += at(ib, jb, ik);
+  double acc;
+  if (mode == 2) {   // ib, jb, ik (ik fastest)
+    acc = warp_ordered_sum<double>(NB * NB * nk, [&](int64_t e) {
+      return at(e / (NB * nk), (e / nk) % NB, e % nk);
+    });
+  } else {           // ik, ib, jb (jb fastest)
+    acc = warp_ordered_sum<double>(NB * NB * nk, [&](int64_t e) {
+      return at((e / NB) % NB, e % NB, e / (NB * NB));
+    });
   }
-  out[t] = acc;
+  if ((threadIdx.x & 31) == 0) out[t] = acc;
 }
 
 // DOS of write_dos_summed_over_k (:4832-4840): one running sum per energy
-// over j, k, ik, ib in that order
+// over j, k, ik, ib in that order (ib fastest); one warp per energy
 __global__ void dos_kernel(const double2* G, int64_t NB, int64_t NS, int64_t length, int64_t nen, int64_t nk,
                            double2* out) {
-  const int64_t ie = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t ie = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (ie >= nen) return;
   const int64_t nm = NB * NS;
-  double2 acc = rgf::czero();
-  for (int64_t j = 0; j < length; j++)
-    for (int64_t k = 0; k < NS; k++)
-      for (int64_t ik = 0; ik < nk; ik++)
-        for (int64_t ib = 0; ib < NB; ib++) {
-          const int64_t d = ib + k * NB;
-          acc = rgf::cadd(acc, G[d + nm * (d + nm * (j + length * (ie + nen * ik)))]);
-        }
-  out[ie] = acc;
+  const double2 acc = warp_ordered_sum<double2>(length * NS * nk * NB, [&](int64_t e) {
+    const int64_t ib = e % NB, r = e / NB;
+    const int64_t ik = r % nk, r2 = r / nk;
+    const int64_t k = r2 % NS, j = r2 / NS;
+    const int64_t d = ib + k * NB;
+    return G[d + nm * (d + nm * (j + length * (ie + nen * ik)))];
+  });
+  if ((threadIdx.x & 31) == 0) out[ie] = acc;
 }
 
-// Fortran Ew.d (see the header comment)
-std::string fortran_E(double v, int w, int d) {
-  char buf[64];
-  std::string body;
+// Fortran Ew.d (see the header comment), written as exactly w characters
+// into out
+void fortran_E_to(char* out, double v, int w, int d) {
+  char body[64];
+  int n = 0;
   if (std::isnan(v) || std::isinf(v)) {
-    body = std::isnan(v) ? "NaN" : (v < 0 ? "-Infinity" : "Infinity");
+    const char* t = std::isnan(v) ? "NaN" : (v < 0 ? "-Infinity" : "Infinity");
+    n = (int)std::strlen(t);
+    std::memcpy(body, t, n);
   } else {
+    char buf[64];
     std::snprintf(buf, sizeof(buf), "%.*e", d - 1, std::fabs(v));  // d significant digits
     const char* e = std::strchr(buf, 'e');
-    std::string digits;
-    for (const char* c = buf; c < e; c++)
-      if (*c != '.') digits += *c;
     int ex = std::atoi(e + 1) + 1;
     if (std::fabs(v) == 0.0) ex = 0;
-    std::string exps;
-    char eb[16];
-    if (std::abs(ex) <= 99) {
-      std::snprintf(eb, sizeof(eb), "E%c%02d", ex < 0 ? '-' : '+', std::abs(ex));
+    if (std::signbit(v)) body[n++] = '-';
+    body[n++] = '0';
+    body[n++] = '.';
+    for (const char* c = buf; c < e; c++)
+      if (*c != '.') body[n++] = *c;
+    const int ax = ex < 0 ? -ex : ex;
+    if (ax <= 99) {
+      body[n++] = 'E';
+      body[n++] = ex < 0 ? '-' : '+';
     } else {
-      std::snprintf(eb, sizeof(eb), "%c%03d", ex < 0 ? '-' : '+', std::abs(ex));
+      body[n++] = ex < 0 ? '-' : '+';
+      body[n++] = (char)('0' + ax / 100);
     }
-    exps = eb;
-    body = std::string(std::signbit(v) ? "-" : "") + "0." + digits + exps;
+    body[n++] = (char)('0' + (ax / 10) % 10);
+    body[n++] = (char)('0' + ax % 10);
   }
-  if ((int)body.size() > w) return std::string(w, '*');
-  return std::string(w - body.size(), ' ') + body;
+  if (n > w) {
+    std::memset(out, '*', w);
+    return;
+  }
+  std::memset(out, ' ', w - n);
+  std::memcpy(out + (w - n), body, n);
+}
+
+std::string fortran_E(double v, int w, int d) {
+  std::string s(w, ' ');
+  fortran_E_to(&s[0], v, w, d);
+  return s;
+}
+
+// append Ew.d to a text buffer
+void put_E(std::string& s, double v, int w, int d) {
+  const size_t o = s.size();
+  s.resize(o + w);
+  fortran_E_to(&s[o], v, w, d);
+}
+
+bool write_all(FILE* f, const std::string& text) {
+  const bool ok = std::fwrite(text.data(), 1, text.size(), f) == text.size();
+  return std::fclose(f) == 0 && ok;
 }
 
 std::string fortran_I(long long v, int w) {
@@ -169,27 +233,32 @@ extern "C" int rgf_write_spectrum(rgf_ctx* ctx, const char* dataset, int32_t ite
   const int64_t nm = NB * NS, n = NS * length * nen;
   DevIn g(G, sizeof(rgf_c16) * (size_t)nm * nm * length * nen * nk);
   if (g.err) return io_fail(RGF_E_CUDA, cudaGetErrorString(g.err));
-  double2* d_out = nullptr;
-  if (cudaMalloc(&d_out, sizeof(double2) * n) != cudaSuccess) return io_fail(RGF_E_NOMEM, "cudaMalloc");
+  DevTmp out(sizeof(double2) * n);
+  if (out.err != cudaSuccess) return io_fail(RGF_E_NOMEM, "device scratch");
+  double2* d_out = (double2*)out.p;
   diag_trace_kernel<<<(unsigned)((n + 255) / 256), 256>>>((const double2*)g.d, NB, NS, length, nen, nk, d_out);
   std::vector<double2> tr(n);
   cudaError_t e = cudaMemcpy(tr.data(), d_out, sizeof(double2) * n, cudaMemcpyDeviceToHost);
-  cudaFree(d_out);
   if (e != cudaSuccess) return io_fail(RGF_E_CUDA, cudaGetErrorString(e));
   FILE* f = open_out(std::string(dataset) + fstring(iter) + ".dat", append);
   if (!f) return io_fail(RGF_E_ARG, "cannot open the output file");
+  std::string text;
+  text.reserve((size_t)nen * (length * NS * 73 + 1));
   for (int64_t ie = 0; ie < nen; ie++) {
     for (int64_t j = 0; j < length; j++)
       for (int64_t k = 0; k < NS; k++) {
         double2 t = tr[k + NS * (j + length * ie)];
         if (summed_over_k) t = make_double2(t.x / (double)nk, t.y / (double)nk);
         const double x = (double)j * Lx * (double)NS + (double)k * Lx;
-        std::fprintf(f, "%s%s%s%s\n", fortran_E(x, 18, 4).c_str(), fortran_E(en[ie], 18, 4).c_str(),
-                     fortran_E(t.x * coeff[0], 18, 4).c_str(), fortran_E(t.y * coeff[1], 18, 4).c_str());
+        put_E(text, x, 18, 4);
+        put_E(text, en[ie], 18, 4);
+        put_E(text, t.x * coeff[0], 18, 4);
+        put_E(text, t.y * coeff[1], 18, 4);
+        text += '\n';
       }
-    std::fprintf(f, "\n");
+    text += '\n';
   }
-  std::fclose(f);
+  if (!write_all(f, text)) return io_fail(RGF_E_ARG, "cannot write the output file");
   return RGF_OK;
 }
 
@@ -202,20 +271,23 @@ extern "C" int rgf_write_dos(rgf_ctx* ctx, const char* dataset, int32_t iter, co
   const int64_t nm = NB * NS;
   DevIn g(G, sizeof(rgf_c16) * (size_t)nm * nm * length * nen * nk);
   if (g.err) return io_fail(RGF_E_CUDA, cudaGetErrorString(g.err));
-  double2* d_out = nullptr;
-  if (cudaMalloc(&d_out, sizeof(double2) * nen) != cudaSuccess) return io_fail(RGF_E_NOMEM, "cudaMalloc");
-  dos_kernel<<<(unsigned)((nen + 127) / 128), 128>>>((const double2*)g.d, NB, NS, length, nen, nk, d_out);
+  DevTmp out(sizeof(double2) * nen);
+  if (out.err != cudaSuccess) return io_fail(RGF_E_NOMEM, "device scratch");
+  double2* d_out = (double2*)out.p;
+  dos_kernel<<<(unsigned)((32 * nen + 127) / 128), 128>>>((const double2*)g.d, NB, NS, length, nen, nk, d_out);
   std::vector<double2> tr(nen);
   cudaError_t e = cudaMemcpy(tr.data(), d_out, sizeof(double2) * nen, cudaMemcpyDeviceToHost);
-  cudaFree(d_out);
   if (e != cudaSuccess) return io_fail(RGF_E_CUDA, cudaGetErrorString(e));
   FILE* f = open_out(std::string(dataset) + fstring(iter) + ".dat", append);
   if (!f) return io_fail(RGF_E_ARG, "cannot open the output file");
+  std::string text;
   for (int64_t ie = 0; ie < nen; ie++) {
     const double im = tr[ie].y / (double)nk / (double)length / (double)NS / Lx;
-    std::fprintf(f, "%s%s\n", fortran_E(en[ie], 18, 4).c_str(), fortran_E(im * (-2.0), 18, 4).c_str());
+    put_E(text, en[ie], 18, 4);
+    put_E(text, im * (-2.0), 18, 4);
+    text += '\n';
   }
-  std::fclose(f);
+  if (!write_all(f, text)) return io_fail(RGF_E_ARG, "cannot write the output file");
   return RGF_OK;
 }
 
@@ -231,29 +303,32 @@ extern "C" int rgf_write_current_spectrum(rgf_ctx* ctx, const char* dataset, int
   const int64_t n = length * nen, nkk = kz_summed ? nk : 1;
   DevIn c(cur, sizeof(double) * (size_t)NB * NB * length * nen * nkk);
   if (c.err) return io_fail(RGF_E_CUDA, cudaGetErrorString(c.err));
-  double* d_out = nullptr;
-  if (cudaMalloc(&d_out, sizeof(double) * n) != cudaSuccess) return io_fail(RGF_E_NOMEM, "cudaMalloc");
-  cur_sum_kernel<<<(unsigned)((n + 255) / 256), 256>>>((const double*)c.d, NB, length, nen, nkk,
-                                                       kz_summed ? 1 : 0, d_out);
+  DevTmp out(sizeof(double) * n);
+  if (out.err != cudaSuccess) return io_fail(RGF_E_NOMEM, "device scratch");
+  double* d_out = (double*)out.p;
+  cur_sum_kernel<<<(unsigned)((32 * n + 255) / 256), 256>>>((const double*)c.d, NB, length, nen, nkk,
+                                                            kz_summed ? 1 : 0, d_out);
   std::vector<double> tr(n);
   cudaError_t e = cudaMemcpy(tr.data(), d_out, sizeof(double) * n, cudaMemcpyDeviceToHost);
-  cudaFree(d_out);
   if (e != cudaSuccess) return io_fail(RGF_E_CUDA, cudaGetErrorString(e));
   const std::string name = kz_summed ? std::string(dataset) + fstring(iter) + ".dat"
                                      : std::string(dataset) + "_" + fstring(iter) + ".dat";
   FILE* f = open_out(name, kz_summed ? append : 0);
   if (!f) return io_fail(RGF_E_ARG, "cannot open the output file");
   const int64_t jmax = kz_summed ? length - 1 : length;
+  std::string text;
   for (int64_t ie = 0; ie < nen; ie++) {
     for (int64_t j = 0; j < jmax; j++) {
       double t = tr[j + length * ie];
       if (kz_summed) t = t / (double)nk;
-      std::fprintf(f, "%s%s%s\n", fortran_E((double)j * Lx, 18, 4).c_str(), fortran_E(en[ie], 18, 4).c_str(),
-                   fortran_E(t, 18, 4).c_str());
+      put_E(text, (double)j * Lx, 18, 4);
+      put_E(text, en[ie], 18, 4);
+      put_E(text, t, 18, 4);
+      text += '\n';
     }
-    std::fprintf(f, "\n");
+    text += '\n';
   }
-  std::fclose(f);
+  if (!write_all(f, text)) return io_fail(RGF_E_ARG, "cannot write the output file");
   return RGF_OK;
 }
 
@@ -263,13 +338,13 @@ extern "C" int rgf_write_current_summed_over_k(rgf_ctx* ctx, const char* dataset
   if (!ctx || !dataset || !cur || nx < 1 || NB < 1 || nk < 1) return io_fail(RGF_E_ARG, "invalid argument");
   DevIn c(cur, sizeof(double) * (size_t)NB * NB * nx * nk);
   if (c.err) return io_fail(RGF_E_CUDA, cudaGetErrorString(c.err));
-  double* d_out = nullptr;
-  if (cudaMalloc(&d_out, sizeof(double) * nx) != cudaSuccess) return io_fail(RGF_E_NOMEM, "cudaMalloc");
+  DevTmp out(sizeof(double) * nx);
+  if (out.err != cudaSuccess) return io_fail(RGF_E_NOMEM, "device scratch");
+  double* d_out = (double*)out.p;
   // (nb, nb, nx, nk) is the (nb, nb, length = nx, nen = 1, nk) layout
-  cur_sum_kernel<<<(unsigned)((nx + 255) / 256), 256>>>((const double*)c.d, NB, nx, 1, nk, 2, d_out);
+  cur_sum_kernel<<<(unsigned)((32 * nx + 255) / 256), 256>>>((const double*)c.d, NB, nx, 1, nk, 2, d_out);
   std::vector<double> tr(nx);
   cudaError_t e = cudaMemcpy(tr.data(), d_out, sizeof(double) * nx, cudaMemcpyDeviceToHost);
-  cudaFree(d_out);
   if (e != cudaSuccess) return io_fail(RGF_E_CUDA, cudaGetErrorString(e));
   FILE* f = open_out(std::string(dataset) + "_" + fstring(iter) + ".dat", 0);
   if (!f) return io_fail(RGF_E_ARG, "cannot open the output file");

@@ -52,7 +52,8 @@ EXPORTS = (
     "rgf_gw_polarization", "rgf_gw_self_energy", "rgf_gw_last_error", "rgf_permute_c16",
     "rgf_permute_last_error", "rgf_write_spectrum", "rgf_write_dos", "rgf_write_current_spectrum",
     "rgf_write_current_summed_over_k", "rgf_write_transmission_spectrum", "rgf_write_id_iteration",
-    "rgf_io_last_error", "rgf_read_ham_dat",
+    "rgf_io_last_error", "rgf_read_ham_dat", "rgf_gw_polarization_fft", "rgf_gw_self_energy_fft",
+    "rgf_gw_fft_last_error",
 )
 
 # kernel variant ids (rgf_variant_name)
@@ -168,6 +169,11 @@ def load(path: str = LIB_PATH):
     L.rgf_gw_polarization.restype = ctypes.c_int
     L.rgf_gw_self_energy.restype = ctypes.c_int
     L.rgf_gw_last_error.restype = ctypes.c_char_p
+    L.rgf_gw_polarization_fft.argtypes = [P] + [I64] * 8 + [D, D] + [P] * 9
+    L.rgf_gw_self_energy_fft.argtypes = [P] + [I64] * 8 + [D] + [P] * 10
+    L.rgf_gw_polarization_fft.restype = ctypes.c_int
+    L.rgf_gw_self_energy_fft.restype = ctypes.c_int
+    L.rgf_gw_fft_last_error.restype = ctypes.c_char_p
     L.rgf_permute_c16.argtypes = [P, P, P, ctypes.c_int32, P, P, P]
     L.rgf_permute_c16.restype = ctypes.c_int
     L.rgf_permute_last_error.restype = ctypes.c_char_p
@@ -457,6 +463,27 @@ class Context:
                                        _ptr(WL), _ptr(WG), _ptr(WR), _ptr(SL), _ptr(SG), _ptr(SR), stream)
         if rc != RGF_OK:
             raise RgfError(rc, load().rgf_gw_last_error().decode())
+
+    def gw_polarization_fft(self, GL, GG, GR, GLt, GGt, *, PL, PG, PR, nky, nkz, nm, ndiag, first_ij, dEn,
+                            spindeg, stream=None):
+        """rgf_gw_polarization_fft on device arrays in the *_by_blocks layout,
+        NumPy view (nij, nx, nk, nen) of the Fortran (nen, nk, nx, nij)."""
+        nij, nx, nk, nen = (int(v) for v in GL.shape)
+        rc = load().rgf_gw_polarization_fft(self.h, int(nm), nx, nen, int(nky), int(nkz), int(ndiag), nij,
+                                            int(first_ij), float(dEn), float(spindeg), _ptr(GL), _ptr(GG),
+                                            _ptr(GR), _ptr(GLt), _ptr(GGt), _ptr(PL), _ptr(PG), _ptr(PR), stream)
+        if rc != RGF_OK:
+            raise RgfError(rc, load().rgf_gw_fft_last_error().decode())
+
+    def gw_self_energy_fft(self, GL, GG, GR, WL, WG, WR, *, SL, SG, SR, nky, nkz, nm, ndiag, first_ij, dEn,
+                           stream=None):
+        """rgf_gw_self_energy_fft (same layout as gw_polarization_fft)."""
+        nij, nx, nk, nen = (int(v) for v in GL.shape)
+        rc = load().rgf_gw_self_energy_fft(self.h, int(nm), nx, nen, int(nky), int(nkz), int(ndiag), nij,
+                                           int(first_ij), float(dEn), _ptr(GL), _ptr(GG), _ptr(GR), _ptr(WL),
+                                           _ptr(WG), _ptr(WR), _ptr(SL), _ptr(SG), _ptr(SR), stream)
+        if rc != RGF_OK:
+            raise RgfError(rc, load().rgf_gw_fft_last_error().decode())
 
     def permute(self, src, dst, src_shape, order, stream=None):
         """rgf_permute_c16: dst = RESHAPE(src, ORDER=order) (Fortran meaning,

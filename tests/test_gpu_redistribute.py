@@ -22,7 +22,8 @@ def rgf():
 
 @pytest.mark.parametrize("shape,order", [((64, 4, 10, 8, 4), (1, 5, 2, 3, 4)), ((64, 10, 8, 4, 4), (5, 4, 1, 3, 2)),
                                          ((8, 4, 4, 10, 64), (3, 5, 4, 2, 1)), ((64, 10, 8, 4, 4), (1, 3, 4, 5, 2)),
-                                         ((3, 5, 7), (2, 3, 1))])
+                                         ((3, 5, 7), (2, 3, 1)), ((37, 5, 70), (3, 1, 2)), ((300, 3), (1, 2)),
+                                         ((33, 65, 2), (2, 1, 3)), ((7,), (1,))])
 def test_permute_matches_oracle(rgf, shape, order):
     import torch
     rng = np.random.default_rng(1)

@@ -26,10 +26,13 @@ def _read(path):
         return f.read()
 
 
-def test_writers_match_oracle_text(rgf, tmp_path):
+@pytest.mark.parametrize("NB,NS,length,nen,nk", [(3, 2, 4, 5, 2), (5, 3, 7, 9, 3)])
+def test_writers_match_oracle_text(rgf, tmp_path, NB, NS, length, nen, nk):
+    """Small sizes, and sizes whose ordered sums span several 32-term warp
+    chunks with a ragged last one (DOS: 315 terms, current: 75)."""
     from liteqt_b200 import writers as W
     rng = np.random.default_rng(0)
-    NB, NS, length, nen, nk, Lx = 3, 2, 4, 5, 2, 0.5
+    Lx = 0.5
     nm = NB * NS
     en = np.linspace(-1.0, 1.0, nen)
     G = rng.normal(size=(nk, nen, length, nm, nm)) + 1j * rng.normal(size=(nk, nen, length, nm, nm))
