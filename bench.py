@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--full-outputs", action="store_true",
                    help="request the reference's full output set per energy (G^R_ll, G^<_ll, G^>_ll, the bond "
                         "current cur, G^R_{l,l+1}, tr, tre, T) instead of G^R_ll, G^<_ll, T, tr, tre")
+    p.add_argument("--consistent", action="store_true",
+                   help="the consistent backward coupling H1i(:,:,l+1) instead of the reference's H1i(:,:,l)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-threads", type=int, default=0)
@@ -71,6 +73,9 @@ def parse():
     p.add_argument("--gw", action="store_true",
                    help="time the GW-loop convolutions (polarization, self-energy) on a 2x2 k-grid, "
                         "nen=512, nx=10, nm=16, ndiag=3")
+    p.add_argument("--blocks", action="store_true",
+                   help="time the building blocks alone (FP64 and split-integer products, FP64 and refined FP32 "
+                        "inverses) on 1480 blocks of 128 x 128, one CTA per SM")
     p.add_argument("--gw-fft", action="store_true",
                    help="time the FFT form of the GW convolutions (rgf_gw_polarization_fft / "
                         "rgf_gw_self_energy_fft) at nk=16, nen=4096, nx=40, nm=64 on one rank's (i,j) slice")
@@ -107,6 +112,7 @@ def config(args, world):
             "outputs": (["G^R_ll", "G^<_ll", "G^>_ll", "cur", "G^R_l,l+1", "T", "tr", "tre"]
                         if args.full_outputs else ["G^R_ll", "G^<_ll", "T", "tr", "tre"]),
             "precision": args.precision, "parallelism": f"energy-sharded x{world}",
+            "backward_coupling": "H1i(l+1) (consistent)" if args.consistent else "H1i(l) (the reference's)",
             "l2": "flushed between timed steps (256 MiB write)", "seed": 1}
 
 
@@ -293,7 +299,7 @@ def run_ours(args):
     E = np.ascontiguousarray(E_all[rank * args.nen:(rank + 1) * args.nen])
     nen, nx, nb = args.nen, args.nx, args.nb
     mixed = args.precision == "mixed"
-    opts = rgf.Options(device=local, eta_dev=ETA, eta_lead=ETA,
+    opts = rgf.Options(device=local, eta_dev=ETA, eta_lead=ETA, consistent=args.consistent,
                        precision=rgf.RGF_PREC_MIXED if mixed else rgf.RGF_PREC_FP64)
     ctx = rgf.Context(opts)
     stream = torch.cuda.Stream(device=dev)
@@ -448,7 +454,8 @@ def run_ours(args):
     other = None
     if not args.no_other and nb == 128 and not args.full_outputs:
         oprec = rgf.RGF_PREC_FP64 if mixed else rgf.RGF_PREC_MIXED
-        ctx2 = rgf.Context(rgf.Options(device=local, eta_dev=ETA, eta_lead=ETA, precision=oprec))
+        ctx2 = rgf.Context(rgf.Options(device=local, eta_dev=ETA, eta_lead=ETA, precision=oprec,
+                                       consistent=args.consistent))
         with torch.cuda.stream(stream):
             for _ in range(max(1, args.warmup)):
                 ctx2.solve_energies(Hii, H1i, E, MU, temp, ldos=ldos, ndens=ndens, tr=tr, tre=tre, T=T,
@@ -732,6 +739,70 @@ def run_gw(args):
                          "traffic": None,
                          "peak_source": "cuBLAS ZGEMM 4096^3 measured live (DMMA and DFMA peaks are "
                                         "equal on B200: 37.1 vs 36.5 TFLOP/s in a probe)"}}
+    print(json.dumps(line), flush=True)
+
+
+def run_blocks(args):
+    """The solver's building blocks alone, one CTA per SM, 10 blocks per SM
+    (1480 seeded 128 x 128 complex blocks): the FP64 DMMA product, the
+    split-integer int8 product, the FP64 blocked Gauss-Jordan inverse and the
+    refined FP32 inverse, through rgf_block_product / rgf_block_inverse.
+    Reported per operation: device time per block per SM in SM cycles (at
+    the sampled clock) and the rate in complex-GEMM-equivalent TFLOP/s
+    (8 nb^3 per block)."""
+    import torch
+    from liteqt_b200 import rgf
+    nb, count = 128, 1480
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    g = torch.Generator(device=dev).manual_seed(13)
+
+    def rnd():
+        return torch.complex(torch.randn((count, nb, nb), generator=g, device=dev, dtype=torch.float64),
+                             torch.randn((count, nb, nb), generator=g, device=dev, dtype=torch.float64))
+    A, B = rnd(), rnd()
+    C = torch.empty_like(A)
+    ctx = rgf.Context(rgf.Options())
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    ops = {
+        "product_fp64": lambda: ctx.block_product(A, B, C, precision=rgf.RGF_PREC_FP64),
+        "product_int8_split": lambda: ctx.block_product(A, B, C, precision=rgf.RGF_PREC_MIXED),
+        "inverse_fp64": lambda: ctx.block_inverse(A, C, precision=rgf.RGF_PREC_FP64),
+        "inverse_fp32_refined": lambda: ctx.block_inverse(A, C, precision=rgf.RGF_PREC_MIXED),
+    }
+    clocks = ClockSampler(0)
+    clocks.start()
+    out = {}
+    for name, fn in ops.items():
+        ms = []
+        for it in range(args.warmup + args.steps):
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record()
+            fn()
+            e.record()
+            e.synchronize()
+            if it >= args.warmup:
+                ms.append(s.elapsed_time(e))
+        out[name] = float(np.mean(ms))
+    clk = clocks.stop()
+    ctx.close()
+    mhz = clk.get("sm_mhz") or 1965.0
+    per_sm = count / sms
+    res = {k: {"ms": v, "kcycles_per_block_per_sm": v * 1e-3 * mhz * 1e6 / per_sm / 1e3,
+               "tflops_equiv": 8.0 * nb ** 3 * count / (v * 1e-3) / 1e12} for k, v in out.items()}
+    peak = zgemm_peak_tflops(torch, dev)
+    line = {"metric": "block operations per second (nb 128, one CTA per SM)",
+            "value": count / (out["product_fp64"] * 1e-3), "unit": "FP64 products/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": out["product_fp64"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 / int8", "data": "synthetic",
+            "config": {"workload": "block_ops_nb128_x1480", "nb": nb, "blocks": count, "blocks_per_sm": per_sm,
+                       "l2": "operands 3 x 388 MB, larger than L2"},
+            "ops": res,
+            "roofline": {"bound": "tensor", "achieved": res["product_fp64"]["tflops_equiv"], "peak": peak,
+                         "unit": "TFLOP/s", "frac": res["product_fp64"]["tflops_equiv"] / peak, "traffic": None,
+                         "peak_source": "cuBLAS ZGEMM 4096^3 measured live"},
+            "clocks": clk}
     print(json.dumps(line), flush=True)
 
 
@@ -1140,6 +1211,8 @@ def main():
         run_band_edge(args)
     elif args.gw_fft:
         run_gw_fft(args)
+    elif args.blocks:
+        run_blocks(args)
     elif args.dropin:
         run_dropin(args)
     elif args.gw:

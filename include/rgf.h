@@ -368,8 +368,10 @@ RGF_API const char* rgf_gw_last_error(void);
  *   rgf_gw_self_energy_fft: Sigma^< = sum_q conv(G^<_kd, W^<_q), Sigma^>
  *     likewise, Sigma^R = conv(G^<, W^R) + conv(G^R, W^<) + conv(G^R, W^R),
  *     times i dEn/(2 pi)/nk, then Sigma^R = Re + i Im(Sigma^> - Sigma^<)/2.
- * The transforms are cuFFT's, in chunks of (i,j, ix) lines within a few GB of
- * stream-ordered scratch (RGF_GW_FFT_CHUNK sets the lines per chunk).
+ * The transforms are cuFFT's, in chunks of (i,j, ix) lines within at most
+ * 4 GB of device scratch (RGF_GW_FFT_CHUNK sets the lines per chunk); the
+ * context keeps the scratch and the cuFFT plans of the last shape between
+ * calls and frees them in rgf_ctx_destroy.
  * Stream-ordered on `stream`; returns when the results are written.  Error
  * text: rgf_gw_fft_last_error(). */
 RGF_API int rgf_gw_polarization_fft(rgf_ctx* ctx, int64_t nm, int64_t nx, int64_t nen, int64_t nky,

@@ -90,7 +90,15 @@ struct rgf_ctx {
   rgf_stats stats;
   int8_t variant[kVariantSlots];  // kernel variant per block size (defaults; rgf_autotune may override)
   int8_t ctas[kVariantSlots];     // resident CTAs per SM per block size, 0 = as many as fit
+  void* ext_cache = nullptr;      // per-context state of other modules (the FFT form's plans)
+  void (*ext_cache_free)(void*) = nullptr;
 };
+
+void* rgf::ctx_ext_cache(rgf_ctx* c) { return c->ext_cache; }
+void rgf::ctx_set_ext_cache(rgf_ctx* c, void* cache, void (*free_fn)(void*)) {
+  c->ext_cache = cache;
+  c->ext_cache_free = free_fn;
+}
 
 extern "C" void rgf_opts_default(rgf_opts* o) {
   std::memset(o, 0, sizeof(*o));
@@ -154,6 +162,7 @@ extern "C" int rgf_ctx_destroy(rgf_ctx* c) {
   if (!c) return RGF_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->ext_cache_free) c->ext_cache_free(c->ext_cache);
   c->work.release();
   c->tasks.release();
   c->devs.release();

@@ -168,13 +168,30 @@ struct Plan {
   }
 };
 
-struct Scratch {
-  void* p = nullptr;
-  cudaStream_t st;
-  cudaError_t err;
-  Scratch(size_t bytes, cudaStream_t s) : st(s) { err = cudaMallocAsync(&p, bytes, s); }
-  ~Scratch() { if (p) cudaFreeAsync(p, st); }
+// Kept in the context between calls (a GW loop calls these every
+// iteration): the cuFFT plans of the last shape and the device scratch, so a
+// call neither re-plans nor re-allocates.  Freed with the context.
+struct FftCache {
+  int dev = -1;
+  int64_t nky = 0, nkz = 0, N = 0, chunk = 0, tail = 0;
+  std::unique_ptr<struct Plan> full, part;
+  void* scratch = nullptr;
+  size_t bytes = 0;
+  ~FftCache();
+  static void destroy(void* p) { delete static_cast<FftCache*>(p); }
 };
+
+FftCache::~FftCache() {
+  full.reset();
+  part.reset();
+  if (scratch) {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(dev);
+    cudaFree(scratch);
+    cudaSetDevice(cur);
+  }
+}
 
 unsigned grid_for(int64_t total) {
   const int64_t g = (total + 255) / 256;
@@ -183,9 +200,9 @@ unsigned grid_for(int64_t total) {
 
 // mode 0: polarization (x: in[0..2], y: in[3..5]); mode 1: self-energy
 // (G: in[0..2], W: in[3..5]).
-int run_fft_form(int mode, int64_t nm, int64_t nx, int64_t nen, int64_t nky, int64_t nkz, int64_t ndiag,
-                 int64_t nij, int64_t first_ij, double dEn, double spindeg, const double2* const in[6],
-                 double2* const out[3], cudaStream_t st) {
+int run_fft_form(rgf_ctx* ctx, int mode, int64_t nm, int64_t nx, int64_t nen, int64_t nky, int64_t nkz,
+                 int64_t ndiag, int64_t nij, int64_t first_ij, double dEn, double spindeg,
+                 const double2* const in[6], double2* const out[3], cudaStream_t st) {
   g_fft_err[0] = 0;
   if (nm < 1 || nx < 1 || nen < 2 || (nen % 2) != 0 || nky < 1 || nkz < 1 || ndiag < 0 || nij < 0 ||
       first_ij < 1)
@@ -247,12 +264,51 @@ int run_fft_form(int mode, int64_t nm, int64_t nx, int64_t nen, int64_t nky, int
   const int64_t cap = (int64_t)(0x7fffffff / ((size_t)d.nk * d.N));
   if (chunk > cap) chunk = cap;
   if (chunk < 1) return fft_fail(RGF_E_UNSUPPORTED, "one line exceeds the transform size limit");
-  Scratch ws(per_line * chunk + sizeof(int64_t) * lines.size() + sizeof(double2) * d.nk, st);
-  if (ws.err != cudaSuccess) return fft_fail(RGF_E_NOMEM, "device scratch for the transforms");
+  const int64_t nl = (int64_t)lines.size();
+  int dev = 0;
+  cudaGetDevice(&dev);
+  FftCache* cache = static_cast<FftCache*>(rgf::ctx_ext_cache(ctx));
+  if (!cache) {
+    cache = new FftCache();
+    rgf::ctx_set_ext_cache(ctx, cache, &FftCache::destroy);
+  }
+  const size_t need = per_line * chunk + sizeof(int64_t) * lines.size() + sizeof(double2) * d.nk;
+  if (cache->dev != dev || cache->bytes < need) {
+    cudaError_t e = cudaStreamSynchronize(st);   // earlier calls may still use the old scratch
+    if (cache->scratch) cudaFree(cache->scratch);
+    cache->scratch = nullptr;
+    cache->bytes = 0;
+    if (e == cudaSuccess) e = cudaMalloc(&cache->scratch, need);
+    if (e != cudaSuccess) {
+      cache->scratch = nullptr;
+      return fft_fail(RGF_E_NOMEM, "device scratch for the transforms");
+    }
+    cache->bytes = need;
+  }
+  const int64_t tail = nl % chunk;
+  if (cache->dev != dev || cache->nky != nky || cache->nkz != nkz || cache->N != d.N || cache->chunk != chunk ||
+      cache->tail != tail || !cache->full) {
+    cache->full.reset(new Plan(d, chunk, st));
+    cache->part.reset(tail ? new Plan(d, tail, st) : nullptr);
+    if (!cache->full->ok || (tail && !cache->part->ok)) {
+      cache->full.reset();
+      cache->part.reset();
+      return fft_fail(RGF_E_CUDA, "cuFFT plan");
+    }
+    cache->dev = dev;
+    cache->nky = nky;
+    cache->nkz = nkz;
+    cache->N = d.N;
+    cache->chunk = chunk;
+    cache->tail = tail;
+  }
+  if (cufftSetStream(cache->full->h, st) != CUFFT_SUCCESS ||
+      (cache->part && cufftSetStream(cache->part->h, st) != CUFFT_SUCCESS))
+    return fft_fail(RGF_E_CUDA, "cuFFT stream");
   const size_t spec = (size_t)chunk * d.nk * d.N;
   double2* buf[6];
-  for (int a = 0; a < 6; a++) buf[a] = (double2*)ws.p + a * spec;
-  int64_t* d_lines = (int64_t*)((double2*)ws.p + 6 * spec);
+  for (int a = 0; a < 6; a++) buf[a] = (double2*)cache->scratch + a * spec;
+  int64_t* d_lines = (int64_t*)((double2*)cache->scratch + 6 * spec);
   double2* d_ph = (double2*)(d_lines + lines.size());
   cudaError_t ce = cudaMemcpyAsync(d_lines, lines.data(), sizeof(int64_t) * lines.size(), cudaMemcpyHostToDevice, st);
   if (ce == cudaSuccess) ce = cudaMemcpyAsync(d_ph, ph.data(), sizeof(double2) * d.nk, cudaMemcpyHostToDevice, st);
@@ -260,17 +316,9 @@ int run_fft_form(int mode, int64_t nm, int64_t nx, int64_t nen, int64_t nky, int
   // the host vectors must outlive the asynchronous copies from them
   ce = cudaStreamSynchronize(st);
   if (ce != cudaSuccess) return fft_fail(RGF_E_CUDA, cudaGetErrorString(ce));
-  const int64_t nl = (int64_t)lines.size();
-  Plan full(d, chunk, st);
-  if (!full.ok) return fft_fail(RGF_E_CUDA, "cuFFT plan");
-  std::unique_ptr<Plan> tail;
-  if (nl % chunk != 0) {
-    tail.reset(new Plan(d, nl % chunk, st));
-    if (!tail->ok) return fft_fail(RGF_E_CUDA, "cuFFT plan");
-  }
   for (int64_t c0 = 0; c0 < nl; c0 += chunk) {
     const int64_t nb = (nl - c0) < chunk ? (nl - c0) : chunk;
-    const Plan& plan = nb == chunk ? full : *tail;
+    const Plan& plan = nb == chunk ? *cache->full : *cache->part;
     const int64_t* L = d_lines + c0;
     const int64_t tot = nb * d.nk * d.N;
     for (int a = 0; a < 6; a++) {
@@ -309,7 +357,7 @@ extern "C" int rgf_gw_polarization_fft(rgf_ctx* ctx, int64_t nm, int64_t nx, int
   const double2* in[6] = {(const double2*)G_lesser, (const double2*)G_greater, (const double2*)G_r,
                           (const double2*)G_greater_t, (const double2*)G_lesser_t, (const double2*)G_r};
   double2* out[3] = {(double2*)P_lesser, (double2*)P_greater, (double2*)P_retarded};
-  return run_fft_form(0, nm, nx, nen, nky, nkz, ndiag, nij, first_ij, dEn, spindeg, in, out, (cudaStream_t)stream);
+  return run_fft_form(ctx, 0, nm, nx, nen, nky, nkz, ndiag, nij, first_ij, dEn, spindeg, in, out, (cudaStream_t)stream);
 }
 
 extern "C" int rgf_gw_self_energy_fft(rgf_ctx* ctx, int64_t nm, int64_t nx, int64_t nen, int64_t nky,
@@ -322,5 +370,5 @@ extern "C" int rgf_gw_self_energy_fft(rgf_ctx* ctx, int64_t nm, int64_t nx, int6
   const double2* in[6] = {(const double2*)G_lesser, (const double2*)G_greater, (const double2*)G_r,
                           (const double2*)W_lesser, (const double2*)W_greater, (const double2*)W_retarded};
   double2* out[3] = {(double2*)Sigma_lesser_new, (double2*)Sigma_greater_new, (double2*)Sigma_r_new};
-  return run_fft_form(1, nm, nx, nen, nky, nkz, ndiag, nij, first_ij, dEn, 1.0, in, out, (cudaStream_t)stream);
+  return run_fft_form(ctx, 1, nm, nx, nen, nky, nkz, ndiag, nij, first_ij, dEn, 1.0, in, out, (cudaStream_t)stream);
 }

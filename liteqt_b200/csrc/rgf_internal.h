@@ -151,4 +151,9 @@ cudaError_t launch_block_mixed(int mode, int ns, const double2* A, int cA, const
 cudaError_t launch_block_fp64_inv(int nb, const double2* X, double2* Xi, int64_t count, double2* ws, int grid,
                                   int32_t* status, cudaStream_t stream);
 
+// Per-context state owned by another module (one slot): a pointer and the
+// function that frees it when the context is destroyed.
+void* ctx_ext_cache(rgf_ctx* c);
+void ctx_set_ext_cache(rgf_ctx* c, void* cache, void (*free_fn)(void*));
+
 }  // namespace rgf

@@ -105,6 +105,25 @@ def test_benchmark_workload_nb128_nx100(rgf):
     _check_iters(g, r)
 
 
+@pytest.mark.parametrize("nm,nx", [(128, 100), (256, 24)])
+def test_consistent_coupling_at_size(rgf, nm, nx):
+    """The consistent backward coupling H1i(:,:,l+1) on the benchmark's
+    device (nb = 128, Nx = 100) and at nb = 256, eta = 1e-5: there the G^<
+    recursion is stable (|G^<| ~ 1 along the chain), unlike the reference's
+    coupling, whose recursion grows by ~1e110 over the 100 blocks."""
+    from oracle import oracle as O
+    d = S.make_device(nm, nx, seed=1)
+    E = np.array([-1.7635, 0.5676, 2.3716])
+    opts = rgf.Options(eta_dev=1e-5, eta_lead=1e-5, consistent=True)
+    oo = O.Opts(eta_dev=1e-5, eta_lead=1e-5, consistent=1)
+    g = _gpu(rgf, d, E, opts, ("ldos", "ndens"))
+    assert g["rc"] == 0 and np.all(g["info"]["status"] == 0)
+    r = _oracle(d.Hii, d.H1i, E, oo, outputs=("ldos", "ndens"))
+    floors = [_oracle(*perturbed_inputs(d.Hii, d.H1i, s), E, oo, outputs=("ldos", "ndens")) for s in range(2)]
+    compare_spread(g, r, floors, nm, d.H1i)
+    _check_iters(g, r)
+
+
 def test_band_edge_workload_nb256_nx64_plain(rgf):
     from oracle import oracle as O
     nm, nx = 256, 64
