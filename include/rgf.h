@@ -89,7 +89,17 @@ typedef struct rgf_opts {
                               writes (all but `cur`) are written by the kernels through their
                               device mapping, so the transfer overlaps the solve; 0: staged in
                               device memory and copied back after the launch */
-  int32_t reserved[6];
+  int32_t pipelined;       /* 1: rgf_solve_batch / rgf_solve_energies called with info = NULL
+                              return once the solve and the copies of its host outputs are
+                              queued: outputs are staged in one of two device buffers (taken in
+                              turn) and copied to the host by the copy engine on the context's
+                              copy stream, so one call's copy overlaps the next call's solve.
+                              Host outputs (and tr, tre, T) hold the results after
+                              rgf_ctx_synchronize(ctx), which also completes the statistics;
+                              until then the host arrays must not be read or reused.  Overlap
+                              needs pinned host outputs (pageable ones make the call wait for
+                              its copies).  A call with info != NULL runs as with 0. */
+  int32_t reserved[5];
 } rgf_opts;
 
 typedef struct rgf_ctx rgf_ctx;
@@ -166,6 +176,9 @@ RGF_API int rgf_ctx_create(const rgf_opts* opts, rgf_ctx** ctx);
 RGF_API int rgf_ctx_destroy(rgf_ctx* ctx);
 RGF_API int rgf_ctx_set_opts(rgf_ctx* ctx, const rgf_opts* opts);
 RGF_API int rgf_ctx_get_stats(const rgf_ctx* ctx, rgf_stats* stats);
+/* Waits until every solve and output copy the context has queued
+ * (rgf_opts.pipelined) is complete and fills the last call's statistics. */
+RGF_API int rgf_ctx_synchronize(rgf_ctx* ctx);
 
 /* Batched solve: replaces the whole `do ik / !$omp do ie / call green_RGF_RS`
  * loop.  All tasks run in one persistent launch that drains a work queue.

@@ -92,6 +92,17 @@ struct rgf_ctx {
   int8_t ctas[kVariantSlots];     // resident CTAs per SM per block size, 0 = as many as fit
   void* ext_cache = nullptr;      // per-context state of other modules (the FFT form's plans)
   void (*ext_cache_free)(void*) = nullptr;
+  // pipelined host outputs (rgf_opts.pipelined): two staging buffers used in
+  // turn, the copy stream that takes each call's outputs to the host, and per
+  // buffer the event after its copies and a pinned copy of the call's task info
+  DevBuf pipe_stage[2];
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t pipe_free[2] = {nullptr, nullptr};
+  cudaEvent_t pipe_solved = nullptr, pipe_info_done = nullptr;
+  DInfo* pipe_info[2] = {nullptr, nullptr};
+  int64_t pipe_info_cap[2] = {0, 0}, pipe_info_n[2] = {0, 0};
+  int pipe_sel = 0, pipe_last = -1;
+  std::vector<int64_t> pipe_nb[2];   // block size of each task of the call, for the stats
 };
 
 void* rgf::ctx_ext_cache(rgf_ctx* c) { return c->ext_cache; }
@@ -162,7 +173,16 @@ extern "C" int rgf_ctx_destroy(rgf_ctx* c) {
   if (!c) return RGF_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
   if (c->ext_cache_free) c->ext_cache_free(c->ext_cache);
+  for (int b = 0; b < 2; b++) {
+    c->pipe_stage[b].release();
+    if (c->pipe_free[b]) cudaEventDestroy(c->pipe_free[b]);
+    if (c->pipe_info[b]) cudaFreeHost(c->pipe_info[b]);
+  }
+  if (c->pipe_solved) cudaEventDestroy(c->pipe_solved);
+  if (c->pipe_info_done) cudaEventDestroy(c->pipe_info_done);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   c->work.release();
   c->tasks.release();
   c->devs.release();
@@ -179,6 +199,30 @@ extern "C" int rgf_ctx_destroy(rgf_ctx* c) {
 extern "C" int rgf_ctx_get_stats(const rgf_ctx* c, rgf_stats* s) {
   if (!c || !s) return fail(RGF_E_ARG, "NULL argument");
   *s = c->stats;
+  return RGF_OK;
+}
+
+// Waits for every queued solve and output copy of the context (pipelined
+// calls), then completes the statistics of the last call.
+extern "C" int rgf_ctx_synchronize(rgf_ctx* c) {
+  if (!c) return fail(RGF_E_ARG, "ctx is NULL");
+  RGF_CUDA(cudaSetDevice(c->device));
+  if (c->copy_stream) RGF_CUDA(cudaStreamSynchronize(c->copy_stream));
+  const int b = c->pipe_last;
+  if (b >= 0) {
+    double flops = 0.0, int8_ops = 0.0;
+    for (int64_t t = 0; t < c->pipe_info_n[b]; t++) {
+      const double nb = (double)c->pipe_nb[b][t];
+      flops += 8.0 * nb * nb * nb * (double)(c->pipe_info[b][t].n_gemm + c->pipe_info[b][t].n_inv);
+      int8_ops += 8.0 * nb * nb * nb * (double)c->pipe_info[b][t].pad;
+    }
+    float kms = 0.0f;
+    RGF_CUDA(cudaEventElapsedTime(&kms, c->ev0, c->ev1));
+    c->stats.last_kernel_ms = kms;
+    c->stats.last_flops = flops;
+    c->stats.last_int8_ops = int8_ops;
+    c->pipe_last = -1;
+  }
   return RGF_OK;
 }
 
@@ -379,9 +423,13 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
                     "only)", d);
     }
 
-  // ---- staging of host arrays
+  // ---- staging of host arrays.  Pipelined calls (no info requested)
+  // stage in one of two buffers, taken in turn, and leave before the
+  // outputs are on the host; the buffer waits for the copies of the call
+  // that used it last.
+  const bool pipe = c->opts.pipelined != 0 && info == nullptr;
   Stage sg;
-  sg.zero_copy = c->opts.zero_copy != 0;
+  sg.zero_copy = c->opts.zero_copy != 0 && !pipe;
   for (int32_t d = 0; d < n_devices; d++) {
     const size_t bytes = (size_t)devices[d].nm * devices[d].nm * devices[d].nx * sizeof(rgf_c16);
     sg.add(devices[d].Hii, bytes, true, false);
@@ -409,9 +457,42 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
     if (want_T) sg.add(k.T, sizeof(double), false, true, true);
   }
   sg.layout();
-  rc = c->stage.reserve(std::max<size_t>(sg.total, 256));
+  const int pb = c->pipe_sel;
+  if (pipe) {
+    if (!c->copy_stream) {
+      RGF_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+      RGF_CUDA(cudaEventCreateWithFlags(&c->pipe_solved, cudaEventDisableTiming));
+      RGF_CUDA(cudaEventCreateWithFlags(&c->pipe_info_done, cudaEventDisableTiming));
+      RGF_CUDA(cudaEventRecord(c->pipe_info_done, c->copy_stream));
+      for (int b = 0; b < 2; b++) {
+        RGF_CUDA(cudaEventCreateWithFlags(&c->pipe_free[b], cudaEventDisableTiming));
+        RGF_CUDA(cudaEventRecord(c->pipe_free[b], c->copy_stream));
+      }
+    }
+    // a buffer that must grow is freed only once its copies are done
+    if (c->pipe_stage[pb].bytes < sg.total) RGF_CUDA(cudaEventSynchronize(c->pipe_free[pb]));
+    if (c->pipe_info_cap[pb] < n_tasks) {
+      RGF_CUDA(cudaEventSynchronize(c->pipe_free[pb]));
+      if (c->pipe_info[pb]) cudaFreeHost(c->pipe_info[pb]);
+      c->pipe_info[pb] = nullptr;
+      c->pipe_info_cap[pb] = 0;
+      RGF_CUDA(cudaMallocHost((void**)&c->pipe_info[pb], sizeof(DInfo) * (size_t)n_tasks));
+      c->pipe_info_cap[pb] = n_tasks;
+    }
+    RGF_CUDA(cudaStreamWaitEvent(st, c->pipe_free[pb], 0));
+  }
+  if (c->copy_stream) {
+    // the task info of the previous pipelined call is copied out before this
+    // call resets it; a call that is not pipelined also waits for every
+    // pending copy (it may write the same host arrays)
+    RGF_CUDA(cudaStreamWaitEvent(st, c->pipe_info_done, 0));
+    if (!pipe)
+      for (int b = 0; b < 2; b++) RGF_CUDA(cudaStreamWaitEvent(st, c->pipe_free[b], 0));
+  }
+  DevBuf& stg = pipe ? c->pipe_stage[pb] : c->stage;
+  rc = stg.reserve(std::max<size_t>(sg.total, 256));
   if (rc) return rc;
-  char* sbase = (char*)c->stage.p;
+  char* sbase = (char*)stg.p;
   for (const auto& s : sg.segs)
     if (s.copy_in) RGF_CUDA(cudaMemcpyAsync(sbase + s.off, s.host, s.bytes, cudaMemcpyHostToDevice, st));
 
@@ -489,6 +570,27 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
   if (e != cudaSuccess) return fail(RGF_E_CUDA, "solver launch failed: %s", cudaGetErrorString(e));
   c->stats.launches++;
   RGF_CUDA(cudaEventRecord(c->ev1, st));
+
+  if (pipe) {
+    // ---- outputs back on the copy stream; the call returns now
+    RGF_CUDA(cudaEventRecord(c->pipe_solved, st));
+    RGF_CUDA(cudaStreamWaitEvent(c->copy_stream, c->pipe_solved, 0));
+    RGF_CUDA(cudaMemcpyAsync(c->pipe_info[pb], c->info.p, sizeof(DInfo) * n_tasks, cudaMemcpyDeviceToHost,
+                             c->copy_stream));
+    RGF_CUDA(cudaEventRecord(c->pipe_info_done, c->copy_stream));
+    for (const auto& s : sg.segs)
+      if (s.copy_out)
+        RGF_CUDA(cudaMemcpyAsync(const_cast<char*>(s.host), sbase + s.off, s.bytes, cudaMemcpyDeviceToHost,
+                                 c->copy_stream));
+    RGF_CUDA(cudaEventRecord(c->pipe_free[pb], c->copy_stream));
+    c->pipe_info_n[pb] = n_tasks;
+    c->pipe_nb[pb].resize(n_tasks);
+    for (int64_t t = 0; t < n_tasks; t++) c->pipe_nb[pb][t] = devices[tasks[t].device].nm;
+    c->pipe_last = pb;
+    c->pipe_sel ^= 1;
+    c->stats.last_tasks = n_tasks;
+    return RGF_OK;
+  }
 
   // ---- outputs back
   for (const auto& s : sg.segs)

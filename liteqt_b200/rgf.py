@@ -53,7 +53,7 @@ EXPORTS = (
     "rgf_permute_last_error", "rgf_write_spectrum", "rgf_write_dos", "rgf_write_current_spectrum",
     "rgf_write_current_summed_over_k", "rgf_write_transmission_spectrum", "rgf_write_id_iteration",
     "rgf_io_last_error", "rgf_read_ham_dat", "rgf_gw_polarization_fft", "rgf_gw_self_energy_fft",
-    "rgf_gw_fft_last_error",
+    "rgf_gw_fft_last_error", "rgf_ctx_synchronize",
 )
 
 # kernel variant ids (rgf_variant_name)
@@ -73,7 +73,8 @@ class c_opts(ctypes.Structure):
         ("boltz", ctypes.c_double), ("sancho_tol", ctypes.c_double),
         ("sancho_nmax", ctypes.c_int32), ("consistent", ctypes.c_int32),
         ("precision", ctypes.c_int32), ("want_T", ctypes.c_int32),
-        ("verbose", ctypes.c_int32), ("zero_copy", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6),
+        ("verbose", ctypes.c_int32), ("zero_copy", ctypes.c_int32), ("pipelined", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 5),
     ]
 
 
@@ -196,6 +197,8 @@ def load(path: str = LIB_PATH):
     L.rgf_calc_n_electron.argtypes = [P, P, P, ctypes.c_int64, P, ctypes.c_int64, ctypes.c_int64,
                                       ctypes.c_int64, P, P, P]
     L.rgf_ctx_get_stats.argtypes = [P, ctypes.POINTER(c_stats)]
+    L.rgf_ctx_synchronize.argtypes = [P]
+    L.rgf_ctx_synchronize.restype = ctypes.c_int
     L.rgf_calc_block_current.argtypes = [P, P, P, ctypes.c_int64, P, ctypes.c_double, ctypes.c_int64,
                                          ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, P, P, P]
     L.rgf_calc_block_current.restype = ctypes.c_int
@@ -249,6 +252,7 @@ class Options:
     want_T: bool = True
     verbose: bool = False
     zero_copy: bool = True
+    pipelined: bool = False
 
     def c(self) -> c_opts:
         o = c_opts()
@@ -264,6 +268,7 @@ class Options:
         o.want_T = int(self.want_T)
         o.verbose = int(self.verbose)
         o.zero_copy = int(self.zero_copy)
+        o.pipelined = int(self.pipelined)
         return o
 
 
@@ -342,6 +347,10 @@ class Context:
         o = opts.c()
         _check(load().rgf_ctx_set_opts(self.h, ctypes.byref(o)))
         self.opts = opts
+
+    def synchronize(self):
+        """rgf_ctx_synchronize: wait for queued (pipelined) solves and copies."""
+        _check(load().rgf_ctx_synchronize(self.h))
 
     def close(self):
         if getattr(self, "h", None):

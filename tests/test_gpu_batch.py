@@ -212,3 +212,45 @@ def test_T_only_solve_skips_nothing_it_needs(rgf):
         ctx.solve_energies(d.Hii, d.H1i, E, MU, _temp(), info=info_p, **part)
     assert np.array_equal(part["T"], full["T"]) and np.array_equal(part["tr"], full["tr"])
     assert np.all(info_p["n_gemm"] < info_f["n_gemm"])
+
+
+def test_pipelined_calls_match_synchronous_calls(rgf):
+    """rgf_opts.pipelined: calls return once queued, outputs staged in two
+    alternating device buffers and copied on the context's copy stream;
+    after rgf_ctx_synchronize every pinned host output equals the
+    synchronous call's, bit for bit (three calls in a row, the first and
+    third into the same arrays), and the statistics are those of the last
+    call."""
+    import torch
+    from liteqt_b200 import synthetic as S
+    nm, nx, nen = 32, 12, 40
+    d = S.make_device(nm, nx, seed=31)
+    temp = (S.temperature_for_kT(0.025),) * 2
+    Es = [S.energy_grid(nen, -2.5, 2.5) + 0.01 * k for k in range(3)]
+
+    def pinned():
+        o = {k: torch.zeros((nen, nx, nm, nm), dtype=torch.complex128).pin_memory() for k in ("ldos", "ndens")}
+        o.update({k: torch.zeros(nen, dtype=torch.float64).pin_memory() for k in ("T", "tr", "tre")})
+        return o
+    want = []
+    with rgf.Context(rgf.Options(eta_dev=1e-5, eta_lead=1e-5)) as ctx:
+        for E in Es:
+            o = pinned()
+            ctx.solve_energies(d.Hii, d.H1i, E, (0.1, -0.1), temp, **{k: v.numpy() for k, v in o.items()})
+            want.append({k: v.numpy().copy() for k, v in o.items()})
+    A, B = pinned(), pinned()
+    outs = [A, B, A]
+    with rgf.Context(rgf.Options(eta_dev=1e-5, eta_lead=1e-5, pipelined=True)) as ctx:
+        got = []
+        for k, E in enumerate(Es):
+            ctx.solve_energies(d.Hii, d.H1i, E, (0.1, -0.1), temp, **{n: v.numpy() for n, v in outs[k].items()})
+            if k == 1:   # the second call's outputs are final once the context is synchronised
+                ctx.synchronize()
+                got.append({n: v.numpy().copy() for n, v in B.items()})
+        ctx.synchronize()
+        got.append({n: v.numpy().copy() for n, v in A.items()})
+        st = ctx.stats()
+    for g, w in zip(got, (want[1], want[2])):
+        for n in w:
+            assert np.array_equal(g[n], w[n]), n
+    assert st["last_tasks"] == nen and st["last_kernel_ms"] > 0 and st["last_flops"] > 0
