@@ -53,9 +53,13 @@ struct StagedCfg {
   static constexpr int NSTAGE = 3;                             // cp.async pipeline depth (>= 2)
   static constexpr int PW = NB >= 256 ? 16 : (NB >= 128 ? 48 : 32);  // inverse panel width (max)
   static constexpr bool SMEM_INV = NB <= 64;                   // whole inverse in shared memory
+  // column pitch of the blocked inverse's shared panel (complex values): NB + 2
+  // makes the rank-8 updates' fragment reads of 4 columns x 2 rows hit 8
+  // distinct 16-byte bank groups (pitch NB: 4-way conflicts)
+  static constexpr int LDP = SMEM_INV ? NB : NB + 2;
   static constexpr size_t GEMM_SMEM = size_t(NSTAGE) * STAGE * sizeof(double2);
   // inverse: the matrix (nb <= 64) or one panel, then the row / column vectors
-  static constexpr size_t INV_MAT = SMEM_INV ? size_t(NB) * NB : size_t(NB) * PW;
+  static constexpr size_t INV_MAT = SMEM_INV ? size_t(NB) * NB : size_t(LDP) * PW;
   // inverse scratch after the matrix / panel, per form (complex values):
   // blocked (nb >= 128): pivot row + multiplier column + 8 pivot rows of the
   // panel's other columns, which also covers the sub-block elimination's
@@ -334,7 +338,7 @@ __device__ __noinline__ int gj_invert_reg(const double2* X, double2* dst, double
 // parity so one column's readers never race the next column's writers.
 // Returns with the sub-block written back to the panel and a barrier passed;
 // s.singular is set on a zero pivot.
-template <int NB>
+template <int NB, int LD = NB>
 __device__ __forceinline__ void gj_subblock(double2* panel, int PW, int p0, int sb0, double2* scr,
                                             int16_t* rmap, SmemInv& s) {
   constexpr int KB = 8;
@@ -351,7 +355,7 @@ __device__ __forceinline__ void gj_subblock(double2* panel, int PW, int p0, int 
   int* pi = reinterpret_cast<int*>(pk + 2 * WPC);               // [2][WPC] rows
   double2 x[CPT];
 #pragma unroll
-  for (int m = 0; m < CPT; m++) x[m] = panel[i + (size_t)(sb0 + h * CPT + m) * NB];
+  for (int m = 0; m < CPT; m++) x[m] = panel[i + (size_t)(sb0 + h * CPT + m) * LD];
 #pragma unroll
   for (int cc = 0; cc < KB; cc++) {
     const int k = p0 + sb0 + cc, par = cc & 1;
@@ -405,9 +409,9 @@ __device__ __forceinline__ void gj_subblock(double2* panel, int PW, int p0, int 
     if (q != k) {  // the panel's other columns: interchange rows k <-> q
       for (int j = tid; j < PW; j += kThreads) {
         if (j >= sb0 && j < sb0 + KB) continue;
-        const double2 a = panel[k + (size_t)j * NB];
-        panel[k + (size_t)j * NB] = panel[q + (size_t)j * NB];
-        panel[q + (size_t)j * NB] = a;
+        const double2 a = panel[k + (size_t)j * LD];
+        panel[k + (size_t)j * LD] = panel[q + (size_t)j * LD];
+        panel[q + (size_t)j * LD] = a;
       }
     }
     __syncthreads();
@@ -426,7 +430,7 @@ __device__ __forceinline__ void gj_subblock(double2* panel, int PW, int p0, int 
     }
   }
 #pragma unroll
-  for (int m = 0; m < CPT; m++) panel[i + (size_t)(sb0 + h * CPT + m) * NB] = x[m];
+  for (int m = 0; m < CPT; m++) panel[i + (size_t)(sb0 + h * CPT + m) * LD] = x[m];
   __syncthreads();
 }
 
@@ -437,7 +441,7 @@ __device__ __forceinline__ void gj_subblock(double2* panel, int PW, int p0, int 
 // on the FP64 tensor pipe: warp w owns rows 8 TMU w .. (TMU 8-row subtiles)
 // and walks the 8-column subtiles of the other columns; K = 8 is two m8n8k4
 // steps, U's fragments loaded once.  Ends with a barrier.
-template <int NB>
+template <int NB, int LD = NB>
 __device__ __forceinline__ void panel_rank8_update(double2* panel, int PW, int p0, int sb0, double2* rbuf) {
   constexpr int KB = 8;
   const int tid = threadIdx.x;
@@ -446,7 +450,7 @@ __device__ __forceinline__ void panel_rank8_update(double2* panel, int PW, int p
   for (int e = tid; e < KB * nrest; e += kThreads) {
     const int t = e % KB, jr = e / KB;
     const int j = jr < sb0 ? jr : jr + KB;
-    rbuf[t + jr * KB] = panel[(p0 + sb0 + t) + (size_t)j * NB];
+    rbuf[t + jr * KB] = panel[(p0 + sb0 + t) + (size_t)j * LD];
   }
   __syncthreads();
   constexpr int TMU = NB / (8 * (kThreads / 32));
@@ -457,7 +461,7 @@ __device__ __forceinline__ void panel_rank8_update(double2* panel, int PW, int p
 #pragma unroll
   for (int ks = 0; ks < 2; ks++)
 #pragma unroll
-    for (int a = 0; a < TMU; a++) av[ks][a] = panel[(wm + 8 * a + g) + (size_t)(sb0 + 4 * ks + t4) * NB];
+    for (int a = 0; a < TMU; a++) av[ks][a] = panel[(wm + 8 * a + g) + (size_t)(sb0 + 4 * ks + t4) * LD];
   for (int b = 0; b < nrest / 8; b++) {
     double cr[TMU][1][2], ci[TMU][1][2];
 #pragma unroll
@@ -474,7 +478,7 @@ __device__ __forceinline__ void panel_rank8_update(double2* panel, int PW, int p
         const int i = wm + 8 * a + g, jr = 8 * b + 2 * t4 + c;
         const int j = jr < sb0 ? jr : jr + KB;
         const bool prow = i >= p0 + sb0 && i < p0 + sb0 + KB;
-        const size_t o = i + (size_t)j * NB;
+        const size_t o = i + (size_t)j * LD;
         const double2 x = prow ? czero() : panel[o];
         panel[o] = make_double2(x.x + cr[a][0][c], x.y + ci[a][0][c]);
       }
@@ -546,7 +550,7 @@ __device__ int gj_invert_blocked(double2* X0, double2* X1, double2* dst, double2
   using C = StagedCfg<NB>;
   constexpr int PWM = C::PW;
   double2* panel = smem;
-  double2* rowk = panel + (size_t)NB * PWM;
+  double2* rowk = panel + (size_t)C::LDP * PWM;
   double2* fcol = rowk + PWM;
   int16_t* rmap = s.rmap;
   const int tid = threadIdx.x;
@@ -555,8 +559,11 @@ __device__ int gj_invert_blocked(double2* X0, double2* X1, double2* dst, double2
   if (tid == 0) s.singular = 0;
   for (int p0 = 0; p0 < NB; p0 += PWM) {
     const int PW = (NB - p0) < PWM ? (NB - p0) : PWM;
-    // (a) panel columns of the current matrix -> shared memory (ld NB)
-    for (int e = tid; e < NB * PW; e += kThreads) cp_async16(panel + e, cur + (size_t)p0 * NB + e);
+    // (a) panel columns of the current matrix -> shared memory (pitch LDP)
+    for (int e = tid; e < NB * PW; e += kThreads) {
+      const int jj = e / NB, i = e - jj * NB;
+      cp_async16(panel + i + (size_t)jj * C::LDP, cur + (size_t)p0 * NB + e);
+    }
     cp_async_commit();
     for (int i = tid; i < NB; i += kThreads) rmap[i] = (int16_t)i;
     cp_async_wait<0>();
@@ -572,9 +579,9 @@ __device__ int gj_invert_blocked(double2* X0, double2* X1, double2* dst, double2
     static_assert(PWM % KB == 0 && (NB % PWM) % KB == 0, "panels of whole sub-blocks");
     double2* rbuf = fcol + NB;  // KB x PWM pivot rows of the other columns
     for (int sb0 = 0; sb0 < PW && !s.singular; sb0 += KB) {
-      gj_subblock<NB>(panel, PW, p0, sb0, rowk, rmap, s);
+      gj_subblock<NB, C::LDP>(panel, PW, p0, sb0, rowk, rmap, s);
       if (s.singular) break;
-      panel_rank8_update<NB>(panel, PW, p0, sb0, rbuf);
+      panel_rank8_update<NB, C::LDP>(panel, PW, p0, sb0, rbuf);
     }
     if (s.singular) break;
     // the last panel writes the inverse itself: its column j is column
@@ -595,10 +602,10 @@ __device__ int gj_invert_blocked(double2* X0, double2* X1, double2* dst, double2
     }
     // (c) eliminated panel -> next matrix (its rows are already in the new order)
     for (int e = tid; e < NB * PW; e += kThreads) {
-      const double2 v = panel[e];
+      const int jj = e / NB, i = e - jj * NB;
+      const double2 v = panel[i + (size_t)jj * C::LDP];
       nxt[(size_t)p0 * NB + e] = v;
       if (last) {
-        const int jj = e / NB, i = e - jj * NB;
         const size_t o = i + (size_t)s.coldst[p0 + jj] * NB;
         dst[o] = v;
         if (dst2) dst2[o] = v;
