@@ -13,10 +13,12 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "rgf_internal.h"
@@ -78,6 +80,141 @@ struct DevBuf {
   }
 };
 
+// The copier of pipelined calls (rgf_opts.pipelined): one thread per context
+// follows each call's per-task progress counters (written by the kernel into
+// host-mapped memory after each block's outputs) and queues on the copy
+// stream the host copies of the blocks that are done, in chunks, while the
+// solve runs; once the solve has finished it queues the rest (blocks of tasks
+// without a backward sweep, scalars, task info) and records the call's event.
+struct PipeJob {
+  int slot = 0;
+  const volatile int32_t* prog = nullptr;   // host view of the progress counters
+  cudaEvent_t solved = nullptr;             // recorded after the solve
+  cudaEvent_t freed = nullptr;              // recorded after the call's last copy
+  struct Blocks {                           // one block-structured output of one task
+    char* host;
+    const char* dev;
+    size_t blk;                             // bytes per block
+    int64_t task;
+    int32_t nx;
+  };
+  struct Copy {
+    char* host;
+    const char* dev;
+    size_t bytes;
+  };
+  std::vector<Blocks> blocks;
+  std::vector<Copy> rest;
+};
+
+class PipeWorker {
+ public:
+  PipeWorker(int device, cudaStream_t cs) : dev_(device), cs_(cs), th_([this] { loop(); }) {}
+  ~PipeWorker() {
+    {
+      std::lock_guard<std::mutex> l(m_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    th_.join();
+  }
+  void push(PipeJob&& j) {
+    {
+      std::lock_guard<std::mutex> l(m_);
+      pending_[j.slot]++;
+      pushed_++;
+      q_.push_back(std::move(j));
+    }
+    cv_.notify_all();
+  }
+  // every job pushed so far has queued its copies
+  void drain() {
+    std::unique_lock<std::mutex> l(m_);
+    cv_.wait(l, [&] { return issued_ == pushed_; });
+  }
+  // the jobs of staging slot `slot` have queued their copies
+  void wait_slot(int slot) {
+    std::unique_lock<std::mutex> l(m_);
+    cv_.wait(l, [&] { return pending_[slot] == 0; });
+  }
+  cudaError_t take_error() {
+    std::lock_guard<std::mutex> l(m_);
+    const cudaError_t e = err_;
+    err_ = cudaSuccess;
+    return e;
+  }
+
+ private:
+  void loop() {
+    cudaSetDevice(dev_);
+    for (;;) {
+      PipeJob j;
+      {
+        std::unique_lock<std::mutex> l(m_);
+        cv_.wait(l, [&] { return stop_ || !q_.empty(); });
+        if (q_.empty()) return;
+        j = std::move(q_.front());
+        q_.pop_front();
+      }
+      const cudaError_t e = run(j);
+      {
+        std::lock_guard<std::mutex> l(m_);
+        if (e != cudaSuccess && err_ == cudaSuccess) err_ = e;
+        issued_++;
+        pending_[j.slot]--;
+      }
+      cv_.notify_all();
+    }
+  }
+  cudaError_t run(const PipeJob& j) {
+    constexpr int32_t kChunk = 8;   // blocks per copy while the solve runs
+    std::vector<int32_t> done(j.blocks.size(), 0);
+    cudaError_t e = cudaSuccess;
+    auto copy = [&](char* host, const char* dev, size_t bytes) {
+      const cudaError_t r = cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, cs_);
+      if (r != cudaSuccess && e == cudaSuccess) e = r;
+    };
+    for (;;) {
+      const cudaError_t q = cudaEventQuery(j.solved);
+      const bool fin = q != cudaErrorNotReady;
+      if (q != cudaSuccess && q != cudaErrorNotReady && e == cudaSuccess) e = q;
+      for (size_t b = 0; b < j.blocks.size(); b++) {
+        const PipeJob::Blocks& o = j.blocks[b];
+        int32_t c = j.prog[o.task];
+        c = c < 0 ? 0 : (c > o.nx ? o.nx : c);
+        if (c > done[b] && (fin || c - done[b] >= kChunk)) {
+          const size_t off = (size_t)(o.nx - c) * o.blk;
+          copy(o.host + off, o.dev + off, (size_t)(c - done[b]) * o.blk);
+          done[b] = c;
+        }
+      }
+      if (fin) break;
+      std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+    const cudaError_t w = cudaStreamWaitEvent(cs_, j.solved, 0);
+    if (w != cudaSuccess && e == cudaSuccess) e = w;
+    for (size_t b = 0; b < j.blocks.size(); b++) {   // blocks no counter covered
+      const PipeJob::Blocks& o = j.blocks[b];
+      if (done[b] < o.nx) copy(o.host, o.dev, (size_t)(o.nx - done[b]) * o.blk);
+    }
+    for (const PipeJob::Copy& r : j.rest) copy(r.host, r.dev, r.bytes);
+    const cudaError_t f = cudaEventRecord(j.freed, cs_);
+    if (f != cudaSuccess && e == cudaSuccess) e = f;
+    return e;
+  }
+
+  int dev_;
+  cudaStream_t cs_;
+  std::mutex m_;
+  std::condition_variable cv_;
+  std::deque<PipeJob> q_;
+  bool stop_ = false;
+  uint64_t pushed_ = 0, issued_ = 0;
+  int pending_[2] = {0, 0};
+  cudaError_t err_ = cudaSuccess;
+  std::thread th_;   // last member: started once the others exist
+};
+
 }  // namespace
 
 struct rgf_ctx {
@@ -92,17 +229,19 @@ struct rgf_ctx {
   int8_t ctas[kVariantSlots];     // resident CTAs per SM per block size, 0 = as many as fit
   void* ext_cache = nullptr;      // per-context state of other modules (the FFT form's plans)
   void (*ext_cache_free)(void*) = nullptr;
-  // pipelined host outputs (rgf_opts.pipelined): two staging buffers used in
-  // turn, the copy stream that takes each call's outputs to the host, and per
-  // buffer the event after its copies and a pinned copy of the call's task info
-  DevBuf pipe_stage[2];
+  // pipelined host outputs (rgf_opts.pipelined): two staging slots used in
+  // turn, each with its staging buffer, device and pinned task info, host-
+  // mapped progress counters and events (solve done, copies done); the copy
+  // stream and the copier thread that follows the counters
+  DevBuf pipe_stage[2], pipe_dinfo[2];
   cudaStream_t copy_stream = nullptr;
-  cudaEvent_t pipe_free[2] = {nullptr, nullptr};
-  cudaEvent_t pipe_solved = nullptr, pipe_info_done = nullptr;
+  cudaEvent_t pipe_free[2] = {nullptr, nullptr}, pipe_solved[2] = {nullptr, nullptr};
   DInfo* pipe_info[2] = {nullptr, nullptr};
-  int64_t pipe_info_cap[2] = {0, 0}, pipe_info_n[2] = {0, 0};
+  int32_t* pipe_prog[2] = {nullptr, nullptr};   // host-mapped, one counter per task
+  int64_t pipe_cap[2] = {0, 0}, pipe_info_n[2] = {0, 0};
   int pipe_sel = 0, pipe_last = -1;
   std::vector<int64_t> pipe_nb[2];   // block size of each task of the call, for the stats
+  std::unique_ptr<PipeWorker> worker;
 };
 
 void* rgf::ctx_ext_cache(rgf_ctx* c) { return c->ext_cache; }
@@ -173,15 +312,17 @@ extern "C" int rgf_ctx_destroy(rgf_ctx* c) {
   if (!c) return RGF_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  c->worker.reset();   // queues the copies of every pushed call, then stops
   if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
   if (c->ext_cache_free) c->ext_cache_free(c->ext_cache);
   for (int b = 0; b < 2; b++) {
     c->pipe_stage[b].release();
+    c->pipe_dinfo[b].release();
     if (c->pipe_free[b]) cudaEventDestroy(c->pipe_free[b]);
+    if (c->pipe_solved[b]) cudaEventDestroy(c->pipe_solved[b]);
     if (c->pipe_info[b]) cudaFreeHost(c->pipe_info[b]);
+    if (c->pipe_prog[b]) cudaFreeHost(c->pipe_prog[b]);
   }
-  if (c->pipe_solved) cudaEventDestroy(c->pipe_solved);
-  if (c->pipe_info_done) cudaEventDestroy(c->pipe_info_done);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   c->work.release();
   c->tasks.release();
@@ -207,6 +348,11 @@ extern "C" int rgf_ctx_get_stats(const rgf_ctx* c, rgf_stats* s) {
 extern "C" int rgf_ctx_synchronize(rgf_ctx* c) {
   if (!c) return fail(RGF_E_ARG, "ctx is NULL");
   RGF_CUDA(cudaSetDevice(c->device));
+  if (c->worker) {
+    c->worker->drain();
+    const cudaError_t e = c->worker->take_error();
+    if (e != cudaSuccess) return fail(RGF_E_CUDA, "pipelined output copies: %s", cudaGetErrorString(e));
+  }
   if (c->copy_stream) RGF_CUDA(cudaStreamSynchronize(c->copy_stream));
   const int b = c->pipe_last;
   if (b >= 0) {
@@ -307,6 +453,19 @@ struct Stage {
       s.off = total;
       total += (s.bytes + 255) & ~size_t(255);
     }
+  }
+  // the staged segment holding host address p, or nullptr (device memory,
+  // written through its mapping, or NULL)
+  const Seg* find(const void* p) const {
+    if (!p) return nullptr;
+    const char* h = (const char*)p;
+    size_t lo = 0, hi = segs.size();
+    while (lo < hi) {
+      const size_t mid = (lo + hi) / 2;
+      if (segs[mid].host <= h) lo = mid + 1; else hi = mid;
+    }
+    if (lo > 0 && h < segs[lo - 1].host + segs[lo - 1].bytes) return &segs[lo - 1];
+    return nullptr;
   }
   // device address of a registered host pointer (or p itself if device / NULL)
   void* resolve(const void* p, char* dbase) const {
@@ -459,35 +618,39 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
   sg.layout();
   const int pb = c->pipe_sel;
   if (pipe) {
-    if (!c->copy_stream) {
+    if (!c->worker) {
       RGF_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
-      RGF_CUDA(cudaEventCreateWithFlags(&c->pipe_solved, cudaEventDisableTiming));
-      RGF_CUDA(cudaEventCreateWithFlags(&c->pipe_info_done, cudaEventDisableTiming));
-      RGF_CUDA(cudaEventRecord(c->pipe_info_done, c->copy_stream));
       for (int b = 0; b < 2; b++) {
         RGF_CUDA(cudaEventCreateWithFlags(&c->pipe_free[b], cudaEventDisableTiming));
+        RGF_CUDA(cudaEventCreateWithFlags(&c->pipe_solved[b], cudaEventDisableTiming));
         RGF_CUDA(cudaEventRecord(c->pipe_free[b], c->copy_stream));
       }
+      c->worker.reset(new PipeWorker(c->device, c->copy_stream));
     }
-    // a buffer that must grow is freed only once its copies are done
-    if (c->pipe_stage[pb].bytes < sg.total) RGF_CUDA(cudaEventSynchronize(c->pipe_free[pb]));
-    if (c->pipe_info_cap[pb] < n_tasks) {
+    // the call that used this slot has queued its copies (its event is
+    // recorded, its solve is done, its counters are no longer read)
+    c->worker->wait_slot(pb);
+    // buffers that must grow are freed only once their copies are done
+    if (c->pipe_stage[pb].bytes < sg.total || c->pipe_cap[pb] < n_tasks)
       RGF_CUDA(cudaEventSynchronize(c->pipe_free[pb]));
+    if (c->pipe_cap[pb] < n_tasks) {
       if (c->pipe_info[pb]) cudaFreeHost(c->pipe_info[pb]);
+      if (c->pipe_prog[pb]) cudaFreeHost(c->pipe_prog[pb]);
       c->pipe_info[pb] = nullptr;
-      c->pipe_info_cap[pb] = 0;
+      c->pipe_prog[pb] = nullptr;
+      c->pipe_cap[pb] = 0;
       RGF_CUDA(cudaMallocHost((void**)&c->pipe_info[pb], sizeof(DInfo) * (size_t)n_tasks));
-      c->pipe_info_cap[pb] = n_tasks;
+      RGF_CUDA(cudaHostAlloc((void**)&c->pipe_prog[pb], sizeof(int32_t) * (size_t)n_tasks, cudaHostAllocMapped));
+      c->pipe_cap[pb] = n_tasks;
     }
+    if ((rc = c->pipe_dinfo[pb].reserve(sizeof(DInfo) * n_tasks))) return rc;
+    std::memset(c->pipe_prog[pb], 0, sizeof(int32_t) * (size_t)n_tasks);
     RGF_CUDA(cudaStreamWaitEvent(st, c->pipe_free[pb], 0));
-  }
-  if (c->copy_stream) {
-    // the task info of the previous pipelined call is copied out before this
-    // call resets it; a call that is not pipelined also waits for every
-    // pending copy (it may write the same host arrays)
-    RGF_CUDA(cudaStreamWaitEvent(st, c->pipe_info_done, 0));
-    if (!pipe)
-      for (int b = 0; b < 2; b++) RGF_CUDA(cudaStreamWaitEvent(st, c->pipe_free[b], 0));
+  } else if (c->worker) {
+    // a call that is not pipelined may write the same host arrays: it
+    // follows every queued copy
+    c->worker->drain();
+    for (int b = 0; b < 2; b++) RGF_CUDA(cudaStreamWaitEvent(st, c->pipe_free[b], 0));
   }
   DevBuf& stg = pipe ? c->pipe_stage[pb] : c->stage;
   rc = stg.reserve(std::max<size_t>(sg.total, 256));
@@ -553,7 +716,8 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
   RGF_CUDA(cudaMemcpyAsync(c->devs.p, ddev.data(), sizeof(DDev) * n_devices, cudaMemcpyHostToDevice, st));
   RGF_CUDA(cudaMemcpyAsync(c->tasks.p, dtask.data(), sizeof(DTask) * n_tasks, cudaMemcpyHostToDevice, st));
   RGF_CUDA(cudaMemcpyAsync(order_d, order.data(), sizeof(int32_t) * n_tasks, cudaMemcpyHostToDevice, st));
-  RGF_CUDA(cudaMemsetAsync(c->info.p, 0, sizeof(DInfo) * n_tasks, st));
+  DInfo* dinfo = pipe ? (DInfo*)c->pipe_dinfo[pb].p : (DInfo*)c->info.p;
+  RGF_CUDA(cudaMemsetAsync(dinfo, 0, sizeof(DInfo) * n_tasks, st));
   RGF_CUDA(cudaMemsetAsync(c->queue.p, 0, sizeof(int32_t), st));
   KParams p;
   fill_params(c, p);
@@ -564,7 +728,8 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
   p.queue = (int32_t*)c->queue.p;
   p.work = (double2*)c->work.p;
   p.slot_elems = slot;
-  p.info = (DInfo*)c->info.p;
+  p.info = dinfo;
+  if (pipe) RGF_CUDA(cudaHostGetDevicePointer((void**)&p.progress, c->pipe_prog[pb], 0));
   RGF_CUDA(cudaEventRecord(c->ev0, st));
   cudaError_t e = mixed ? launch_mixed(p, grid, st) : launch_solver(p, grid, smem, st);
   if (e != cudaSuccess) return fail(RGF_E_CUDA, "solver launch failed: %s", cudaGetErrorString(e));
@@ -572,17 +737,43 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
   RGF_CUDA(cudaEventRecord(c->ev1, st));
 
   if (pipe) {
-    // ---- outputs back on the copy stream; the call returns now
-    RGF_CUDA(cudaEventRecord(c->pipe_solved, st));
-    RGF_CUDA(cudaStreamWaitEvent(c->copy_stream, c->pipe_solved, 0));
-    RGF_CUDA(cudaMemcpyAsync(c->pipe_info[pb], c->info.p, sizeof(DInfo) * n_tasks, cudaMemcpyDeviceToHost,
-                             c->copy_stream));
-    RGF_CUDA(cudaEventRecord(c->pipe_info_done, c->copy_stream));
-    for (const auto& s : sg.segs)
-      if (s.copy_out)
-        RGF_CUDA(cudaMemcpyAsync(const_cast<char*>(s.host), sbase + s.off, s.bytes, cudaMemcpyDeviceToHost,
-                                 c->copy_stream));
-    RGF_CUDA(cudaEventRecord(c->pipe_free[pb], c->copy_stream));
+    // ---- outputs back: the copier queues them as the blocks are written;
+    // the call returns now
+    RGF_CUDA(cudaEventRecord(c->pipe_solved[pb], st));
+    PipeJob j;
+    j.slot = pb;
+    j.prog = c->pipe_prog[pb];
+    j.solved = c->pipe_solved[pb];
+    j.freed = c->pipe_free[pb];
+    std::vector<std::pair<const char*, const char*>> covered;   // host ranges copied block by block
+    for (int64_t t = 0; t < n_tasks; t++) {
+      const rgf_task& k = tasks[t];
+      const rgf_device& v = devices[k.device];
+      const size_t n2 = (size_t)v.nm * v.nm;
+      const void* outs[7] = {k.ldos, k.ndens, k.pdens, k.GRi1, k.GLi1, k.GGi1, k.cur};
+      for (int a = 0; a < 7; a++) {
+        if (!sg.find(outs[a])) continue;
+        const size_t blk = n2 * (a == 6 ? sizeof(double) : sizeof(rgf_c16));
+        char* h = (char*)outs[a];
+        j.blocks.push_back({h, (const char*)sg.resolve(outs[a], sbase), blk, t, (int32_t)v.nx});
+        covered.push_back({h, h + blk * (size_t)v.nx});
+      }
+    }
+    std::sort(covered.begin(), covered.end());
+    for (const auto& sgm : sg.segs) {   // the rest of every output segment
+      if (!sgm.copy_out) continue;
+      const char* end = sgm.host + sgm.bytes;
+      const char* at = sgm.host;
+      for (const auto& r : covered) {
+        if (r.second <= at || r.first >= end) continue;
+        if (r.first > at) j.rest.push_back({(char*)at, sbase + sgm.off + (at - sgm.host), (size_t)(r.first - at)});
+        at = std::max(at, r.second);
+        if (at >= end) break;
+      }
+      if (at < end) j.rest.push_back({(char*)at, sbase + sgm.off + (at - sgm.host), (size_t)(end - at)});
+    }
+    j.rest.push_back({(char*)c->pipe_info[pb], (const char*)dinfo, sizeof(DInfo) * (size_t)n_tasks});
+    c->worker->push(std::move(j));
     c->pipe_info_n[pb] = n_tasks;
     c->pipe_nb[pb].resize(n_tasks);
     for (int64_t t = 0; t < n_tasks; t++) c->pipe_nb[pb][t] = devices[tasks[t].device].nm;

@@ -108,6 +108,8 @@ struct KParams {
   double2* work;           // workspace: one slot per resident CTA
   int64_t slot_elems;      // complex elements per slot (>= slot_elems_for(nb, nx) of every task)
   DInfo* info;             // per task
+  int32_t* progress;       // per task, or NULL: blocks whose outputs are written, counted from
+                           // the last (host-mapped; the pipelined output copies follow it)
   const DAdj* adj;         // non-null: run the adjoint instead of the drop-in solve
   const DWTask* wtasks;    // non-null: run W solves (green_rgf_calc_w)
   int8_t variant[kVariantSlots];  // kernel variant per block size (nb / 8), KV_NONE = unsupported

@@ -89,7 +89,7 @@ __device__ __noinline__ void task_mixed128(const KParams& p, int64_t t, double2*
                temps + (size_t)kNumTemps * n2, temps + (size_t)(kNumTemps + 1) * n2,
                temps + (size_t)(kNumTemps + 2) * n2, c.tmem, c.st);
   Solver<MixedOps> s(p.o, dv.nx, sm, ops, slot, 128, (int)dv.nx);
-  s.run(p.tasks[t], dv, info);
+  s.run(p.tasks[t], dv, info, p.progress ? p.progress + t : nullptr);
   if (info && threadIdx.x == 0) {
     info->n_inv += ops.n_fallback + ops.n_fp64_inv;
     info->pad = ops.n_pairs;

@@ -329,7 +329,17 @@ struct Solver {
     return taken;
   }
 
-  __device__ void run(const DTask& tk, const DDev& dv, DInfo* info) {
+  // Publishes that the outputs of the last `count` blocks are in memory for
+  // a reader outside the GPU (the pipelined host copies): every thread's
+  // stores are made visible system-wide, then one thread sets the counter.
+  __device__ static void publish(int32_t* progress, int count) {
+    if (!progress) return;
+    __threadfence_system();
+    __syncthreads();
+    if (threadIdx.x == 0) *(volatile int32_t*)progress = count;
+  }
+
+  __device__ void run(const DTask& tk, const DDev& dv, DInfo* info, int32_t* progress = nullptr) {
     const int nn = n;
     const double E = tk.E;
     const double2 z = make_double2(E, o.eta_dev);
@@ -568,6 +578,7 @@ struct Solver {
     // (g Sigma^<_lead g^H and g H Gl< H^H g^H with anti-Hermitian factors)
     if (need_cur)
       for_each_elem(n, [&](int, int, int idx) { blk2(tk.cur, nx - 1)[idx] = 0.0; });
+    if (need_back) publish(progress, 1);   // block nx-1: from the right closure
     for (int l = need_back ? nx - 2 : -1; l >= 0; l--) {
       const double2* Hb = blk(H1i, o.consistent ? l + 1 : l);
       const double2* gl = Gl(l);
@@ -668,6 +679,7 @@ struct Solver {
       }
       double2* t1 = G00; G00 = G00n; G00n = t1;
       double2* t2 = Gn; Gn = Gnn; Gnn = t2;
+      publish(progress, nx - l);
     }
 
     // ------------------------------------------------ left trace (tre)
@@ -1099,7 +1111,7 @@ __device__ __forceinline__ void solve_task(const KParams& p, int64_t t, double2*
   Solver<Ops> s(p.o, dv.nx, sm, ops, slot, n, (int)dv.nx);
   if (p.adj) s.run_adjoint(p.adj[t], dv, info);
   else if (p.wtasks) s.run_w(p.wtasks[t], dv, info);
-  else s.run(p.tasks[t], dv, info);
+  else s.run(p.tasks[t], dv, info, p.progress ? p.progress + t : nullptr);
 }
 
 }  // namespace

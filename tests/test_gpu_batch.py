@@ -216,9 +216,11 @@ def test_T_only_solve_skips_nothing_it_needs(rgf):
 
 def test_pipelined_calls_match_synchronous_calls(rgf):
     """rgf_opts.pipelined: calls return once queued, outputs staged in two
-    alternating device buffers and copied on the context's copy stream;
-    after rgf_ctx_synchronize every pinned host output equals the
-    synchronous call's, bit for bit (three calls in a row, the first and
+    alternating device buffers and copied on the context's copy stream, the
+    blocks of the backward sweep as the kernel reports them written; after
+    rgf_ctx_synchronize every pinned host output (block outputs of both
+    element types, the untouched last block of GRi1, the scalars) equals
+    the synchronous call's, bit for bit (three calls in a row, the first and
     third into the same arrays), and the statistics are those of the last
     call."""
     import torch
@@ -229,7 +231,10 @@ def test_pipelined_calls_match_synchronous_calls(rgf):
     Es = [S.energy_grid(nen, -2.5, 2.5) + 0.01 * k for k in range(3)]
 
     def pinned():
-        o = {k: torch.zeros((nen, nx, nm, nm), dtype=torch.complex128).pin_memory() for k in ("ldos", "ndens")}
+        o = {k: torch.zeros((nen, nx, nm, nm), dtype=torch.complex128).pin_memory()
+             for k in ("ldos", "ndens", "pdens", "GRi1")}
+        o["GRi1"].fill_(complex(3.0, -1.0))   # block nx is left untouched
+        o["cur"] = torch.zeros((nen, nx, nm, nm), dtype=torch.float64).pin_memory()
         o.update({k: torch.zeros(nen, dtype=torch.float64).pin_memory() for k in ("T", "tr", "tre")})
         return o
     want = []
