@@ -90,10 +90,11 @@ typedef struct rgf_opts {
                               device mapping, so the transfer overlaps the solve; 0: staged in
                               device memory and copied back after the launch */
   int32_t pipelined;       /* 1: rgf_solve_batch / rgf_solve_energies called with info = NULL
-                              return once the solve and the copies of its host outputs are
-                              queued: outputs are staged in one of two device buffers (taken in
-                              turn) and copied to the host by the copy engine on the context's
-                              copy stream, so one call's copy overlaps the next call's solve.
+                              return once the solve is queued: outputs are staged in one of two
+                              device buffers (taken in turn); a copier thread of the context
+                              queues the host copies of each task's blocks as the kernel reports
+                              them written, on the context's copy stream, so the copies run
+                              while the solve runs and overlap the next call's solve.
                               Host outputs (and tr, tre, T) hold the results after
                               rgf_ctx_synchronize(ctx), which also completes the statistics;
                               until then the host arrays must not be read or reused.  Overlap
