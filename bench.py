@@ -83,6 +83,9 @@ def parse():
                    help="time the per-energy drop-in green_RGF_RS called from every host thread at once, "
                         "each on its own energies (the reference's `!$omp do` loop), against the batched "
                         "entry point on the same energies and outputs")
+    p.add_argument("--per-thread", type=int, default=2,
+                   help="energies each host thread solves in --dropin (the thread count is --cpu-threads, "
+                        "default every host thread; OMP_NUM_THREADS plays that role for the reference's loop)")
     p.add_argument("--uneven", action="store_true",
                    help="uneven batch: 64 devices, Nx in {20..200}, nb in {32,64,128}, one graph-replayed "
                         "persistent launch (--nen energies per device per step; default 32)")
@@ -932,7 +935,7 @@ def run_dropin(args):
     rgf.load()
     d, E_all, temp = workload(args)
     nthr = host_threads(args)
-    per = 2
+    per = max(1, args.per_thread)
     nen = nthr * per
     E = np.ascontiguousarray(E_all[np.linspace(0, len(E_all) - 1, nen).astype(int)])
     nm, nx = args.nb, args.nx
@@ -966,6 +969,7 @@ def run_dropin(args):
     for t in threads:
         t.join()
     t_drop = time.perf_counter() - t0
+    outs.clear()   # the drop-in arrays go before the batched arm's are made (host memory)
     # the batched entry point on the same energies, options and output set
     shape = (nen, nx, nm, nm)
     B = dict(ldos=np.zeros(shape, complex), ndens=np.zeros(shape, complex), pdens=np.zeros(shape, complex),
@@ -978,6 +982,7 @@ def run_dropin(args):
     line = {"metric": "per-energy drop-in energy-pts/s (green_RGF_RS from every host thread)",
             "value": nen / t_drop, "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
             "config": {"workload": f"rgf_nb{nm}_nx{nx}", "host_threads": nthr, "energies": nen,
+                       "energies_per_thread": per,
                        "options": "the reference's (device eta 0, lead eta 1e-3)",
                        "outputs": ["ndens", "pdens", "ldos", "cur", "GRi1", "tr", "tre"],
                        "memory": "pageable host arrays, as Fortran passes them"},

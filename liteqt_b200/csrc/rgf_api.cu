@@ -6,6 +6,7 @@
 // happens on the host, and there is no CPU fallback: if the CUDA path cannot
 // run, the call fails with RGF_E_CUDA / RGF_E_UNSUPPORTED.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -80,6 +81,279 @@ struct DevBuf {
   }
 };
 
+// Host threads that share out the memcpy chunks of one bounce piece (below).
+// One pool per process: a piece takes it whole (its caller copying too), and
+// a caller that finds it taken copies its piece alone, so concurrent copiers
+// (one context per host thread) never run more copy threads than the pool's
+// plus their own.
+class CopyPool {
+ public:
+  struct Chunk {
+    char* dst;
+    const char* src;
+    size_t bytes;
+  };
+  static CopyPool& get() {
+    static CopyPool* p = new CopyPool();   // never destroyed: its threads outlive static destructors
+    return *p;
+  }
+  // copies every chunk; returns once all are done
+  void copy(const std::vector<Chunk>& chunks) {
+    std::unique_lock<std::mutex> busy(use_, std::try_to_lock);
+    if (!busy.owns_lock() || th_.empty() || chunks.size() < 2) {
+      for (const Chunk& c : chunks) std::memcpy(c.dst, c.src, c.bytes);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> l(m_);
+      list_ = &chunks;
+      next_ = 0;
+      remaining_ = (int)th_.size();
+      gen_++;
+    }
+    cv_.notify_all();
+    take();
+    std::unique_lock<std::mutex> l(m_);
+    done_cv_.wait(l, [&] { return remaining_ == 0; });
+    list_ = nullptr;
+  }
+
+ private:
+  CopyPool() {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int n = (int)std::max(1u, std::min(12u, hw * 3 / 4));
+    for (int t = 0; t + 1 < n; t++) th_.emplace_back([this] { worker(); });
+  }
+  void take() {
+    const std::vector<Chunk>& v = *list_;
+    for (;;) {
+      const size_t i = next_.fetch_add(1);
+      if (i >= v.size()) return;
+      std::memcpy(v[i].dst, v[i].src, v[i].bytes);
+    }
+  }
+  void worker() {
+    uint64_t seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> l(m_);
+        cv_.wait(l, [&] { return gen_ != seen; });
+        seen = gen_;
+      }
+      take();
+      {
+        std::lock_guard<std::mutex> l(m_);
+        if (--remaining_ == 0) done_cv_.notify_one();
+      }
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex use_;   // held by the piece the pool works on
+  std::mutex m_;
+  std::condition_variable cv_, done_cv_;
+  uint64_t gen_ = 0;
+  int remaining_ = 0;
+  const std::vector<Chunk>* list_ = nullptr;
+  std::atomic<size_t> next_{0};
+};
+
+// Copies between device memory and pageable (not page-locked) host memory at
+// the host link's speed.  The driver moves a pageable copy through its own
+// pinned buffer with one host thread (about 12 GB/s on the B200 hosts, a
+// quarter of the link); here the DMA lands in (or leaves from) pinned bounce
+// slots, kSlots x kPiece bytes, and the host side of the pieces -- pinned slot
+// <-> the caller's arrays -- is cut into chunks of at most kChunk bytes that
+// the CopyPool copies, every piece that has landed at once, while the next
+// pieces are on the link.
+//   enqueue_d2h queues device -> slot copies on `st` (after the work already
+//   on it), packing the runs into pieces; poll writes the destinations of the
+//   pieces that have landed, finish those of every queued piece (a slot is
+//   reused once its piece is written out, so enqueue_d2h itself completes
+//   older pieces when it runs out of slots).  d2h = enqueue_d2h + finish.
+//   h2d copies host -> device and returns with every source read.
+class PageableCopier {
+ public:
+  struct Copy {
+    char* host;
+    char* dev;
+    size_t bytes;
+  };
+  static constexpr int kSlots = 16;
+  static constexpr size_t kPiece = size_t(8) << 20;
+  static constexpr size_t kChunk = size_t(2) << 20;
+  static constexpr size_t kSmall = size_t(1) << 20;
+
+  ~PageableCopier() {
+    for (int s = 0; s < kSlots; s++) {
+      if (ev_[s]) cudaEventDestroy(ev_[s]);
+      if (slot_[s]) cudaFreeHost(slot_[s]);
+    }
+  }
+
+  cudaError_t enqueue_d2h(const std::vector<Copy>& copies, cudaStream_t st) {
+    cudaError_t e = setup();
+    if (e != cudaSuccess) return e;
+    Piece cur;
+    cur.slot = -1;
+    size_t fill = 0;
+    for (const Copy& c : copies)
+      for (size_t at = 0; at < c.bytes;) {
+        if (cur.slot < 0) {
+          if (free_.empty() && (e = complete(false, true)) != cudaSuccess) return e;
+          cur.slot = free_.back();
+          free_.pop_back();
+          fill = 0;
+        }
+        const size_t n = std::min(c.bytes - at, kPiece - fill);
+        cur.parts.push_back({c.host + at, c.dev + at, n, fill});
+        fill = (fill + n + 255) & ~size_t(255);
+        at += n;
+        if (fill >= kPiece) {
+          if ((e = issue(cur, st, true)) != cudaSuccess) return e;
+          cur = Piece();
+          cur.slot = -1;
+        }
+      }
+    if (cur.slot >= 0 && (e = issue(cur, st, true)) != cudaSuccess) return e;
+    return cudaSuccess;
+  }
+  cudaError_t poll() { return complete(false, false); }
+  cudaError_t finish() { return complete(true, false); }
+  cudaError_t d2h(const std::vector<Copy>& copies, cudaStream_t st) {
+    cudaError_t e = enqueue_d2h(copies, st);
+    const cudaError_t f = finish();
+    return e != cudaSuccess ? e : f;
+  }
+  cudaError_t h2d(const std::vector<Copy>& copies, cudaStream_t st) {
+    cudaError_t e = setup();
+    if (e == cudaSuccess) e = finish();   // every slot free
+    if (e != cudaSuccess) return e;
+    // rounds: as many pieces as there are free slots, their sources copied
+    // into the slots in one pool pass, then their DMAs queued; a slot is
+    // free again once its DMA has read it
+    std::vector<Piece> round;
+    size_t ci = 0, at = 0;
+    std::deque<int> busy;
+    while (ci < copies.size()) {
+      while (free_.empty()) {
+        if ((e = cudaEventSynchronize(ev_[busy.front()])) != cudaSuccess) return e;
+        free_.push_back(busy.front());
+        busy.pop_front();
+      }
+      round.clear();
+      while (!free_.empty() && ci < copies.size()) {
+        Piece pc;
+        pc.slot = free_.back();
+        free_.pop_back();
+        size_t fill = 0;
+        while (ci < copies.size() && fill < kPiece) {
+          const Copy& c = copies[ci];
+          const size_t n = std::min(c.bytes - at, kPiece - fill);
+          pc.parts.push_back({c.host + at, c.dev + at, n, fill});
+          fill = (fill + n + 255) & ~size_t(255);
+          at += n;
+          if (at == c.bytes) {
+            ci++;
+            at = 0;
+          }
+        }
+        round.push_back(std::move(pc));
+      }
+      host_side(round, false);
+      for (Piece& pc : round) {
+        if ((e = issue(pc, st, false)) != cudaSuccess) return e;
+        busy.push_back(pc.slot);   // h2d pieces are tracked here, not in inflight_
+      }
+    }
+    for (int sl : busy) {
+      if ((e = cudaEventSynchronize(ev_[sl])) != cudaSuccess) return e;
+      free_.push_back(sl);
+    }
+    return cudaSuccess;
+  }
+
+ private:
+  struct Part {   // one run of a piece: host range <-> slot offset, device address
+    char* host;
+    char* dev;
+    size_t bytes;
+    size_t off;
+  };
+  struct Piece {
+    std::vector<Part> parts;
+    int slot;
+  };
+  cudaError_t setup() {
+    if (slot_[0]) return cudaSuccess;
+    for (int s = 0; s < kSlots; s++) {
+      cudaError_t e = cudaHostAlloc((void**)&slot_[s], kPiece, cudaHostAllocDefault);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_[s], cudaEventDisableTiming);
+      if (e != cudaSuccess) return e;
+      free_.push_back(kSlots - 1 - s);
+    }
+    return cudaSuccess;
+  }
+  // queues the DMA of one piece and records its slot's event
+  cudaError_t issue(Piece& pc, cudaStream_t st, bool d2h) {
+    char* sl = slot_[pc.slot];
+    for (const Part& p : pc.parts) {
+      const cudaError_t r = d2h ? cudaMemcpyAsync(sl + p.off, p.dev, p.bytes, cudaMemcpyDeviceToHost, st)
+                                : cudaMemcpyAsync(p.dev, sl + p.off, p.bytes, cudaMemcpyHostToDevice, st);
+      if (r != cudaSuccess) return r;
+    }
+    const cudaError_t r = cudaEventRecord(ev_[pc.slot], st);
+    if (r != cudaSuccess) return r;
+    if (d2h) inflight_.push_back(std::move(pc));
+    return cudaSuccess;
+  }
+  // host side of pieces: slot -> destinations (d2h) or sources -> slot, in
+  // chunks shared out by the CopyPool
+  void host_side(const std::vector<Piece>& pieces, bool d2h) {
+    chunks_.clear();
+    size_t total = 0;
+    for (const Piece& pc : pieces)
+      for (const Part& p : pc.parts)
+        for (size_t a = 0; a < p.bytes; a += kChunk) {
+          const size_t n = std::min(kChunk, p.bytes - a);
+          char* sl = slot_[pc.slot] + p.off + a;
+          if (d2h) chunks_.push_back({p.host + a, sl, n});
+          else chunks_.push_back({sl, p.host + a, n});
+          total += n;
+        }
+    if (total < kSmall) {
+      for (const CopyPool::Chunk& c : chunks_) std::memcpy(c.dst, c.src, c.bytes);
+      return;
+    }
+    CopyPool::get().copy(chunks_);
+  }
+  // writes out the queued pieces that have landed (all of them if `all`; at
+  // least the oldest if `one`) and frees their slots
+  cudaError_t complete(bool all, bool one) {
+    std::vector<Piece> ready;
+    while (!inflight_.empty()) {
+      const int sl = inflight_.front().slot;
+      cudaError_t q = cudaEventQuery(ev_[sl]);
+      if (q == cudaErrorNotReady) {
+        if (!all && !(one && ready.empty())) break;
+        q = cudaEventSynchronize(ev_[sl]);
+      }
+      if (q != cudaSuccess) return q;
+      ready.push_back(std::move(inflight_.front()));
+      inflight_.pop_front();
+    }
+    if (ready.empty()) return cudaSuccess;
+    host_side(ready, true);
+    for (const Piece& pc : ready) free_.push_back(pc.slot);
+    return cudaSuccess;
+  }
+
+  char* slot_[kSlots] = {};
+  cudaEvent_t ev_[kSlots] = {};
+  std::vector<int> free_;          // slots without a queued piece
+  std::deque<Piece> inflight_;     // queued device -> host pieces, oldest first
+  std::vector<CopyPool::Chunk> chunks_;
+};
+
 // The copier of pipelined calls (rgf_opts.pipelined): one thread per context
 // follows each call's per-task progress counters (written by the kernel into
 // host-mapped memory after each block's outputs) and queues on the copy
@@ -96,12 +370,15 @@ struct PipeJob {
     const char* dev;
     size_t blk;                             // bytes per block
     int64_t task;
-    int32_t nx;
+    int32_t nx;                             // blocks of the output
+    int32_t lag;                            // counter value at which its last block is done, minus nx
+    bool pageable;                          // host array not page-locked
   };
   struct Copy {
     char* host;
     const char* dev;
     size_t bytes;
+    bool pageable;
   };
   std::vector<Blocks> blocks;
   std::vector<Copy> rest;
@@ -170,9 +447,30 @@ class PipeWorker {
     constexpr int32_t kChunk = 8;   // blocks per copy while the solve runs
     std::vector<int32_t> done(j.blocks.size(), 0);
     cudaError_t e = cudaSuccess;
-    auto copy = [&](char* host, const char* dev, size_t bytes) {
+    // copies to pageable arrays are gathered per round (flush below); the
+    // others are queued on the copy stream
+    std::vector<PageableCopier::Copy> slow;
+    auto copy = [&](char* host, const char* dev, size_t bytes, bool pageable) {
+      if (pageable) {
+        slow.push_back({host, const_cast<char*>(dev), bytes});
+        return;
+      }
       const cudaError_t r = cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, cs_);
       if (r != cudaSuccess && e == cudaSuccess) e = r;
+    };
+    // pageable runs are queued through this thread's PageableCopier, whose
+    // landed pieces are written out each round and the rest at the end
+    auto flush = [&] {
+      if (!slow.empty()) {
+        if (!pc_) pc_.reset(new PageableCopier());
+        const cudaError_t r = pc_->enqueue_d2h(slow, cs_);
+        if (r != cudaSuccess && e == cudaSuccess) e = r;
+        slow.clear();
+      }
+      if (pc_) {
+        const cudaError_t r = pc_->poll();
+        if (r != cudaSuccess && e == cudaSuccess) e = r;
+      }
     };
     for (;;) {
       const cudaError_t q = cudaEventQuery(j.solved);
@@ -180,14 +478,15 @@ class PipeWorker {
       if (q != cudaSuccess && q != cudaErrorNotReady && e == cudaSuccess) e = q;
       for (size_t b = 0; b < j.blocks.size(); b++) {
         const PipeJob::Blocks& o = j.blocks[b];
-        int32_t c = j.prog[o.task];
+        int32_t c = j.prog[o.task] - o.lag;
         c = c < 0 ? 0 : (c > o.nx ? o.nx : c);
         if (c > done[b] && (fin || c - done[b] >= kChunk)) {
           const size_t off = (size_t)(o.nx - c) * o.blk;
-          copy(o.host + off, o.dev + off, (size_t)(c - done[b]) * o.blk);
+          copy(o.host + off, o.dev + off, (size_t)(c - done[b]) * o.blk, o.pageable);
           done[b] = c;
         }
       }
+      flush();
       if (fin) break;
       std::this_thread::sleep_for(std::chrono::microseconds(50));
     }
@@ -195,9 +494,14 @@ class PipeWorker {
     if (w != cudaSuccess && e == cudaSuccess) e = w;
     for (size_t b = 0; b < j.blocks.size(); b++) {   // blocks no counter covered
       const PipeJob::Blocks& o = j.blocks[b];
-      if (done[b] < o.nx) copy(o.host, o.dev, (size_t)(o.nx - done[b]) * o.blk);
+      if (done[b] < o.nx) copy(o.host, o.dev, (size_t)(o.nx - done[b]) * o.blk, o.pageable);
     }
-    for (const PipeJob::Copy& r : j.rest) copy(r.host, r.dev, r.bytes);
+    for (const PipeJob::Copy& r : j.rest) copy(r.host, r.dev, r.bytes, r.pageable);
+    flush();
+    if (pc_) {
+      const cudaError_t r = pc_->finish();
+      if (r != cudaSuccess && e == cudaSuccess) e = r;
+    }
     const cudaError_t f = cudaEventRecord(j.freed, cs_);
     if (f != cudaSuccess && e == cudaSuccess) e = f;
     return e;
@@ -212,6 +516,7 @@ class PipeWorker {
   uint64_t pushed_ = 0, issued_ = 0;
   int pending_[2] = {0, 0};
   cudaError_t err_ = cudaSuccess;
+  std::unique_ptr<PageableCopier> pc_;   // made by the thread on its first pageable copy
   std::thread th_;   // last member: started once the others exist
 };
 
@@ -242,6 +547,7 @@ struct rgf_ctx {
   int pipe_sel = 0, pipe_last = -1;
   std::vector<int64_t> pipe_nb[2];   // block size of each task of the call, for the stats
   std::unique_ptr<PipeWorker> worker;
+  std::unique_ptr<PageableCopier> pcopy;   // the calling thread's copies to / from pageable arrays
 };
 
 void* rgf::ctx_ext_cache(rgf_ctx* c) { return c->ext_cache; }
@@ -393,12 +699,13 @@ struct Stage {
     size_t bytes;
     bool copy_in;   // input, or output whose untouched parts must survive
     bool copy_out;  // output
+    bool pageable;  // not page-locked: copied through the PageableCopier
   };
   struct Seg {
     const char* host;
     size_t bytes;
     size_t off;
-    bool copy_in, copy_out;
+    bool copy_in, copy_out, pageable;
   };
   // Pinned (page-locked, mapped) host outputs the kernels only write are not
   // staged: the kernels write them through their device mapping, so the
@@ -431,7 +738,7 @@ struct Stage {
         return;
       }
     }
-    items.push_back({(const char*)p, bytes, copy_in, copy_out});
+    items.push_back({(const char*)p, bytes, copy_in, copy_out, a.type == cudaMemoryTypeUnregistered});
   }
   void layout() {
     std::vector<Item> v = items;
@@ -444,8 +751,9 @@ struct Stage {
         s.bytes = (size_t)(end - s.host);
         s.copy_in = s.copy_in || it.copy_in;
         s.copy_out = s.copy_out || it.copy_out;
+        s.pageable = s.pageable || it.pageable;
       } else {
-        segs.push_back({it.host, it.bytes, 0, it.copy_in, it.copy_out});
+        segs.push_back({it.host, it.bytes, 0, it.copy_in, it.copy_out, it.pageable});
       }
     }
     total = 0;
@@ -487,6 +795,40 @@ struct Stage {
 };
 
 }  // namespace
+
+// The calling thread's copier for pageable host arrays (made on first use).
+static PageableCopier& pageable_copier(rgf_ctx* c) {
+  if (!c->pcopy) c->pcopy.reset(new PageableCopier());
+  return *c->pcopy;
+}
+
+// Host -> staging copies of a call's input segments, after the work already
+// on st: page-locked ones as stream copies, pageable ones through the
+// PageableCopier (its sources are read when this returns).
+static int stage_in(rgf_ctx* c, const Stage& sg, char* sbase, cudaStream_t st) {
+  std::vector<PageableCopier::Copy> slow;
+  for (const auto& s : sg.segs) {
+    if (!s.copy_in) continue;
+    if (s.pageable) slow.push_back({const_cast<char*>(s.host), sbase + s.off, s.bytes});
+    else RGF_CUDA(cudaMemcpyAsync(sbase + s.off, s.host, s.bytes, cudaMemcpyHostToDevice, st));
+  }
+  if (!slow.empty()) RGF_CUDA(pageable_copier(c).h2d(slow, st));
+  return RGF_OK;
+}
+
+// Staging -> host copies of a call's output segments, queued on st after the
+// solve: the pageable ones are on the host when this returns, the others
+// once st has drained.
+static int stage_out(rgf_ctx* c, const Stage& sg, char* sbase, cudaStream_t st) {
+  std::vector<PageableCopier::Copy> slow;
+  for (const auto& s : sg.segs) {
+    if (!s.copy_out) continue;
+    if (s.pageable) slow.push_back({const_cast<char*>(s.host), sbase + s.off, s.bytes});
+    else RGF_CUDA(cudaMemcpyAsync(const_cast<char*>(s.host), sbase + s.off, s.bytes, cudaMemcpyDeviceToHost, st));
+  }
+  if (!slow.empty()) RGF_CUDA(pageable_copier(c).d2h(slow, st));
+  return RGF_OK;
+}
 
 // Kernel parameters common to every launch of a context.
 static void fill_params(const rgf_ctx* c, KParams& p) {
@@ -607,9 +949,12 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
     sg.add(k.ldos, cb, false, true, true);
     sg.add(k.ndens, cb, false, true, true);
     sg.add(k.pdens, cb, false, true, true);
-    sg.add(k.GRi1, cb, true, true, true);   // block nx is left untouched, as in the reference
-    sg.add(k.GLi1, cb, true, true, true);
-    sg.add(k.GGi1, cb, true, true, true);
+    // block nx of GRi1 / GLi1 / GGi1 is never written (the reference leaves
+    // it untouched): blocks 1 .. nx-1 alone are staged and copied back
+    const size_t cb1 = cb - (size_t)v.nm * v.nm * sizeof(rgf_c16);
+    sg.add(k.GRi1, cb1, false, true, true);
+    sg.add(k.GLi1, cb1, false, true, true);
+    sg.add(k.GGi1, cb1, false, true, true);
     sg.add(k.cur, rb, false, true);
     sg.add(k.tr, sizeof(double), false, true, true);
     sg.add(k.tre, sizeof(double), false, true, true);
@@ -656,8 +1001,7 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
   rc = stg.reserve(std::max<size_t>(sg.total, 256));
   if (rc) return rc;
   char* sbase = (char*)stg.p;
-  for (const auto& s : sg.segs)
-    if (s.copy_in) RGF_CUDA(cudaMemcpyAsync(sbase + s.off, s.host, s.bytes, cudaMemcpyHostToDevice, st));
+  if ((rc = stage_in(c, sg, sbase, st))) return rc;
 
   // ---- device tables
   std::vector<DDev> ddev(n_devices);
@@ -752,11 +1096,15 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
       const size_t n2 = (size_t)v.nm * v.nm;
       const void* outs[7] = {k.ldos, k.ndens, k.pdens, k.GRi1, k.GLi1, k.GGi1, k.cur};
       for (int a = 0; a < 7; a++) {
-        if (!sg.find(outs[a])) continue;
+        const Stage::Seg* sgm = sg.find(outs[a]);
+        if (!sgm) continue;
         const size_t blk = n2 * (a == 6 ? sizeof(double) : sizeof(rgf_c16));
         char* h = (char*)outs[a];
-        j.blocks.push_back({h, (const char*)sg.resolve(outs[a], sbase), blk, t, (int32_t)v.nx});
-        covered.push_back({h, h + blk * (size_t)v.nx});
+        // GRi1 / GLi1 / GGi1: blocks 1 .. nx-1, done one counter step later
+        const int32_t lag = (a >= 3 && a <= 5) ? 1 : 0;
+        const int32_t nblk = (int32_t)v.nx - lag;
+        j.blocks.push_back({h, (const char*)sg.resolve(outs[a], sbase), blk, t, nblk, lag, sgm->pageable});
+        covered.push_back({h, h + blk * (size_t)nblk});
       }
     }
     std::sort(covered.begin(), covered.end());
@@ -766,13 +1114,14 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
       const char* at = sgm.host;
       for (const auto& r : covered) {
         if (r.second <= at || r.first >= end) continue;
-        if (r.first > at) j.rest.push_back({(char*)at, sbase + sgm.off + (at - sgm.host), (size_t)(r.first - at)});
+        if (r.first > at)
+          j.rest.push_back({(char*)at, sbase + sgm.off + (at - sgm.host), (size_t)(r.first - at), sgm.pageable});
         at = std::max(at, r.second);
         if (at >= end) break;
       }
-      if (at < end) j.rest.push_back({(char*)at, sbase + sgm.off + (at - sgm.host), (size_t)(end - at)});
+      if (at < end) j.rest.push_back({(char*)at, sbase + sgm.off + (at - sgm.host), (size_t)(end - at), sgm.pageable});
     }
-    j.rest.push_back({(char*)c->pipe_info[pb], (const char*)dinfo, sizeof(DInfo) * (size_t)n_tasks});
+    j.rest.push_back({(char*)c->pipe_info[pb], (const char*)dinfo, sizeof(DInfo) * (size_t)n_tasks, false});
     c->worker->push(std::move(j));
     c->pipe_info_n[pb] = n_tasks;
     c->pipe_nb[pb].resize(n_tasks);
@@ -784,9 +1133,11 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
   }
 
   // ---- outputs back
-  for (const auto& s : sg.segs)
-    if (s.copy_out)
-      RGF_CUDA(cudaMemcpyAsync(const_cast<char*>(s.host), sbase + s.off, s.bytes, cudaMemcpyDeviceToHost, st));
+  if ((rc = stage_out(c, sg, sbase, st))) return rc;
+  // the stream is drained before the task info comes back: a copy into
+  // pageable memory that waits for a running kernel stalls other host
+  // threads' launches (per-thread contexts then run one after another)
+  RGF_CUDA(cudaStreamSynchronize(st));
   std::vector<DInfo> hinfo(n_tasks);
   RGF_CUDA(cudaMemcpyAsync(hinfo.data(), c->info.p, sizeof(DInfo) * n_tasks, cudaMemcpyDeviceToHost, st));
   RGF_CUDA(cudaStreamSynchronize(st));
@@ -845,6 +1196,7 @@ extern "C" int rgf_block_product(rgf_ctx* c, int32_t precision, int64_t nb, int6
   cudaError_t e = launch_block_mixed(mode, 0, (const double2*)A, conj_a, (const double2*)B, conj_b, (double2*)C,
                                      count, (double2*)c->work.p, grid, (int32_t*)c->info.p, st);
   if (e != cudaSuccess) return fail(RGF_E_CUDA, "block product launch failed: %s", cudaGetErrorString(e));
+  RGF_CUDA(cudaStreamSynchronize(st));   // see rgf_solve_batch: no pageable copy behind a running kernel
   std::vector<int32_t> h((size_t)count);
   RGF_CUDA(cudaMemcpyAsync(h.data(), c->info.p, sizeof(int32_t) * (size_t)count, cudaMemcpyDeviceToHost, st));
   RGF_CUDA(cudaStreamSynchronize(st));
@@ -872,6 +1224,7 @@ extern "C" int rgf_block_inverse(rgf_ctx* c, int32_t precision, int64_t nb, int6
                         : launch_block_fp64_inv((int)nb, (const double2*)X, (double2*)Xinv, count,
                                                 (double2*)c->work.p, grid, (int32_t*)c->info.p, st);
   if (e != cudaSuccess) return fail(RGF_E_CUDA, "block inverse launch failed: %s", cudaGetErrorString(e));
+  RGF_CUDA(cudaStreamSynchronize(st));   // see rgf_solve_batch: no pageable copy behind a running kernel
   std::vector<int32_t> h((size_t)count);
   RGF_CUDA(cudaMemcpyAsync(h.data(), c->info.p, sizeof(int32_t) * (size_t)count, cudaMemcpyDeviceToHost, st));
   RGF_CUDA(cudaStreamSynchronize(st));
@@ -909,8 +1262,7 @@ extern "C" int rgf_adjoint_energies(rgf_ctx* c, const rgf_device* v, int64_t nen
   int rc = c->stage.reserve(std::max<size_t>(sg.total, 256));
   if (rc) return rc;
   char* sbase = (char*)c->stage.p;
-  for (const auto& s : sg.segs)
-    if (s.copy_in) RGF_CUDA(cudaMemcpyAsync(sbase + s.off, s.host, s.bytes, cudaMemcpyHostToDevice, st));
+  if ((rc = stage_in(c, sg, sbase, st))) return rc;
   // the gradients are always produced on the device (the current needs them)
   const size_t grad_bytes = sizeof(double) * (size_t)nen * (nx + 2);
   double* dT_d = dTdV ? (double*)sg.resolve(dTdV, sbase) : nullptr;
@@ -976,9 +1328,11 @@ extern "C" int rgf_adjoint_energies(rgf_ctx* c, const rgf_device* v, int64_t nen
       w[k] = (fl - fr) * dE * kE0 / kTpi / kHbar * kE0 * spindeg;
     }
   }
-  for (const auto& sgm : sg.segs)
-    if (sgm.copy_out)
-      RGF_CUDA(cudaMemcpyAsync(const_cast<char*>(sgm.host), sbase + sgm.off, sgm.bytes, cudaMemcpyDeviceToHost, st));
+  if ((rc = stage_out(c, sg, sbase, st))) return rc;
+  // the stream is drained before the task info comes back: a copy into
+  // pageable memory that waits for a running kernel stalls other host
+  // threads' launches (per-thread contexts then run one after another)
+  RGF_CUDA(cudaStreamSynchronize(st));
   std::vector<double> hgrad;
   std::vector<double> hds;
   if (dIdV || dIds) {
@@ -1089,6 +1443,7 @@ void run_batch(Coalescer& co, std::vector<Pending*>& batch, double boltz) {
     rgf_opts_default(&o);
     o.boltz = boltz;
     o.want_T = 0;
+    o.pipelined = 1;   // the batch's host copies run while it solves (synchronised below)
     rc = rgf_ctx_create(&o, &co.ctx[slot]);
     co.ctx_boltz[slot] = boltz;
   }
@@ -1106,7 +1461,7 @@ void run_batch(Coalescer& co, std::vector<Pending*>& batch, double boltz) {
     }
     rc = rgf_solve_batch(co.ctx[slot], devs.data(), (int32_t)devs.size(), tasks.data(), (int64_t)tasks.size(),
                          nullptr, nullptr);
-    if (rc == RGF_E_STATUS) rc = RGF_OK;   // status bits only mean "SEVERE warning"
+    if (rc == RGF_OK) rc = rgf_ctx_synchronize(co.ctx[slot]);   // every output on the host
   }
   const std::string err = rc ? rgf_last_error() : std::string();
   std::lock_guard<std::mutex> g(co.mu);
@@ -1435,6 +1790,7 @@ extern "C" int rgf_plan_execute(rgf_plan* pl, rgf_task_info* info, void* stream_
   c->stats.launches++;
   if (!info) return RGF_OK;
   std::vector<DInfo> h(pl->n_tasks);
+  RGF_CUDA(cudaStreamSynchronize(st));   // see rgf_solve_batch: no pageable copy behind a running kernel
   RGF_CUDA(cudaMemcpyAsync(h.data(), pl->info.p, sizeof(DInfo) * pl->n_tasks, cudaMemcpyDeviceToHost, st));
   RGF_CUDA(cudaStreamSynchronize(st));
   int worst = 0;
@@ -1607,8 +1963,7 @@ extern "C" int rgf_w_solve_batch(rgf_ctx* c, const rgf_w_device* devices, int32_
   int rc = c->stage.reserve(std::max<size_t>(sg.total, 256));
   if (rc) return rc;
   char* sbase = (char*)c->stage.p;
-  for (const auto& s : sg.segs)
-    if (s.copy_in) RGF_CUDA(cudaMemcpyAsync(sbase + s.off, s.host, s.bytes, cudaMemcpyHostToDevice, st));
+  if ((rc = stage_in(c, sg, sbase, st))) return rc;
   std::vector<DDev> ddev(n_devices);
   for (int32_t d = 0; d < n_devices; d++) {
     std::memset(&ddev[d], 0, sizeof(DDev));
@@ -1671,9 +2026,11 @@ extern "C" int rgf_w_solve_batch(rgf_ctx* c, const rgf_w_device* devices, int32_
   if (e != cudaSuccess) return fail(RGF_E_CUDA, "W launch failed: %s", cudaGetErrorString(e));
   c->stats.launches++;
   RGF_CUDA(cudaEventRecord(c->ev1, st));
-  for (const auto& s : sg.segs)
-    if (s.copy_out)
-      RGF_CUDA(cudaMemcpyAsync(const_cast<char*>(s.host), sbase + s.off, s.bytes, cudaMemcpyDeviceToHost, st));
+  if ((rc = stage_out(c, sg, sbase, st))) return rc;
+  // the stream is drained before the task info comes back: a copy into
+  // pageable memory that waits for a running kernel stalls other host
+  // threads' launches (per-thread contexts then run one after another)
+  RGF_CUDA(cudaStreamSynchronize(st));
   std::vector<DInfo> hinfo(n_tasks);
   RGF_CUDA(cudaMemcpyAsync(hinfo.data(), c->info.p, sizeof(DInfo) * n_tasks, cudaMemcpyDeviceToHost, st));
   RGF_CUDA(cudaStreamSynchronize(st));

@@ -259,3 +259,53 @@ def test_pipelined_calls_match_synchronous_calls(rgf):
         for n in w:
             assert np.array_equal(g[n], w[n]), n
     assert st["last_tasks"] == nen and st["last_kernel_ms"] > 0 and st["last_flops"] > 0
+
+
+def test_pageable_host_arrays_match_device_arrays(rgf):
+    """Pageable (not page-locked) host inputs and outputs go through the
+    library's bounce copier (pinned slots of 32 MB, host side split over a
+    thread pool) in both directions.  With per-energy Sigma^R / Sigma^< and
+    every output kind about 126 MB per array -- several passes over the four
+    slots -- a synchronous call and a pipelined call on pageable NumPy arrays
+    give bit for bit the outputs of the same solve on device-resident arrays,
+    and block nx of GRi1, which the solver never writes, keeps its host value
+    in both."""
+    import torch
+    nm, nx, nen = 64, 40, 48
+    d = S.make_device(nm, nx, seed=41)
+    E = S.energy_grid(nen, -2.5, 2.5)
+    rng = np.random.default_rng(5)
+    shape = (nen, nx, nm, nm)
+    eye = np.eye(nm)
+    sig_r = np.ascontiguousarray(np.broadcast_to(-0.01j * eye, shape)
+                                 + 1e-3 * (rng.normal(size=shape) + 1j * rng.normal(size=shape)))
+    sig_l = np.ascontiguousarray(np.broadcast_to(0.004j * eye, shape)
+                                 + 1e-4 * (rng.normal(size=shape) + 1j * rng.normal(size=shape)))
+    kinds = ("ldos", "ndens", "pdens", "GRi1")
+
+    def host_outs():
+        o = {k: np.zeros(shape, complex) for k in kinds}
+        o["GRi1"][:] = complex(3.0, -1.0)
+        o["cur"] = np.zeros(shape)
+        o.update({k: np.zeros(nen) for k in ("tr", "tre")})
+        return o
+    opts = dict(eta_dev=1e-5, eta_lead=1e-5)
+    dev = {k: torch.full(shape, complex(3.0, -1.0), dtype=torch.complex128, device="cuda") for k in kinds}
+    dev["cur"] = torch.zeros(shape, dtype=torch.float64, device="cuda")
+    dev.update({k: torch.zeros(nen, dtype=torch.float64, device="cuda") for k in ("tr", "tre")})
+    with rgf.Context(rgf.Options(**opts)) as ctx:
+        ctx.solve_energies(torch.from_numpy(d.Hii).cuda(), torch.from_numpy(d.H1i).cuda(), E, MU, _temp(),
+                           sigma_lesser=torch.from_numpy(sig_l).cuda(), sigma_r=torch.from_numpy(sig_r).cuda(),
+                           **dev)
+        torch.cuda.synchronize()
+        want = {k: v.cpu().numpy() for k, v in dev.items()}
+        sync = host_outs()
+        ctx.solve_energies(d.Hii, d.H1i, E, MU, _temp(), sigma_lesser=sig_l, sigma_r=sig_r, **sync)
+    with rgf.Context(rgf.Options(pipelined=True, **opts)) as ctx:
+        pipe = host_outs()
+        ctx.solve_energies(d.Hii, d.H1i, E, MU, _temp(), sigma_lesser=sig_l, sigma_r=sig_r, **pipe)
+        ctx.synchronize()
+    assert np.all(want["GRi1"][:, -1] == complex(3.0, -1.0))
+    for got in (sync, pipe):
+        for k in want:
+            assert np.array_equal(got[k], want[k]), k
