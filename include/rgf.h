@@ -97,9 +97,15 @@ typedef struct rgf_opts {
                               while the solve runs and overlap the next call's solve.
                               Host outputs (and tr, tre, T) hold the results after
                               rgf_ctx_synchronize(ctx), which also completes the statistics;
-                              until then the host arrays must not be read or reused.  Overlap
-                              needs pinned host outputs (pageable ones make the call wait for
-                              its copies).  A call with info != NULL runs as with 0. */
+                              until then the host arrays must not be read or reused.
+                              Pageable host outputs are copied by the same thread through
+                              pinned bounce buffers (below), also while the solve runs.  A
+                              call with info != NULL runs as with 0.
+                              Pageable (not page-locked) host arrays, in either mode, move
+                              through pinned bounce slots of the context (16 x 8 MB) with the
+                              host side split over a process-wide pool of host threads, at
+                              the host link's speed rather than the driver's one-thread
+                              pageable path. */
   int32_t reserved[5];
 } rgf_opts;
 
