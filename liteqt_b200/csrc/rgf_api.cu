@@ -200,6 +200,7 @@ class PageableCopier {
       for (size_t at = 0; at < c.bytes;) {
         if (cur.slot < 0) {
           if (free_.empty() && (e = complete(false, true)) != cudaSuccess) return e;
+          if (free_.empty()) return cudaErrorMemoryAllocation;   // a failed call kept its slots
           cur.slot = free_.back();
           free_.pop_back();
           fill = 0;
@@ -234,9 +235,14 @@ class PageableCopier {
     std::vector<Piece> round;
     size_t ci = 0, at = 0;
     std::deque<int> busy;
+    auto give_back = [&](cudaError_t err) {   // slots return to the free list on an error too
+      for (int sl : busy) free_.push_back(sl);
+      return err;
+    };
     while (ci < copies.size()) {
       while (free_.empty()) {
-        if ((e = cudaEventSynchronize(ev_[busy.front()])) != cudaSuccess) return e;
+        if (busy.empty()) return cudaErrorMemoryAllocation;   // a failed call kept its slots
+        if ((e = cudaEventSynchronize(ev_[busy.front()])) != cudaSuccess) return give_back(e);
         free_.push_back(busy.front());
         busy.pop_front();
       }
@@ -260,14 +266,18 @@ class PageableCopier {
         round.push_back(std::move(pc));
       }
       host_side(round, false);
-      for (Piece& pc : round) {
-        if ((e = issue(pc, st, false)) != cudaSuccess) return e;
-        busy.push_back(pc.slot);   // h2d pieces are tracked here, not in inflight_
+      for (size_t i = 0; i < round.size(); i++) {
+        if ((e = issue(round[i], st, false)) != cudaSuccess) {
+          for (size_t k = i; k < round.size(); k++) free_.push_back(round[k].slot);
+          return give_back(e);
+        }
+        busy.push_back(round[i].slot);   // h2d pieces are tracked here, not in inflight_
       }
     }
-    for (int sl : busy) {
-      if ((e = cudaEventSynchronize(ev_[sl])) != cudaSuccess) return e;
-      free_.push_back(sl);
+    while (!busy.empty()) {
+      if ((e = cudaEventSynchronize(ev_[busy.front()])) != cudaSuccess) return give_back(e);
+      free_.push_back(busy.front());
+      busy.pop_front();
     }
     return cudaSuccess;
   }
@@ -293,18 +303,22 @@ class PageableCopier {
     }
     return cudaSuccess;
   }
-  // queues the DMA of one piece and records its slot's event
+  // queues the DMA of one piece and records its slot's event (a d2h piece
+  // whose DMA could not be queued gives its slot back)
   cudaError_t issue(Piece& pc, cudaStream_t st, bool d2h) {
     char* sl = slot_[pc.slot];
+    cudaError_t r = cudaSuccess;
     for (const Part& p : pc.parts) {
-      const cudaError_t r = d2h ? cudaMemcpyAsync(sl + p.off, p.dev, p.bytes, cudaMemcpyDeviceToHost, st)
-                                : cudaMemcpyAsync(p.dev, sl + p.off, p.bytes, cudaMemcpyHostToDevice, st);
-      if (r != cudaSuccess) return r;
+      r = d2h ? cudaMemcpyAsync(sl + p.off, p.dev, p.bytes, cudaMemcpyDeviceToHost, st)
+              : cudaMemcpyAsync(p.dev, sl + p.off, p.bytes, cudaMemcpyHostToDevice, st);
+      if (r != cudaSuccess) break;
     }
-    const cudaError_t r = cudaEventRecord(ev_[pc.slot], st);
-    if (r != cudaSuccess) return r;
-    if (d2h) inflight_.push_back(std::move(pc));
-    return cudaSuccess;
+    if (r == cudaSuccess) r = cudaEventRecord(ev_[pc.slot], st);
+    if (d2h) {
+      if (r == cudaSuccess) inflight_.push_back(std::move(pc));
+      else free_.push_back(pc.slot);
+    }
+    return r;
   }
   // host side of pieces: slot -> destinations (d2h) or sources -> slot, in
   // chunks shared out by the CopyPool
