@@ -470,32 +470,33 @@ def run_ours(args):
         assert np.array_equal(arrs["T"], T.cpu().numpy())
         # (c) the same pipelined calls on pageable NumPy arrays, as a Fortran
         # caller passes them: the library moves them through its pinned
-        # bounce slots (pool of host threads for the pageable side)
-        pg = {k: np.empty(v.shape, v.dtype) for k, v in arrs.items()}
-        Hii_p, H1i_p = np.array(d.Hii), np.array(d.H1i)
+        # bounce slots (pool of host threads for the pageable side).  One
+        # GPU only: every rank would hold another 15.5 GB of host arrays
+        t_pg = None
+        if world == 1:
+            pg = {k: np.empty(v.shape, v.dtype) for k, v in arrs.items()}
+            Hii_p, H1i_p = np.array(d.Hii), np.array(d.H1i)
 
-        def step_pageable():
-            pctx.solve_energies(Hii_p, H1i_p, E, MU, temp, stream=sh, **pg)
-        for _ in range(2):
-            step_pageable()
-        pctx.synchronize()
-        barrier()
-        with torch.cuda.stream(stream):
-            torch.cuda.synchronize(dev)
-            t0 = time.perf_counter()
-            for _ in range(args.steps):
-                flush.fill_(1.0)
+            def step_pageable():
+                pctx.solve_energies(Hii_p, H1i_p, E, MU, temp, stream=sh, **pg)
+            for _ in range(2):
                 step_pageable()
             pctx.synchronize()
-            t_pg = time.perf_counter() - t0
-        barrier()
-        assert np.array_equal(pg["T"], T.cpu().numpy())
-        del pg
+            with torch.cuda.stream(stream):
+                torch.cuda.synchronize(dev)
+                t0 = time.perf_counter()
+                for _ in range(args.steps):
+                    flush.fill_(1.0)
+                    step_pageable()
+                pctx.synchronize()
+                t_pg = time.perf_counter() - t0
+            assert np.array_equal(pg["T"], T.cpu().numpy())
+            del pg
         pctx.close()
         if world > 1:
-            tt = torch.tensor([t_e2e, t_sync, t_pg], dtype=torch.float64, device=dev)
+            tt = torch.tensor([t_e2e, t_sync], dtype=torch.float64, device=dev)
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t_e2e, t_sync, t_pg = float(tt[0].item()), float(tt[1].item()), float(tt[2].item())
+            t_e2e, t_sync = float(tt[0].item()), float(tt[1].item())
         bi = Hii_h.numel() * 16 + H1i_h.numel() * 16
         bo = (ldos_h.numel() + ndens_h.numel()) * 16 + 3 * nen * 8 + \
             sum(v.numel() * v.element_size() for v in extra_h.values())
@@ -507,9 +508,10 @@ def run_ours(args):
                                      "ms_per_step": 1e3 * t_sync / args.steps,
                                      "api": "synchronous rgf_solve_energies per step, outputs written "
                                             "through their device mapping"},
-               "pageable": {"value": nen * world * args.steps / t_pg, "ms_per_step": 1e3 * t_pg / args.steps,
-                            "api": "pipelined rgf_solve_energies on pageable NumPy arrays (as Fortran "
-                                   "passes them), copied through the library's pinned bounce slots"}}
+               "pageable": None if t_pg is None else {
+                   "value": nen * world * args.steps / t_pg, "ms_per_step": 1e3 * t_pg / args.steps,
+                   "api": "pipelined rgf_solve_energies on pageable NumPy arrays (as Fortran passes them), "
+                          "copied through the library's pinned bounce slots"}}
 
     # the other precision form on the same workload and timing, for the ratio
     # the metric names (mixed vs plain FP64)
