@@ -161,16 +161,17 @@ class CopyPool {
 // the host link's speed.  The driver moves a pageable copy through its own
 // pinned buffer with one host thread (about 12 GB/s on the B200 hosts, a
 // quarter of the link); here the DMA lands in (or leaves from) pinned bounce
-// slots, kSlots x kPiece bytes, and the host side of the pieces -- pinned slot
-// <-> the caller's arrays -- is cut into chunks of at most kChunk bytes that
-// the CopyPool copies, every piece that has landed at once, while the next
-// pieces are on the link.
+// slots, kSlots x kPiece bytes, and the host side -- pinned slot <-> the
+// caller's arrays -- is cut into chunks of at most kChunk bytes that the
+// CopyPool copies.
 //   enqueue_d2h queues device -> slot copies on `st` (after the work already
-//   on it), packing the runs into pieces; poll writes the destinations of the
-//   pieces that have landed, finish those of every queued piece (a slot is
-//   reused once its piece is written out, so enqueue_d2h itself completes
-//   older pieces when it runs out of slots).  d2h = enqueue_d2h + finish.
-//   h2d copies host -> device and returns with every source read.
+//   on it), packing the runs into pieces, and hands each queued piece to the
+//   copier's landing thread, which waits for the piece (and every later one
+//   that has also landed), writes out their destinations and frees their
+//   slots; enqueue_d2h waits for a slot when all are queued.  So the calling
+//   thread keeps the link busy while the landed pieces are copied out.
+//   finish waits until every queued piece is written out; d2h = enqueue_d2h
+//   + finish.  h2d copies host -> device and returns with every source read.
 class PageableCopier {
  public:
   struct Copy {
@@ -184,6 +185,14 @@ class PageableCopier {
   static constexpr size_t kSmall = size_t(1) << 20;
 
   ~PageableCopier() {
+    if (th_.joinable()) {
+      {
+        std::lock_guard<std::mutex> l(m_);
+        stop_ = true;
+      }
+      cv_.notify_all();
+      th_.join();
+    }
     for (int s = 0; s < kSlots; s++) {
       if (ev_[s]) cudaEventDestroy(ev_[s]);
       if (slot_[s]) cudaFreeHost(slot_[s]);
@@ -199,10 +208,7 @@ class PageableCopier {
     for (const Copy& c : copies)
       for (size_t at = 0; at < c.bytes;) {
         if (cur.slot < 0) {
-          if (free_.empty() && (e = complete(false, true)) != cudaSuccess) return e;
-          if (free_.empty()) return cudaErrorMemoryAllocation;   // a failed call kept its slots
-          cur.slot = free_.back();
-          free_.pop_back();
+          if ((cur.slot = take_slot()) < 0) return error();
           fill = 0;
         }
         const size_t n = std::min(c.bytes - at, kPiece - fill);
@@ -218,8 +224,14 @@ class PageableCopier {
     if (cur.slot >= 0 && (e = issue(cur, st, true)) != cudaSuccess) return e;
     return cudaSuccess;
   }
-  cudaError_t poll() { return complete(false, false); }
-  cudaError_t finish() { return complete(true, false); }
+  cudaError_t poll() { return error(); }   // the landing thread's first error, if any
+  cudaError_t finish() {
+    std::unique_lock<std::mutex> l(m_);
+    cv_.wait(l, [&] { return inflight_.empty(); });
+    const cudaError_t e = err_;
+    err_ = cudaSuccess;
+    return e;
+  }
   cudaError_t d2h(const std::vector<Copy>& copies, cudaStream_t st) {
     cudaError_t e = enqueue_d2h(copies, st);
     const cudaError_t f = finish();
@@ -227,30 +239,37 @@ class PageableCopier {
   }
   cudaError_t h2d(const std::vector<Copy>& copies, cudaStream_t st) {
     cudaError_t e = setup();
-    if (e == cudaSuccess) e = finish();   // every slot free
+    if (e == cudaSuccess) e = finish();   // the landing thread idle, every slot free
     if (e != cudaSuccess) return e;
     // rounds: as many pieces as there are free slots, their sources copied
     // into the slots in one pool pass, then their DMAs queued; a slot is
     // free again once its DMA has read it
     std::vector<Piece> round;
     size_t ci = 0, at = 0;
-    std::deque<int> busy;
+    std::deque<int> busy_slots;
+    std::vector<int> freel;
+    {
+      std::lock_guard<std::mutex> l(m_);
+      freel.swap(free_);
+    }
     auto give_back = [&](cudaError_t err) {   // slots return to the free list on an error too
-      for (int sl : busy) free_.push_back(sl);
+      for (int sl : busy_slots) freel.push_back(sl);
+      std::lock_guard<std::mutex> l(m_);
+      for (int sl : freel) free_.push_back(sl);
       return err;
     };
     while (ci < copies.size()) {
-      while (free_.empty()) {
-        if (busy.empty()) return cudaErrorMemoryAllocation;   // a failed call kept its slots
-        if ((e = cudaEventSynchronize(ev_[busy.front()])) != cudaSuccess) return give_back(e);
-        free_.push_back(busy.front());
-        busy.pop_front();
+      while (freel.empty()) {
+        if (busy_slots.empty()) return give_back(cudaErrorMemoryAllocation);   // a failed call kept its slots
+        if ((e = cudaEventSynchronize(ev_[busy_slots.front()])) != cudaSuccess) return give_back(e);
+        freel.push_back(busy_slots.front());
+        busy_slots.pop_front();
       }
       round.clear();
-      while (!free_.empty() && ci < copies.size()) {
+      while (!freel.empty() && ci < copies.size()) {
         Piece pc;
-        pc.slot = free_.back();
-        free_.pop_back();
+        pc.slot = freel.back();
+        freel.pop_back();
         size_t fill = 0;
         while (ci < copies.size() && fill < kPiece) {
           const Copy& c = copies[ci];
@@ -268,18 +287,18 @@ class PageableCopier {
       host_side(round, false);
       for (size_t i = 0; i < round.size(); i++) {
         if ((e = issue(round[i], st, false)) != cudaSuccess) {
-          for (size_t k = i; k < round.size(); k++) free_.push_back(round[k].slot);
+          for (size_t k = i; k < round.size(); k++) freel.push_back(round[k].slot);
           return give_back(e);
         }
-        busy.push_back(round[i].slot);   // h2d pieces are tracked here, not in inflight_
+        busy_slots.push_back(round[i].slot);   // h2d pieces are tracked here, not by the landing thread
       }
     }
-    while (!busy.empty()) {
-      if ((e = cudaEventSynchronize(ev_[busy.front()])) != cudaSuccess) return give_back(e);
-      free_.push_back(busy.front());
-      busy.pop_front();
+    while (!busy_slots.empty()) {
+      if ((e = cudaEventSynchronize(ev_[busy_slots.front()])) != cudaSuccess) return give_back(e);
+      freel.push_back(busy_slots.front());
+      busy_slots.pop_front();
     }
-    return cudaSuccess;
+    return give_back(cudaSuccess);
   }
 
  private:
@@ -295,16 +314,44 @@ class PageableCopier {
   };
   cudaError_t setup() {
     if (slot_[0]) return cudaSuccess;
-    for (int s = 0; s < kSlots; s++) {
-      cudaError_t e = cudaHostAlloc((void**)&slot_[s], kPiece, cudaHostAllocDefault);
+    cudaError_t e = cudaGetDevice(&dev_);
+    for (int s = 0; e == cudaSuccess && s < kSlots; s++) {
+      e = cudaHostAlloc((void**)&slot_[s], kPiece, cudaHostAllocDefault);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_[s], cudaEventDisableTiming);
-      if (e != cudaSuccess) return e;
-      free_.push_back(kSlots - 1 - s);
     }
+    if (e != cudaSuccess) {
+      for (int s = 0; s < kSlots; s++) {
+        if (ev_[s]) cudaEventDestroy(ev_[s]);
+        if (slot_[s]) cudaFreeHost(slot_[s]);
+        ev_[s] = nullptr;
+        slot_[s] = nullptr;
+      }
+      return e;
+    }
+    for (int s = 0; s < kSlots; s++) free_.push_back(kSlots - 1 - s);
+    th_ = std::thread([this] { lander(); });
     return cudaSuccess;
   }
-  // queues the DMA of one piece and records its slot's event (a d2h piece
-  // whose DMA could not be queued gives its slot back)
+  cudaError_t error() {
+    std::lock_guard<std::mutex> l(m_);
+    return err_;
+  }
+  // a free slot (waiting for the landing thread to release one), or -1
+  // when none can come back
+  int take_slot() {
+    std::unique_lock<std::mutex> l(m_);
+    cv_.wait(l, [&] { return !free_.empty() || inflight_.empty(); });
+    if (free_.empty()) {
+      if (err_ == cudaSuccess) err_ = cudaErrorMemoryAllocation;   // a failed call kept its slots
+      return -1;
+    }
+    const int sl = free_.back();
+    free_.pop_back();
+    return sl;
+  }
+  // queues the DMA of one piece and records its slot's event; a d2h piece
+  // goes to the landing thread, or gives its slot back if it could not be
+  // queued
   cudaError_t issue(Piece& pc, cudaStream_t st, bool d2h) {
     char* sl = slot_[pc.slot];
     cudaError_t r = cudaSuccess;
@@ -315,57 +362,90 @@ class PageableCopier {
     }
     if (r == cudaSuccess) r = cudaEventRecord(ev_[pc.slot], st);
     if (d2h) {
-      if (r == cudaSuccess) inflight_.push_back(std::move(pc));
-      else free_.push_back(pc.slot);
+      {
+        std::lock_guard<std::mutex> l(m_);
+        if (r == cudaSuccess) inflight_.push_back(std::move(pc));
+        else free_.push_back(pc.slot);
+      }
+      cv_.notify_all();
     }
     return r;
   }
   // host side of pieces: slot -> destinations (d2h) or sources -> slot, in
   // chunks shared out by the CopyPool
   void host_side(const std::vector<Piece>& pieces, bool d2h) {
-    chunks_.clear();
+    std::vector<CopyPool::Chunk>& chunks = d2h ? land_chunks_ : h2d_chunks_;
+    chunks.clear();
     size_t total = 0;
     for (const Piece& pc : pieces)
       for (const Part& p : pc.parts)
         for (size_t a = 0; a < p.bytes; a += kChunk) {
           const size_t n = std::min(kChunk, p.bytes - a);
           char* sl = slot_[pc.slot] + p.off + a;
-          if (d2h) chunks_.push_back({p.host + a, sl, n});
-          else chunks_.push_back({sl, p.host + a, n});
+          if (d2h) chunks.push_back({p.host + a, sl, n});
+          else chunks.push_back({sl, p.host + a, n});
           total += n;
         }
     if (total < kSmall) {
-      for (const CopyPool::Chunk& c : chunks_) std::memcpy(c.dst, c.src, c.bytes);
+      for (const CopyPool::Chunk& c : chunks) std::memcpy(c.dst, c.src, c.bytes);
       return;
     }
-    CopyPool::get().copy(chunks_);
+    CopyPool::get().copy(chunks);
   }
-  // writes out the queued pieces that have landed (all of them if `all`; at
-  // least the oldest if `one`) and frees their slots
-  cudaError_t complete(bool all, bool one) {
+  // landing thread: waits for the oldest queued piece, takes it with every
+  // later piece that has landed too, writes their destinations and frees
+  // their slots
+  void lander() {
+    bool dev_set = false;
     std::vector<Piece> ready;
-    while (!inflight_.empty()) {
-      const int sl = inflight_.front().slot;
-      cudaError_t q = cudaEventQuery(ev_[sl]);
-      if (q == cudaErrorNotReady) {
-        if (!all && !(one && ready.empty())) break;
-        q = cudaEventSynchronize(ev_[sl]);
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> l(m_);
+        cv_.wait(l, [&] { return stop_ || !inflight_.empty(); });
+        if (inflight_.empty()) return;   // stop_
+        if (!dev_set) {
+          cudaSetDevice(dev_);
+          dev_set = true;
+        }
       }
-      if (q != cudaSuccess) return q;
-      ready.push_back(std::move(inflight_.front()));
-      inflight_.pop_front();
+      // the front piece stays queued (finish waits for it) until written out
+      int front;
+      {
+        std::lock_guard<std::mutex> l(m_);
+        front = inflight_.front().slot;
+      }
+      cudaError_t e = cudaEventSynchronize(ev_[front]);
+      size_t take = 1;
+      {
+        std::lock_guard<std::mutex> l(m_);
+        while (take < inflight_.size() && cudaEventQuery(ev_[inflight_[take].slot]) == cudaSuccess) take++;
+        ready.clear();
+        for (size_t k = 0; k < take; k++) ready.push_back(inflight_[k]);
+      }
+      if (e == cudaSuccess) host_side(ready, true);
+      {
+        std::lock_guard<std::mutex> l(m_);
+        if (e != cudaSuccess && err_ == cudaSuccess) err_ = e;
+        for (size_t k = 0; k < take; k++) {
+          free_.push_back(inflight_.front().slot);
+          inflight_.pop_front();
+        }
+      }
+      cv_.notify_all();
     }
-    if (ready.empty()) return cudaSuccess;
-    host_side(ready, true);
-    for (const Piece& pc : ready) free_.push_back(pc.slot);
-    return cudaSuccess;
   }
 
   char* slot_[kSlots] = {};
   cudaEvent_t ev_[kSlots] = {};
+  int dev_ = 0;
+  std::mutex m_;
+  std::condition_variable cv_;
+  bool stop_ = false;
+  cudaError_t err_ = cudaSuccess;
   std::vector<int> free_;          // slots without a queued piece
   std::deque<Piece> inflight_;     // queued device -> host pieces, oldest first
-  std::vector<CopyPool::Chunk> chunks_;
+  std::vector<CopyPool::Chunk> land_chunks_, h2d_chunks_;
+  std::thread th_;                 // the landing thread, started by setup()
 };
 
 // The copier of pipelined calls (rgf_opts.pipelined): one thread per context
@@ -473,7 +553,7 @@ class PipeWorker {
       if (r != cudaSuccess && e == cudaSuccess) e = r;
     };
     // pageable runs are queued through this thread's PageableCopier, whose
-    // landed pieces are written out each round and the rest at the end
+    // landing thread writes them out as they arrive (finish at the end)
     auto flush = [&] {
       if (!slow.empty()) {
         if (!pc_) pc_.reset(new PageableCopier());
