@@ -24,6 +24,10 @@
 
 #include "rgf_internal.h"
 
+#if defined(__x86_64__) && defined(__SSE2__)
+#include <emmintrin.h>
+#endif
+
 using namespace rgf;
 
 namespace {
@@ -81,6 +85,36 @@ struct DevBuf {
   }
 };
 
+// A large host copy with non-temporal (streaming) stores where the host
+// has them: the destination lines are not read into the cache before they
+// are overwritten, so a byte moved costs two memory transfers, not three.
+void stream_copy(char* dst, const char* src, size_t n) {
+#if defined(__x86_64__) && defined(__SSE2__)
+  if (n >= 4096) {
+    const size_t head = (16 - ((uintptr_t)dst & 15)) & 15;
+    std::memcpy(dst, src, head);
+    dst += head;
+    src += head;
+    n -= head;
+    const size_t body = n & ~size_t(63);
+    for (size_t i = 0; i < body; i += 64) {
+      const __m128i a = _mm_loadu_si128(reinterpret_cast<const __m128i*>(src + i));
+      const __m128i b = _mm_loadu_si128(reinterpret_cast<const __m128i*>(src + i + 16));
+      const __m128i c = _mm_loadu_si128(reinterpret_cast<const __m128i*>(src + i + 32));
+      const __m128i d = _mm_loadu_si128(reinterpret_cast<const __m128i*>(src + i + 48));
+      _mm_stream_si128(reinterpret_cast<__m128i*>(dst + i), a);
+      _mm_stream_si128(reinterpret_cast<__m128i*>(dst + i + 16), b);
+      _mm_stream_si128(reinterpret_cast<__m128i*>(dst + i + 32), c);
+      _mm_stream_si128(reinterpret_cast<__m128i*>(dst + i + 48), d);
+    }
+    _mm_sfence();
+    std::memcpy(dst + body, src + body, n - body);
+    return;
+  }
+#endif
+  std::memcpy(dst, src, n);
+}
+
 // Host threads that share out the memcpy chunks of one bounce piece (below).
 // One pool per process: a piece takes it whole (its caller copying too), and
 // a caller that finds it taken copies its piece alone, so concurrent copiers
@@ -101,7 +135,7 @@ class CopyPool {
   void copy(const std::vector<Chunk>& chunks) {
     std::unique_lock<std::mutex> busy(use_, std::try_to_lock);
     if (!busy.owns_lock() || th_.empty() || chunks.size() < 2) {
-      for (const Chunk& c : chunks) std::memcpy(c.dst, c.src, c.bytes);
+      for (const Chunk& c : chunks) stream_copy(c.dst, c.src, c.bytes);
       return;
     }
     {
@@ -129,7 +163,7 @@ class CopyPool {
     for (;;) {
       const size_t i = next_.fetch_add(1);
       if (i >= v.size()) return;
-      std::memcpy(v[i].dst, v[i].src, v[i].bytes);
+      stream_copy(v[i].dst, v[i].src, v[i].bytes);
     }
   }
   void worker() {
