@@ -1590,6 +1590,10 @@ void run_batch(Coalescer& co, std::vector<Pending*>& batch, double boltz) {
     rc = rgf_solve_batch(co.ctx[slot], devs.data(), (int32_t)devs.size(), tasks.data(), (int64_t)tasks.size(),
                          nullptr, nullptr);
     if (rc == RGF_OK) rc = rgf_ctx_synchronize(co.ctx[slot]);   // every output on the host
+    // the batch is complete, so the next one may take the same staging
+    // buffer: the context lives as long as the process, and one buffer of
+    // the batch's output size is what it then holds instead of two
+    co.ctx[slot]->pipe_sel = 0;
   }
   const std::string err = rc ? rgf_last_error() : std::string();
   std::lock_guard<std::mutex> g(co.mu);
