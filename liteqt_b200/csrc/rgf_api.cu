@@ -512,6 +512,79 @@ struct PipeJob {
   std::vector<Copy> rest;
 };
 
+// Follows one solve's progress counters and copies each output block once it
+// is written (chunks of kChunk blocks while the solve runs) on the copy
+// stream `cs`; pageable destinations go through `pc` (made on first use),
+// whose landing thread writes them out.  After the solve: the blocks no
+// counter covered and the rest (scalars, task info); returns once every
+// pageable destination is written and the page-locked copies are queued,
+// after recording j.freed (if any) on `cs`.
+cudaError_t run_copy_job(const PipeJob& j, cudaStream_t cs, std::unique_ptr<PageableCopier>& pc) {
+  constexpr int32_t kChunk = 8;   // blocks per copy while the solve runs
+  std::vector<int32_t> done(j.blocks.size(), 0);
+  cudaError_t e = cudaSuccess;
+  // copies to pageable arrays are gathered per round (flush below); the
+  // others are queued on the copy stream
+  std::vector<PageableCopier::Copy> slow;
+  auto copy = [&](char* host, const char* dev, size_t bytes, bool pageable) {
+    if (pageable) {
+      slow.push_back({host, const_cast<char*>(dev), bytes});
+      return;
+    }
+    const cudaError_t r = cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, cs);
+    if (r != cudaSuccess && e == cudaSuccess) e = r;
+  };
+  // pageable runs are queued through the PageableCopier, whose landing
+  // thread writes them out as they arrive (finish at the end)
+  auto flush = [&] {
+    if (!slow.empty()) {
+      if (!pc) pc.reset(new PageableCopier());
+      const cudaError_t r = pc->enqueue_d2h(slow, cs);
+      if (r != cudaSuccess && e == cudaSuccess) e = r;
+      slow.clear();
+    }
+    if (pc) {
+      const cudaError_t r = pc->poll();
+      if (r != cudaSuccess && e == cudaSuccess) e = r;
+    }
+  };
+  for (;;) {
+    const cudaError_t q = cudaEventQuery(j.solved);
+    const bool fin = q != cudaErrorNotReady;
+    if (q != cudaSuccess && q != cudaErrorNotReady && e == cudaSuccess) e = q;
+    for (size_t b = 0; b < j.blocks.size(); b++) {
+      const PipeJob::Blocks& o = j.blocks[b];
+      int32_t c = j.prog[o.task] - o.lag;
+      c = c < 0 ? 0 : (c > o.nx ? o.nx : c);
+      if (c > done[b] && (fin || c - done[b] >= kChunk)) {
+        const size_t off = (size_t)(o.nx - c) * o.blk;
+        copy(o.host + off, o.dev + off, (size_t)(c - done[b]) * o.blk, o.pageable);
+        done[b] = c;
+      }
+    }
+    flush();
+    if (fin) break;
+    std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+  const cudaError_t w = cudaStreamWaitEvent(cs, j.solved, 0);
+  if (w != cudaSuccess && e == cudaSuccess) e = w;
+  for (size_t b = 0; b < j.blocks.size(); b++) {   // blocks no counter covered
+    const PipeJob::Blocks& o = j.blocks[b];
+    if (done[b] < o.nx) copy(o.host, o.dev, (size_t)(o.nx - done[b]) * o.blk, o.pageable);
+  }
+  for (const PipeJob::Copy& r : j.rest) copy(r.host, r.dev, r.bytes, r.pageable);
+  flush();
+  if (pc) {
+    const cudaError_t r = pc->finish();
+    if (r != cudaSuccess && e == cudaSuccess) e = r;
+  }
+  if (j.freed) {
+    const cudaError_t f = cudaEventRecord(j.freed, cs);
+    if (f != cudaSuccess && e == cudaSuccess) e = f;
+  }
+  return e;
+}
+
 class PipeWorker {
  public:
   PipeWorker(int device, cudaStream_t cs) : dev_(device), cs_(cs), th_([this] { loop(); }) {}
@@ -571,69 +644,7 @@ class PipeWorker {
       cv_.notify_all();
     }
   }
-  cudaError_t run(const PipeJob& j) {
-    constexpr int32_t kChunk = 8;   // blocks per copy while the solve runs
-    std::vector<int32_t> done(j.blocks.size(), 0);
-    cudaError_t e = cudaSuccess;
-    // copies to pageable arrays are gathered per round (flush below); the
-    // others are queued on the copy stream
-    std::vector<PageableCopier::Copy> slow;
-    auto copy = [&](char* host, const char* dev, size_t bytes, bool pageable) {
-      if (pageable) {
-        slow.push_back({host, const_cast<char*>(dev), bytes});
-        return;
-      }
-      const cudaError_t r = cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, cs_);
-      if (r != cudaSuccess && e == cudaSuccess) e = r;
-    };
-    // pageable runs are queued through this thread's PageableCopier, whose
-    // landing thread writes them out as they arrive (finish at the end)
-    auto flush = [&] {
-      if (!slow.empty()) {
-        if (!pc_) pc_.reset(new PageableCopier());
-        const cudaError_t r = pc_->enqueue_d2h(slow, cs_);
-        if (r != cudaSuccess && e == cudaSuccess) e = r;
-        slow.clear();
-      }
-      if (pc_) {
-        const cudaError_t r = pc_->poll();
-        if (r != cudaSuccess && e == cudaSuccess) e = r;
-      }
-    };
-    for (;;) {
-      const cudaError_t q = cudaEventQuery(j.solved);
-      const bool fin = q != cudaErrorNotReady;
-      if (q != cudaSuccess && q != cudaErrorNotReady && e == cudaSuccess) e = q;
-      for (size_t b = 0; b < j.blocks.size(); b++) {
-        const PipeJob::Blocks& o = j.blocks[b];
-        int32_t c = j.prog[o.task] - o.lag;
-        c = c < 0 ? 0 : (c > o.nx ? o.nx : c);
-        if (c > done[b] && (fin || c - done[b] >= kChunk)) {
-          const size_t off = (size_t)(o.nx - c) * o.blk;
-          copy(o.host + off, o.dev + off, (size_t)(c - done[b]) * o.blk, o.pageable);
-          done[b] = c;
-        }
-      }
-      flush();
-      if (fin) break;
-      std::this_thread::sleep_for(std::chrono::microseconds(50));
-    }
-    const cudaError_t w = cudaStreamWaitEvent(cs_, j.solved, 0);
-    if (w != cudaSuccess && e == cudaSuccess) e = w;
-    for (size_t b = 0; b < j.blocks.size(); b++) {   // blocks no counter covered
-      const PipeJob::Blocks& o = j.blocks[b];
-      if (done[b] < o.nx) copy(o.host, o.dev, (size_t)(o.nx - done[b]) * o.blk, o.pageable);
-    }
-    for (const PipeJob::Copy& r : j.rest) copy(r.host, r.dev, r.bytes, r.pageable);
-    flush();
-    if (pc_) {
-      const cudaError_t r = pc_->finish();
-      if (r != cudaSuccess && e == cudaSuccess) e = r;
-    }
-    const cudaError_t f = cudaEventRecord(j.freed, cs_);
-    if (f != cudaSuccess && e == cudaSuccess) e = f;
-    return e;
-  }
+  cudaError_t run(const PipeJob& j) { return run_copy_job(j, cs_, pc_); }
 
   int dev_;
   cudaStream_t cs_;
@@ -676,6 +687,11 @@ struct rgf_ctx {
   std::vector<int64_t> pipe_nb[2];   // block size of each task of the call, for the stats
   std::unique_ptr<PipeWorker> worker;
   std::unique_ptr<PageableCopier> pcopy;   // the calling thread's copies to / from pageable arrays
+  // synchronous calls whose staged outputs are copied while the solve runs:
+  // host-mapped progress counters and the solve's event
+  int32_t* sync_prog = nullptr;
+  int64_t sync_prog_cap = 0;
+  cudaEvent_t sync_solved = nullptr;
 };
 
 void* rgf::ctx_ext_cache(rgf_ctx* c) { return c->ext_cache; }
@@ -757,6 +773,8 @@ extern "C" int rgf_ctx_destroy(rgf_ctx* c) {
     if (c->pipe_info[b]) cudaFreeHost(c->pipe_info[b]);
     if (c->pipe_prog[b]) cudaFreeHost(c->pipe_prog[b]);
   }
+  if (c->sync_prog) cudaFreeHost(c->sync_prog);
+  if (c->sync_solved) cudaEventDestroy(c->sync_solved);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   c->work.release();
   c->tasks.release();
@@ -956,6 +974,45 @@ static int stage_out(rgf_ctx* c, const Stage& sg, char* sbase, cudaStream_t st) 
   }
   if (!slow.empty()) RGF_CUDA(pageable_copier(c).d2h(slow, st));
   return RGF_OK;
+}
+
+// The copies of a solve's staged outputs for run_copy_job: every block-
+// structured output by blocks (GRi1 / GLi1 / GGi1 without their last block,
+// done one counter step later), and the rest of every output segment.
+static void fill_copy_job(PipeJob& j, const rgf_device* devices, const rgf_task* tasks, int64_t n_tasks,
+                          const Stage& sg, char* sbase) {
+  std::vector<std::pair<const char*, const char*>> covered;   // host ranges copied block by block
+  for (int64_t t = 0; t < n_tasks; t++) {
+    const rgf_task& k = tasks[t];
+    const rgf_device& v = devices[k.device];
+    const size_t n2 = (size_t)v.nm * v.nm;
+    const void* outs[7] = {k.ldos, k.ndens, k.pdens, k.GRi1, k.GLi1, k.GGi1, k.cur};
+    for (int a = 0; a < 7; a++) {
+      const Stage::Seg* sgm = sg.find(outs[a]);
+      if (!sgm) continue;
+      const size_t blk = n2 * (a == 6 ? sizeof(double) : sizeof(rgf_c16));
+      char* h = (char*)outs[a];
+      // GRi1 / GLi1 / GGi1: blocks 1 .. nx-1, done one counter step later
+      const int32_t lag = (a >= 3 && a <= 5) ? 1 : 0;
+      const int32_t nblk = (int32_t)v.nx - lag;
+      j.blocks.push_back({h, (const char*)sg.resolve(outs[a], sbase), blk, t, nblk, lag, sgm->pageable});
+      covered.push_back({h, h + blk * (size_t)nblk});
+    }
+  }
+  std::sort(covered.begin(), covered.end());
+  for (const auto& sgm : sg.segs) {   // the rest of every output segment
+    if (!sgm.copy_out) continue;
+    const char* end = sgm.host + sgm.bytes;
+    const char* at = sgm.host;
+    for (const auto& r : covered) {
+      if (r.second <= at || r.first >= end) continue;
+      if (r.first > at)
+        j.rest.push_back({(char*)at, sbase + sgm.off + (at - sgm.host), (size_t)(r.first - at), sgm.pageable});
+      at = std::max(at, r.second);
+      if (at >= end) break;
+    }
+    if (at < end) j.rest.push_back({(char*)at, sbase + sgm.off + (at - sgm.host), (size_t)(end - at), sgm.pageable});
+  }
 }
 
 // Kernel parameters common to every launch of a context.
@@ -1202,6 +1259,27 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
   p.slot_elems = slot;
   p.info = dinfo;
   if (pipe) RGF_CUDA(cudaHostGetDevicePointer((void**)&p.progress, c->pipe_prog[pb], 0));
+  // a synchronous call with at least kProgressiveBytes of staged outputs
+  // copies them as the kernel reports their blocks written, like a
+  // pipelined call, and returns once they are on the host
+  constexpr size_t kProgressiveBytes = size_t(64) << 20;
+  size_t staged_out = 0;
+  for (const auto& sgm : sg.segs)
+    if (sgm.copy_out) staged_out += sgm.bytes;
+  const bool progressive = !pipe && staged_out >= kProgressiveBytes;
+  if (progressive) {
+    if (!c->copy_stream) RGF_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    if (!c->sync_solved) RGF_CUDA(cudaEventCreateWithFlags(&c->sync_solved, cudaEventDisableTiming));
+    if (c->sync_prog_cap < n_tasks) {
+      if (c->sync_prog) cudaFreeHost(c->sync_prog);
+      c->sync_prog = nullptr;
+      c->sync_prog_cap = 0;
+      RGF_CUDA(cudaHostAlloc((void**)&c->sync_prog, sizeof(int32_t) * (size_t)n_tasks, cudaHostAllocMapped));
+      c->sync_prog_cap = n_tasks;
+    }
+    std::memset(c->sync_prog, 0, sizeof(int32_t) * (size_t)n_tasks);
+    RGF_CUDA(cudaHostGetDevicePointer((void**)&p.progress, c->sync_prog, 0));
+  }
   RGF_CUDA(cudaEventRecord(c->ev0, st));
   cudaError_t e = mixed ? launch_mixed(p, grid, st) : launch_solver(p, grid, smem, st);
   if (e != cudaSuccess) return fail(RGF_E_CUDA, "solver launch failed: %s", cudaGetErrorString(e));
@@ -1217,38 +1295,7 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
     j.prog = c->pipe_prog[pb];
     j.solved = c->pipe_solved[pb];
     j.freed = c->pipe_free[pb];
-    std::vector<std::pair<const char*, const char*>> covered;   // host ranges copied block by block
-    for (int64_t t = 0; t < n_tasks; t++) {
-      const rgf_task& k = tasks[t];
-      const rgf_device& v = devices[k.device];
-      const size_t n2 = (size_t)v.nm * v.nm;
-      const void* outs[7] = {k.ldos, k.ndens, k.pdens, k.GRi1, k.GLi1, k.GGi1, k.cur};
-      for (int a = 0; a < 7; a++) {
-        const Stage::Seg* sgm = sg.find(outs[a]);
-        if (!sgm) continue;
-        const size_t blk = n2 * (a == 6 ? sizeof(double) : sizeof(rgf_c16));
-        char* h = (char*)outs[a];
-        // GRi1 / GLi1 / GGi1: blocks 1 .. nx-1, done one counter step later
-        const int32_t lag = (a >= 3 && a <= 5) ? 1 : 0;
-        const int32_t nblk = (int32_t)v.nx - lag;
-        j.blocks.push_back({h, (const char*)sg.resolve(outs[a], sbase), blk, t, nblk, lag, sgm->pageable});
-        covered.push_back({h, h + blk * (size_t)nblk});
-      }
-    }
-    std::sort(covered.begin(), covered.end());
-    for (const auto& sgm : sg.segs) {   // the rest of every output segment
-      if (!sgm.copy_out) continue;
-      const char* end = sgm.host + sgm.bytes;
-      const char* at = sgm.host;
-      for (const auto& r : covered) {
-        if (r.second <= at || r.first >= end) continue;
-        if (r.first > at)
-          j.rest.push_back({(char*)at, sbase + sgm.off + (at - sgm.host), (size_t)(r.first - at), sgm.pageable});
-        at = std::max(at, r.second);
-        if (at >= end) break;
-      }
-      if (at < end) j.rest.push_back({(char*)at, sbase + sgm.off + (at - sgm.host), (size_t)(end - at), sgm.pageable});
-    }
+    fill_copy_job(j, devices, tasks, n_tasks, sg, sbase);
     j.rest.push_back({(char*)c->pipe_info[pb], (const char*)dinfo, sizeof(DInfo) * (size_t)n_tasks, false});
     c->worker->push(std::move(j));
     c->pipe_info_n[pb] = n_tasks;
@@ -1261,7 +1308,18 @@ extern "C" int rgf_solve_batch(rgf_ctx* c, const rgf_device* devices, int32_t n_
   }
 
   // ---- outputs back
-  if ((rc = stage_out(c, sg, sbase, st))) return rc;
+  if (progressive) {
+    RGF_CUDA(cudaEventRecord(c->sync_solved, st));
+    PipeJob j;
+    j.prog = c->sync_prog;
+    j.solved = c->sync_solved;
+    j.freed = nullptr;
+    fill_copy_job(j, devices, tasks, n_tasks, sg, sbase);
+    RGF_CUDA(run_copy_job(j, c->copy_stream, c->pcopy));
+    RGF_CUDA(cudaStreamSynchronize(c->copy_stream));
+  } else if ((rc = stage_out(c, sg, sbase, st))) {
+    return rc;
+  }
   // the stream is drained before the task info comes back: a copy into
   // pageable memory that waits for a running kernel stalls other host
   // threads' launches (per-thread contexts then run one after another)
