@@ -263,13 +263,15 @@ def test_pipelined_calls_match_synchronous_calls(rgf):
 
 def test_pageable_host_arrays_match_device_arrays(rgf):
     """Pageable (not page-locked) host inputs and outputs go through the
-    library's bounce copier (pinned slots of 32 MB, host side split over a
-    thread pool) in both directions.  With per-energy Sigma^R / Sigma^< and
-    every output kind about 126 MB per array -- several passes over the four
-    slots -- a synchronous call and a pipelined call on pageable NumPy arrays
+    library's bounce copier (pinned slots of 8 MB, a landing thread, host
+    side split over a thread pool) in both directions.  With per-energy
+    Sigma^R / Sigma^< and every output kind about 126 MB per array -- many
+    passes over the sixteen slots -- a synchronous call and a pipelined call
+    on pageable NumPy arrays, and a synchronous call on page-locked arrays
+    with zero copy off (outputs copied by DMA as their blocks are written),
     give bit for bit the outputs of the same solve on device-resident arrays,
     and block nx of GRi1, which the solver never writes, keeps its host value
-    in both."""
+    in all of them."""
     import torch
     nm, nx, nen = 64, 40, 48
     d = S.make_device(nm, nx, seed=41)
@@ -305,7 +307,14 @@ def test_pageable_host_arrays_match_device_arrays(rgf):
         pipe = host_outs()
         ctx.solve_energies(d.Hii, d.H1i, E, MU, _temp(), sigma_lesser=sig_l, sigma_r=sig_r, **pipe)
         ctx.synchronize()
+    # page-locked outputs staged (zero_copy off): a synchronous call copies
+    # them by DMA as the kernel reports their blocks written
+    pinned = {k: torch.from_numpy(v).pin_memory() for k, v in host_outs().items()}
+    with rgf.Context(rgf.Options(zero_copy=False, **opts)) as ctx:
+        ctx.solve_energies(d.Hii, d.H1i, E, MU, _temp(), sigma_lesser=sig_l, sigma_r=sig_r,
+                           **{k: v.numpy() for k, v in pinned.items()})
+    pin = {k: v.numpy() for k, v in pinned.items()}
     assert np.all(want["GRi1"][:, -1] == complex(3.0, -1.0))
-    for got in (sync, pipe):
+    for got in (sync, pipe, pin):
         for k in want:
             assert np.array_equal(got[k], want[k]), k
