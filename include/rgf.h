@@ -190,7 +190,9 @@ RGF_API int rgf_ctx_synchronize(rgf_ctx* ctx);
 /* Batched solve: replaces the whole `do ik / !$omp do ie / call green_RGF_RS`
  * loop.  All tasks run in one persistent launch that drains a work queue.
  * `stream` is a cudaStream_t (NULL = the context's stream).  The call returns
- * when all outputs are written (host outputs copied back).  Returns RGF_OK,
+ * when all outputs are written (host outputs copied back; when a call stages
+ * 64 MB or more of host outputs, they are copied while the solve runs, block
+ * by block as the kernel reports them written).  Returns RGF_OK,
  * RGF_E_STATUS if any task status is non-zero, or an error code. */
 RGF_API int rgf_solve_batch(rgf_ctx* ctx, const rgf_device* devices, int32_t n_devices,
                     const rgf_task* tasks, int64_t n_tasks, rgf_task_info* info, void* stream);
