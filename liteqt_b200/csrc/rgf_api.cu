@@ -1361,6 +1361,7 @@ static int block_args(rgf_ctx* c, int32_t precision, int64_t nb, int64_t count, 
   if (!c) return fail(RGF_E_ARG, "ctx is NULL");
   if (precision != RGF_PREC_FP64 && precision != RGF_PREC_MIXED) return fail(RGF_E_ARG, "unknown precision %d", precision);
   if (count < 0) return fail(RGF_E_ARG, "count < 0");
+  if (nb <= 0) return fail(RGF_E_ARG, "nb=%lld", (long long)nb);
   for (const void* p : ptrs)
     if (count > 0 && !is_device_ptr(p)) return fail(RGF_E_ARG, "block arrays must be device memory");
   return RGF_OK;
