@@ -364,3 +364,25 @@ def test_pinned_host_outputs_match_device_outputs(rgf, zero_copy):
     torch.cuda.synchronize()
     for k in dv:
         assert np.array_equal(pin[k].numpy(), dv[k].cpu().numpy()), k
+
+
+@pytest.mark.parametrize("nm", [40, 48, 80])
+def test_generic_variants_longer_chain_match_oracle(rgf, nm):
+    """The register-direct kernel variants (nb = 40: 1x1 subtiles, 48: 1x2,
+    80: 2x2) on a 24-block chain at eta = 1e-5 with scattering, against the
+    FP64 oracle within the spread of one input rounding."""
+    from conftest import compare_spread
+    from oracle import oracle as O
+    nx = 24
+    d = S.make_device(nm, nx, seed=700 + nm)
+    E = np.array([-1.37, -0.21, 0.58, 1.93])
+    sl, sr = random_sigma(nm, nx, len(E), seed=nm + 3)
+    opts = rgf.Options(eta_dev=1e-5, eta_lead=1e-5)
+    oopts = O.Opts(eta_dev=1e-5, eta_lead=1e-5)
+    g = gpu_solve(rgf, d.Hii, d.H1i, E, opts, sl, sr)
+    r = oracle_solve(d.Hii, d.H1i, E, oopts, sl, sr)
+    floors = [oracle_solve(*perturbed_inputs(d.Hii, d.H1i, seed), E, oopts, sl, sr) for seed in range(3)]
+    assert g["rc"] == 0 and np.all(g["info"]["status"] == 0)
+    compare_spread(g, r, floors, nm, d.H1i)
+    assert np.array_equal(g["info"]["sancho_iters_left"], r["stats"]["sancho_iters_left"])
+    assert np.array_equal(g["info"]["sancho_iters_right"], r["stats"]["sancho_iters_right"])
