@@ -44,7 +44,8 @@ def _check(g, r):
     assert np.all(g["WRi1"][:, -1] == 0)   # block nx untouched
 
 
-@pytest.mark.parametrize("nm,nx", [(8, 2), (16, 7), (32, 6), (48, 5), (64, 4), (128, 3)])
+# (64, 40): the block size and chain length of the GW workload's W solves
+@pytest.mark.parametrize("nm,nx", [(8, 2), (16, 7), (32, 6), (48, 5), (64, 4), (128, 3), (64, 40)])
 def test_w_matches_oracle_coulomb(rgf, nm, nx):
     from oracle import oracle as O
     Vii, V1i = S.make_coulomb(nm, nx, seed=nm)
