@@ -147,3 +147,23 @@ def test_adjoint_refuses_an_overlap(rgf):
         rc = rgf.load().rgf_adjoint_energies(ctx.h, rgf.ctypes.byref(cd), 2, E.ctypes.data, T.ctypes.data,
                                              None, None, 1.0, None, None, None, None)
     assert rc == rgf.RGF_E_UNSUPPORTED
+
+
+def test_cms_longer_chain_matches_oracle(rgf):
+    """green_RGF_CMS on a 20-block chain (nb = 64, overlap and scattering in
+    every block) against the FP64 oracle within the spread of one input
+    rounding, GLi1 / GGi1 included."""
+    from conftest import compare_spread
+    from oracle import oracle as O
+    nm, nx = 64, 20
+    d = S.make_device(nm, nx, seed=910)
+    Sii = S.make_overlap(nm, nx, seed=911)
+    E = np.array([-1.83, 0.37, 1.41])
+    sl, sr = random_sigma(nm, nx, len(E), seed=912)
+    g = _gpu(rgf, d, Sii, E, rgf.Options(), sl, sr)
+    r = _oracle(d, Sii, E, O.Opts(), sl, sr)
+    floors = [_oracle(d, Sii, E, O.Opts(), sl, sr, H=perturbed_inputs(d.Hii, d.H1i, s)) for s in range(2)]
+    compare_spread(g, r, floors, nm, d.H1i)   # _gpu has checked every task status
+    for k in ("GLi1", "GGi1"):
+        spread = max(rel_err(f[k][:, :-1], r[k][:, :-1]) for f in floors)
+        assert rel_err(g[k][:, :-1], r[k][:, :-1]) <= max(1e-9, 8.0 * spread), k
